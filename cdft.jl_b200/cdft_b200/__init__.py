@@ -1,0 +1,414 @@
+"""cdft_b200 -- B200-native converge! path of cDFT.jl behind the reference's API.
+
+Host-side mirror of the reference's Julia interface for this path (same names,
+argument meaning and error behaviour, Julia's ``!`` dropped):
+
+    model     = PCSAFT([...], m=..., sigma=..., epsilon=...)       # Clapeyron model stand-in
+    structure = Uniform1DCart((p, T), rho_bulk, [lb, ub], ngrid)   # src/base/structure.jl:310-352
+    system    = DFTSystem(model, structure, Steele(["graphite"]))  # src/base/base.jl:75-90
+    rho       = initialize_profiles(system)                        # src/structure/structure.jl:50-93
+    converge(system, rho, beta=0.1, tol=1e-10, anderson_m=5)        # src/methods/converge.jl:214-254
+    gamma     = surface_tension(system, rho)                       # src/methods/surface_tension.jl:69-91
+
+Every compute call (dF/drho, F_res, converge) runs in libcdft_b200.so on the
+GPU; importing this package raises if the library has not been built.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import CDFTError, PREC_FP64, PREC_MIXED
+from .thermo import PCSAFT, N_A, K_B, R
+
+_LIB = _lib.load()
+
+__all__ = [
+    "PCSAFT", "Steele", "Uniform1DCart", "TwoPhase1DCart", "DFTOptions", "DFTSystem", "AASol",
+    "initialize_profiles", "converge", "batch_converge", "dFdrho_res", "F_res", "F_ideal",
+    "free_energy", "surface_tension", "interfacial_tension", "adsorption", "integrate",
+    "CDFTError", "launch_count",
+]
+
+PSI = 1.3862
+
+# Steele parameter database row (database/Steele/steele_like.csv): epsilon K, sigma A, rho 1/A^3, delta A
+_STEELE_DB = {"graphite": (28.0, 3.4, 0.114, 3.35)}
+
+
+class Steele:
+    """Steele 10-4-3 wall (src/structure/external_fields/steele.jl:31-46);
+    ``width != 0`` adds a second wall at z = width (slit pore)."""
+
+    def __init__(self, surface, width=0.0):
+        self.surface = list(surface)
+        for s in self.surface:
+            if s not in _STEELE_DB:
+                raise KeyError(f"Steele parameters for {s!r} are not in the database")
+        eps, sig, rho, delta = (np.array([_STEELE_DB[s][k] for s in self.surface]) for k in range(4))
+        self.epsilon = eps
+        self.sigma = sig * 1e-10
+        self.rho = rho * 1e30
+        self.delta = delta * 1e-10
+        self.width = float(width)
+
+    def potential(self, model, z, T):
+        """V_ext / k_B T on coordinates z for every component (steele.jl:49-81)."""
+        nc = len(model)
+        V = np.zeros((nc, z.size))
+        for s in range(len(self.surface)):
+            eps_si = np.sqrt(self.epsilon[s] * model.epsilon)
+            sig_si = (self.sigma[s] + model.sigma) / 2
+            for i in range(nc):
+                sg = sig_si[i]
+                pre = 2 * np.pi * self.rho[s] * eps_si[i] * self.delta[s] * sg ** 2
+                for zz in ([z] if self.width == 0 else [z, self.width - z]):
+                    V[i] += pre * (0.4 * (sg / zz) ** 10 - (sg / zz) ** 4
+                                   - sg ** 4 / (3 * self.delta[s] * (zz + 0.61 * self.delta[s]) ** 3))
+        return V / T
+
+
+class Structure:
+    def __init__(self, conditions, rho_bulk, bounds, ngrid, kind, rho_bulk2=None):
+        self.conditions = (float(conditions[0]), float(conditions[1]))
+        self.rho_bulk = np.asarray(rho_bulk, dtype=float)
+        b = np.asarray(bounds, dtype=float).reshape(-1, 2)
+        self.bounds = [tuple(r) for r in b]
+        ng = ngrid if isinstance(ngrid, (tuple, list)) else (ngrid,)
+        self.ngrid = tuple(int(n) for n in ng)
+        if len(self.ngrid) != len(self.bounds):
+            raise ValueError("bounds and ngrid dimensions differ")
+        self.kind = kind
+        self.rho_bulk2 = None if rho_bulk2 is None else np.asarray(rho_bulk2, dtype=float)
+
+    @property
+    def nd(self):
+        return len(self.ngrid)
+
+    def coords(self, d=0):
+        lb, ub = self.bounds[d]
+        return np.linspace(lb, ub, self.ngrid[d])   # LinRange(lb, ub, N)
+
+    def dz(self):
+        return [(ub - lb) / n for (lb, ub), n in zip(self.bounds, self.ngrid)]   # structure_dz
+
+
+def Uniform1DCart(conditions, rho_bulk, bounds, ngrid):
+    """src/base/structure.jl:310-312"""
+    return Structure(conditions, rho_bulk, bounds, ngrid, "uniform")
+
+
+def TwoPhase1DCart(conditions, rho_bulk, rho_bulk2, bounds, ngrid):
+    """src/base/structure.jl:487 (periodic cos seed with two interfaces, two_phase.jl:8-35)"""
+    return Structure(conditions, rho_bulk, bounds, ngrid, "twophase", rho_bulk2)
+
+
+class DFTOptions:
+    """src/base/devices.jl:29-40: ``precision`` is "fp64" (Float64) or "mixed"
+    (FP32 convolutions and Phi, FP64 solver and integrals)."""
+
+    def __init__(self, precision="fp64"):
+        if precision in ("fp64", np.float64, float):
+            self.precision = PREC_FP64
+        elif precision in ("mixed", np.float32):
+            self.precision = PREC_MIXED
+        else:
+            raise ValueError(f"unknown precision {precision!r}")
+
+
+class DFTSystem:
+    """src/base/base.jl:50-90: model, species (get_species, PCSAFT.jl:65-72),
+    structure, external fields and options; owns one device plan."""
+
+    def __init__(self, model, structure, external_field=None, options=None):
+        if structure.nd != 1:
+            raise NotImplementedError("this build converges 1D Cartesian structures")
+        self.model = model
+        self.structure = structure
+        if external_field is None:
+            self.external_field = []
+        elif isinstance(external_field, (list, tuple)):
+            self.external_field = list(external_field)
+        else:
+            self.external_field = [external_field]
+        self.options = options or DFTOptions()
+        p, T = structure.conditions
+        self.L = model.length_scale()
+        self.size = model.d(T)                                   # species.size
+        self.chempot_res = model.mu_res(structure.rho_bulk, T)   # species.chempot_res
+        nc = len(model)
+        N = structure.ngrid[0]
+        self.vext = None
+        if self.external_field:
+            z = structure.coords(0)
+            self.vext = sum(f.potential(model, z, T) for f in self.external_field)
+        d = _lib.SystemDesc()
+        d.nd = 1
+        d.ngrid[0] = N
+        d.bounds[0][0], d.bounds[0][1] = structure.bounds[0]
+        d.coord = _lib.COORD_CART
+        d.nc = nc
+        for i in range(nc):
+            d.m[i] = model.m[i]
+            d.hsd[i] = self.size[i]
+            d.mu_res_plus_ln_rhob[i] = self.chempot_res[i] + np.log(structure.rho_bulk[i])
+            for j in range(nc):
+                d.sigma[i * nc + j] = model.sigma_ij[i, j]
+                d.eps[i * nc + j] = model.eps_ij[i, j]
+        d.L = self.L
+        d.T = T
+        if len(model.assoc) > 1:
+            raise NotImplementedError("one association pair per system is supported")
+        d.n_assoc = len(model.assoc)
+        for i, (eab, kab) in model.assoc.items():
+            d.assoc[0] = _lib.AssocPair(i, i, 1, 1, eab, kab)
+        self._vext_buf = None
+        if self.vext is not None:
+            self._vext_buf = np.ascontiguousarray(self.vext, dtype=np.float64)
+            d.vext = _lib.dptr(self._vext_buf)
+        d.precision = self.options.precision
+        self._desc = d
+        plan = ctypes.c_void_p()
+        _lib.check(_LIB.cdft_plan_create(ctypes.byref(d), ctypes.byref(plan)))
+        self._plan = plan
+
+    @property
+    def nc(self):
+        return len(self.model)
+
+    @property
+    def ngrid(self):
+        return self.structure.ngrid
+
+    def close(self):
+        if getattr(self, "_plan", None):
+            _LIB.cdft_plan_destroy(self._plan)
+            self._plan = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _cos_prof(x, start, stop, shift, coef):
+    # src/structure/structure.jl:2
+    c = np.cos((x - shift) * 2 * np.pi)
+    return 0.5 * (start - stop) * c * np.sqrt((1 + coef ** 2) / (1 + coef ** 2 * c ** 2)) + 0.5 * (start + stop)
+
+
+def initialize_profiles(system, noise=0.0, rng=None):
+    """src/structure/structure.jl:50-93 (+ two_phase.jl:8-35, external_field.jl:21-26).
+    Returns rho with shape (nc, N) -- the memory order of the reference's (N, nc)."""
+    s = system.structure
+    p, T = s.conditions
+    nc = system.nc
+    N = s.ngrid[0]
+    rho = np.empty((nc, N))
+    if s.kind == "uniform":
+        rho[:] = s.rho_bulk[:, None]
+    else:
+        lb, ub = s.bounds[0]
+        H = ub - lb
+        X = s.coords(0)
+        for i in range(nc):
+            Tc = system.model.pure(i).critical_temperature()
+            c0 = (2.4728 - 2.3625 * T / Tc) * (H / system.L)
+            coef = np.sqrt(c0 ** 2 - 1) / 4
+            rho[i] = _cos_prof(X / (ub - lb), s.rho_bulk[i], s.rho_bulk2[i], ub / 4 + 3 * lb / 4, coef)
+    if system.vext is not None:
+        rho *= np.exp(-system.vext / 10)
+    if noise:
+        rng = rng or np.random.default_rng()
+        tot = rho.sum(axis=0)
+        rho *= 1 + noise * (2 * rng.random(rho.shape) - 1)
+        rho *= tot / rho.sum(axis=0)
+    lo = np.finfo(np.float64).tiny ** (1 / 6)
+    hi = np.finfo(np.float64).max ** (1 / 6)
+    return np.clip(rho, lo, hi)
+
+
+class AASol:
+    """src/utils/anderson.jl:193-275 (solver options of aasol)."""
+
+    def __init__(self, m=5, maxit=20, rtol=1e-10, atol=1e-10, beta=1.0, picard_maxit=0, picard_beta=1.0,
+                 picard_rtol=1e-2, picard_atol=1e-2, verbose=False):
+        if m < 0:
+            raise ValueError("m must be >= 0")
+        if not (0 < abs(beta) <= 1):
+            raise ValueError("abs(beta) must be in (0,1]")
+        self.m, self.maxit, self.rtol, self.atol, self.beta = m, maxit, rtol, atol, beta
+        self.picard_maxit, self.picard_beta = picard_maxit, picard_beta
+        self.picard_rtol, self.picard_atol = picard_rtol, picard_atol
+        self.verbose = verbose
+
+    @classmethod
+    def for_system(cls, system=None, maxit=10000, beta=1e-2, tol=1e-4, anderson_start=1e-1, anderson_m=5,
+                   verbose=False):
+        """AASol(system; kwargs...) -> __AASol (converge.jl:3-12)."""
+        return cls(anderson_m, maxit=maxit, rtol=tol, atol=tol, beta=beta, picard_maxit=maxit, picard_beta=beta,
+                   picard_rtol=anderson_start, picard_atol=anderson_start, verbose=verbose)
+
+    def c_opts(self, time_budget_s=0.0, iters_per_launch=0):
+        o = _lib.SolverOpts()
+        o.m, o.maxit, o.rtol, o.atol, o.beta = self.m, self.maxit, self.rtol, self.atol, self.beta
+        o.picard_maxit, o.picard_beta = self.picard_maxit, self.picard_beta
+        o.picard_rtol, o.picard_atol = self.picard_rtol, self.picard_atol
+        o.time_budget_s = time_budget_s
+        o.iters_per_launch = iters_per_launch
+        return o
+
+
+class ConvergeResult:
+    def __init__(self, r, history):
+        self.idid = bool(r.idid)
+        self.errcode = r.errcode
+        self.iterations = r.iterations
+        self.evaluations = r.evaluations
+        self.resnorm = r.resnorm
+        self.tol = r.tol
+        self.history = history
+
+    def __repr__(self):
+        return (f"ConvergeResult(idid={self.idid}, errcode={self.errcode}, iterations={self.iterations}, "
+                f"evaluations={self.evaluations}, resnorm={self.resnorm:.3e})")
+
+
+def _check_rho(system, rho):
+    if not isinstance(rho, np.ndarray) or rho.dtype != np.float64 or not rho.flags["C_CONTIGUOUS"]:
+        raise TypeError("rho must be a C-contiguous float64 numpy array")
+    if rho.shape != (system.nc,) + tuple(reversed(system.ngrid)):
+        raise ValueError(f"rho has shape {rho.shape}, expected {(system.nc,) + tuple(reversed(system.ngrid))}")
+
+
+def converge(system, rho, method=None, time_budget_s=0.0, iters_per_launch=0, keep_history=True, **kwargs):
+    """converge!(system, ρ; kwargs...) / converge!(system, ρ, solver): converges
+    ``rho`` in place (converge.jl:214-254) and returns the aasol status."""
+    _check_rho(system, rho)
+    method = method or AASol.for_system(system, **kwargs)
+    res = _lib.Result()
+    hist = None
+    if keep_history:
+        cap = method.maxit + 2 * method.picard_maxit + 4
+        hist = np.zeros(cap)
+        res.history = _lib.dptr(hist)
+        res.history_cap = cap
+    opts = method.c_opts(time_budget_s, iters_per_launch)
+    _lib.check(_LIB.cdft_converge(system._plan, _lib.dptr(rho), ctypes.byref(opts), ctypes.byref(res)))
+    out = ConvergeResult(res, None if hist is None else hist[: res.history_len].copy())
+    if method.verbose:
+        msg = "DFT converged" if out.idid else "DFT did not converge"
+        print(f"{msg} after {out.evaluations} evaluations: err = {out.resnorm:.3g}")
+    return out
+
+
+def batch_converge(systems, rhos, method=None, time_budget_s=0.0, iters_per_launch=0, **kwargs):
+    """Converge many independent systems (state points, pore widths) together."""
+    n = len(systems)
+    if n != len(rhos):
+        raise ValueError("systems and rhos differ in length")
+    for s, r in zip(systems, rhos):
+        _check_rho(s, r)
+    method = method or AASol.for_system(systems[0], **kwargs)
+    plans = (ctypes.c_void_p * n)(*[s._plan.value for s in systems])
+    ptrs = (ctypes.POINTER(ctypes.c_double) * n)(*[_lib.dptr(r) for r in rhos])
+    res = (_lib.Result * n)()
+    opts = method.c_opts(time_budget_s, iters_per_launch)
+    _lib.check(_LIB.cdft_batch_converge(plans, n, ptrs, ctypes.byref(opts), res))
+    return [ConvergeResult(res[i], None) for i in range(n)]
+
+
+def dFdrho_res(system, rho):
+    """δFδρ_res(system, ρ) (models.jl:194-200): residual functional derivative
+    plus external field, in k_B T, shape (nc, N)."""
+    _check_rho(system, rho)
+    out = np.empty_like(rho)
+    _lib.check(_LIB.cdft_functional_derivative(system._plan, _lib.dptr(rho), _lib.dptr(out)))
+    return out
+
+
+def phi_pointwise(system, n):
+    """Fused Phi and dPhi/dn at points; n has shape (nc, NF, npts)."""
+    n = np.ascontiguousarray(n, dtype=np.float64)
+    npts = n.shape[-1]
+    f = np.empty(npts)
+    g = np.empty_like(n)
+    _lib.check(_LIB.cdft_phi_pointwise(system._plan, _lib.dptr(n), npts, _lib.dptr(f), _lib.dptr(g)))
+    return f, g
+
+
+class _KSum:
+    def __init__(self):
+        self.s = 0.0
+        self.c = 0.0
+
+    def add(self, x):
+        t = self.s + x
+        if abs(self.s) >= abs(x):
+            self.c += (self.s - t) + x
+        else:
+            self.c += (x - t) + self.s
+        self.s = t
+
+    def value(self):
+        return self.s + self.c
+
+
+def integrate(f, structure):
+    """``∫(f, structure)`` (integrals.jl:17,28-41): Simpson weights 1,4,2,...,1,
+    dz = (ub-lb)/N, compensated FP64 summation."""
+    f = np.asarray(f, dtype=float)
+    n = f.shape[-1]
+    k = np.arange(1, n + 1)
+    w = np.where((k == 1) | (k == n), 1.0, np.where(k % 2 == 0, 4.0, 2.0))
+    acc = _KSum()
+    for v in (w * f).ravel():
+        acc.add(float(v))
+    return acc.value() * structure.dz()[0] / 3
+
+
+def F_res(system, rho):
+    """F_res(system, ρ) (models.jl:86-91), per unit area, in k_B T."""
+    _check_rho(system, rho)
+    out = ctypes.c_double()
+    _lib.check(_LIB.cdft_free_energy_res(system._plan, _lib.dptr(rho), ctypes.byref(out)))
+    return out.value
+
+
+def F_ideal(system, rho):
+    """F_ideal(system, ρ) (BasicIdeal.jl:10-38)."""
+    T = system.structure.conditions[1]
+    f = (N_A * rho * (np.log(rho) - 1.5 * np.log(T) - 1)).sum(axis=0)
+    return integrate(f, system.structure)
+
+
+def free_energy(system, rho):
+    """free_energy(system, ρ) = F_ideal + F_res (src/utils/base.jl:8-10)."""
+    return F_ideal(system, rho) + F_res(system, rho)
+
+
+def surface_tension(system, rho):
+    """surface_tension(system, ρ) (surface_tension.jl:69-91), J/m^2; the
+    periodic two-interface seed gives twice the tension (callers divide by 2)."""
+    s = system.structure
+    p, T = s.conditions
+    F = free_energy(system, rho)
+    mu = system.model.chemical_potential(s.rho_bulk, T)
+    chem = sum(mu[i] * integrate(rho[i], s) for i in range(system.nc))
+    return F * K_B * T - chem + p * integrate(np.ones(s.ngrid[0]), s)
+
+
+def interfacial_tension(system, rho):
+    """interfacial_tension(system, ρ) == surface_tension(system, ρ) (interfacial_tension.jl:155)."""
+    return surface_tension(system, rho)
+
+
+def adsorption(system, rho):
+    """adsorption(system, ρ) (adsorption.jl:182-188), mol/m^3 of the domain."""
+    V = np.prod([ub - lb for (lb, ub) in system.structure.bounds])
+    return np.array([integrate(rho[i], system.structure) / V for i in range(system.nc)])
+
+
+def launch_count(reset=False):
+    return _LIB.cdft_launch_count(1 if reset else 0)

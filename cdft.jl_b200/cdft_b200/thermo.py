@@ -1,0 +1,213 @@
+"""Setup-time bulk PC-SAFT for the host API.
+
+In the reference these numbers come from Clapeyron.jl (hard-sphere diameter
+``d``, ``VT_chemical_potential_res``, ``volume``, ``bubble_pressure``,
+``tp_flash``, ``crit_pure``; called from PCSAFT.jl:65-72, two_phase.jl:1-6 and
+src/methods/*.jl).  They enter the hot path only as plain inputs of the C ABI
+(species chemical potentials, bulk densities), so this module is ordinary
+host code: vectorised NumPy, FP64, derivatives by complex step.
+
+Equations: Gross & Sadowski, Ind. Eng. Chem. Res. 40 (2001) 1244 and
+41 (2002) 5510 (2B association).
+"""
+import numpy as np
+
+N_A = 6.02214076e23
+K_B = 1.380649e-23
+R = N_A * K_B
+
+_A = np.array([
+    [0.9105631445, -0.3084016918, -0.0906148351], [0.6361281449, 0.1860531159, 0.4527842806],
+    [2.6861347891, -2.5030047259, 0.5962700728], [-26.547362491, 21.419793629, -1.7241829131],
+    [97.759208784, -65.25588533, -4.1302112531], [-159.59154087, 83.318680481, 13.77663187],
+    [91.297774084, -33.74692293, -8.6728470368]])
+_B = np.array([
+    [0.7240946941, -0.5755498075, 0.0976883116], [2.2382791861, 0.6995095521, -0.2557574982],
+    [-4.0025849485, 3.892567339, -9.155856153], [-21.003576815, -17.215471648, 20.642075974],
+    [26.855641363, 192.67226447, -38.804430052], [206.55133841, -161.82646165, 93.626774077],
+    [-355.60235612, -165.20769346, -29.666905585]])
+
+
+class PCSAFT:
+    """PC-SAFT parameters of a (one-bead-per-component) mixture.
+
+    Clapeyron's parameter database is not shipped, so parameters are explicit:
+    ``m`` segments, ``sigma`` in Angstrom, ``epsilon`` in K, optional ``kij``
+    and 2B association ``assoc = {component_index: (eps_AB_K, kappa_AB)}``.
+    """
+
+    def __init__(self, components, m, sigma, epsilon, kij=None, assoc=None):
+        self.components = list(components)
+        self.m = np.asarray(m, dtype=float)
+        self.sigma = np.asarray(sigma, dtype=float) * 1e-10
+        self.epsilon = np.asarray(epsilon, dtype=float)
+        nc = len(self.m)
+        k = np.zeros((nc, nc)) if kij is None else np.asarray(kij, dtype=float)
+        self.sigma_ij = (self.sigma[:, None] + self.sigma[None, :]) / 2
+        self.eps_ij = np.sqrt(np.outer(self.epsilon, self.epsilon)) * (1 - k)
+        self.assoc = dict(assoc or {})
+
+    def __len__(self):
+        return len(self.m)
+
+    def pure(self, i):
+        a = {0: self.assoc[i]} if i in self.assoc else None
+        return PCSAFT([self.components[i]], [self.m[i]], [self.sigma[i] * 1e10], [self.epsilon[i]], assoc=a)
+
+    def length_scale(self):
+        return float(self.sigma_ij.max())
+
+    def d(self, T):
+        return self.sigma * (1 - 0.12 * np.exp(-3 * self.epsilon / T))
+
+    # -- residual Helmholtz energy density / kT (1/m^3) --------------------------
+    def _f_res(self, rho, T):
+        rn = np.asarray(rho) * N_A
+        tot = rn.sum()
+        x = rn / tot
+        d = self.d(T)
+        z = [np.pi / 6 * (rn * self.m * d ** k).sum() for k in range(4)]
+        e = z[3]
+        ome = 1 - e
+        ahs = (3 * z[1] * z[2] / ome + z[2] ** 3 / (e * ome ** 2) + (z[2] ** 3 / e ** 2 - z[0]) * np.log(ome)) / z[0]
+
+        def gij(dd):
+            return 1 / ome + dd * 3 * z[2] / ome ** 2 + dd ** 2 * 2 * z[2] ** 2 / ome ** 3
+
+        mb = (x * self.m).sum()
+        ahc = mb * ahs - (x * (self.m - 1) * np.log(gij(d / 2))).sum()
+        c1, c2 = (mb - 1) / mb, (mb - 1) * (mb - 2) / mb ** 2
+        pw = e ** np.arange(7)
+        I1 = ((_A[:, 0] + c1 * _A[:, 1] + c2 * _A[:, 2]) * pw).sum()
+        I2 = ((_B[:, 0] + c1 * _B[:, 1] + c2 * _B[:, 2]) * pw).sum()
+        C1 = 1 / (1 + mb * (8 * e - 2 * e ** 2) / ome ** 4
+                  + (1 - mb) * (20 * e - 27 * e ** 2 + 12 * e ** 3 - 2 * e ** 4) / (ome * (2 - e)) ** 2)
+        xx = np.outer(x, x) * np.outer(self.m, self.m) * self.sigma_ij ** 3
+        m2es3 = (xx * self.eps_ij / T).sum()
+        m2e2s3 = (xx * (self.eps_ij / T) ** 2).sum()
+        adisp = -2 * np.pi * tot * I1 * m2es3 - np.pi * tot * mb * C1 * I2 * m2e2s3
+        aas = 0.0
+        for i, (eab, kab) in self.assoc.items():
+            # self-associating 2B: X_A = X_B = X, X = 1/(1 + rho_i X Delta)
+            D = self.sigma_ij[i, i] ** 3 * gij(d[i] / 2) * kab * (np.exp(eab / T) - 1)
+            q = rn[i] * D
+            X = 2 / (1 + np.sqrt(1 + 4 * q))
+            aas = aas + x[i] * 2 * (np.log(X) - X / 2 + 0.5)
+        return tot * (ahc + adisp + aas)
+
+    def mu_res(self, rho, T):
+        """mu_res / kT of every component at molar densities ``rho``."""
+        rho = np.asarray(rho, dtype=float)
+        out = np.empty(len(rho))
+        for i in range(len(rho)):
+            h = 1e-30 * max(rho[i], 1.0)
+            r = rho.astype(complex)
+            r[i] += 1j * h
+            out[i] = self._f_res(r, T).imag / (h * N_A)
+        return out
+
+    def pressure(self, rho, T):
+        rho = np.asarray(rho, dtype=float)
+        rn = rho * N_A
+        return K_B * T * (rn.sum() + (rn * self.mu_res(rho, T)).sum() - self._f_res(rho, T).real)
+
+    def chemical_potential(self, rho, T):
+        """Total mu in J/mol, ideal part matching BasicIdeal (ln rho - 1.5 ln T)."""
+        rho = np.asarray(rho, dtype=float)
+        return R * T * (np.log(rho) - 1.5 * np.log(T) + self.mu_res(rho, T))
+
+    def molar_density(self, p, T, x, phase="liquid"):
+        x = np.asarray(x, dtype=float) / np.sum(x)
+        scale = np.pi / 6 * (x * self.m * self.d(T) ** 3).sum() * N_A
+
+        def f(eta):
+            return self.pressure(x * eta / scale, T) - p
+
+        grid = np.concatenate([np.logspace(-12, -1, 300), np.linspace(0.1005, 0.74, 500)])
+        vals = np.array([f(g) for g in grid])
+        idx = np.nonzero(np.sign(vals[:-1]) != np.sign(vals[1:]))[0]
+        if idx.size == 0:
+            raise ValueError("no density root at the given state")
+        k = idx[-1] if phase == "liquid" else idx[0]
+        a, b, fa = grid[k], grid[k + 1], vals[k]
+        for _ in range(200):
+            c = 0.5 * (a + b)
+            fc = f(c)
+            if (fc > 0) == (fa > 0):
+                a, fa = c, fc
+            else:
+                b = c
+            if b - a <= 1e-16 * b:
+                break
+        return 0.5 * (a + b) / scale
+
+    def volume(self, p, T, x, phase="liquid"):
+        return 1.0 / self.molar_density(p, T, x, phase)
+
+    def saturation(self, T, p0=1e3):
+        """Pure-component VLE: (p_sat, rho_liquid, rho_vapour)."""
+        y = np.log([self.molar_density(p0, T, [1.0], "liquid"), p0 / (R * T)])
+
+        def F(v):
+            a, b = np.exp(v)
+            return np.array([(self.pressure([a], T) - self.pressure([b], T)) / (R * T),
+                             np.log(a / b) + self.mu_res([a], T)[0] - self.mu_res([b], T)[0]])
+
+        for _ in range(100):
+            f0 = F(y)
+            J = np.column_stack([(F(y + h) - F(y - h)) / 2e-7 for h in np.eye(2) * 1e-7])
+            dy = np.linalg.solve(J, f0)
+            dy *= min(1.0, 0.5 / np.max(np.abs(dy)))
+            y = y - dy
+            if np.max(np.abs(dy)) < 1e-13:
+                break
+        a, b = np.exp(y)
+        return float(self.pressure([a], T)), float(a), float(b)
+
+    def critical_temperature(self):
+        """T at which the isotherm first has a horizontal inflection (pure component)."""
+        def min_slope(T):
+            scale = np.pi / 6 * self.m[0] * self.d(T)[0] ** 3 * N_A
+            best = np.inf
+            for eta in np.linspace(0.02, 0.45, 300):
+                r = eta / scale
+                best = min(best, (self.pressure([r * (1 + 1e-6)], T) - self.pressure([r * (1 - 1e-6)], T)) / (2e-6 * r))
+            return best
+        lo, hi = 30.0, 3000.0
+        while min_slope(lo) > 0:
+            lo *= 0.7
+        for _ in range(60):
+            mid = 0.5 * (lo + hi)
+            if min_slope(mid) < 0:
+                lo = mid
+            else:
+                hi = mid
+        return 0.5 * (lo + hi)
+
+    def lle(self, p, T, z=(0.5, 0.5), x1=(0.999, 0.001), x2=(0.001, 0.999), iters=400):
+        """Binary liquid-liquid split at (p, T): K-value substitution + Rachford-Rice."""
+        z = np.asarray(z, dtype=float)
+        x1 = np.asarray(x1, dtype=float)
+        x2 = np.asarray(x2, dtype=float)
+
+        def lnphi(x):
+            r = self.molar_density(p, T, x, "liquid")
+            return self.mu_res(r * x, T) - np.log(p / (r * R * T))
+
+        for _ in range(iters):
+            K = np.exp(lnphi(x1) - lnphi(x2))
+            lo, hi = 1e-12, 1 - 1e-12
+            for _ in range(200):
+                b = 0.5 * (lo + hi)
+                if np.sum(z * (K - 1) / (1 + b * (K - 1))) > 0:
+                    lo = b
+                else:
+                    hi = b
+            n1 = z / (1 + b * (K - 1))
+            n2 = K * n1
+            n1, n2 = n1 / n1.sum(), n2 / n2.sum()
+            done = np.max(np.abs(np.log(n1 / x1))) + np.max(np.abs(np.log(n2 / x2))) < 1e-14
+            x1, x2 = n1, n2
+            if done:
+                break
+        return x1, x2

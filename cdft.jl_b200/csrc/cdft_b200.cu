@@ -1,0 +1,820 @@
+// libcdft_b200: host side of the C ABI declared in include/cdft_b200.h.
+//
+// A plan (one DFTSystem) owns its device tables and work buffers.  A batch is
+// a set of plans converged together: every kernel launch covers all of them
+// and the per-iteration kernel sequence is captured once into a CUDA graph
+// holding `iters_per_launch` fixed-point evaluations; the host only polls a
+// device counter of finished systems between graph launches.
+#include <cuda_runtime.h>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace {
+
+thread_local int g_err_code = 0;
+thread_local char g_err_msg[512] = {0};
+thread_local long long g_launches = 0;
+
+int set_error(int code, const char* fmt, ...)
+{
+    g_err_code = code;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err_msg, sizeof(g_err_msg), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+#define CU(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t _e = (call);                                                                   \
+        if (_e != cudaSuccess)                                                                     \
+            return set_error(CDFT_E_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), \
+                             __FILE__, __LINE__);                                                  \
+    } while (0)
+
+#define CHECK_LAUNCH()                                                                             \
+    do {                                                                                           \
+        cudaError_t _e = cudaGetLastError();                                                       \
+        if (_e != cudaSuccess)                                                                     \
+            return set_error(CDFT_E_CUDA, "kernel launch failed: %s (%s:%d)", cudaGetErrorString(_e), \
+                             __FILE__, __LINE__);                                                  \
+    } while (0)
+
+const double kNA = 6.02214076e23;
+const double kPCSAFT_A[21] = {
+    0.9105631445, -0.3084016918, -0.0906148351, 0.6361281449, 0.1860531159, 0.4527842806,
+    2.6861347891, -2.5030047259, 0.5962700728, -26.547362491, 21.419793629, -1.7241829131,
+    97.759208784, -65.25588533, -4.1302112531, -159.59154087, 83.318680481, 13.77663187,
+    91.297774084, -33.74692293, -8.6728470368};
+const double kPCSAFT_B[21] = {
+    0.7240946941, -0.5755498075, 0.0976883116, 2.2382791861, 0.6995095521, -0.2557574982,
+    -4.0025849485, 3.892567339, -9.155856153, -21.003576815, -17.215471648, 20.642075974,
+    26.855641363, 192.67226447, -38.804430052, 206.55133841, -161.82646165, 93.626774077,
+    -355.60235612, -165.20769346, -29.666905585};
+
+std::once_flag g_const_once;
+int g_const_status = 0;
+
+}  // namespace
+
+struct Batch;
+
+struct cdft_plan {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cdft_system_desc desc;
+    SysDev sys;            // host copy holding device pointers
+    int N = 0, m_cap = -1;
+    double dz[3] = {0, 0, 0};
+    double* d_taps_eval = nullptr;
+    double* d_taps_int = nullptr;
+    float* d_taps_eval32 = nullptr;
+    float* d_taps_int32 = nullptr;
+    double* d_vext = nullptr;
+    double* d_vec = nullptr;      // rho, sol, gx, res, df, out
+    double* d_Q = nullptr;
+    double* d_DG = nullptr;
+    void* d_part = nullptr;
+    void* d_dfield = nullptr;
+    double* d_fval = nullptr;
+    Batch* self = nullptr;        // batch of this plan alone
+};
+
+struct Batch {
+    std::vector<cdft_plan*> plans;
+    int nsys = 0, nc = 0, nd = 0, mixed = 0;
+    cudaStream_t stream = nullptr;
+    SysDev* d_sys = nullptr;
+    AAState* d_st = nullptr;
+    ConvTask* d_tasks = nullptr;
+    int ntasks = 0;
+    Chunk* d_pchunks = nullptr;
+    int npchunks = 0;
+    Chunk* d_echunks = nullptr;
+    int nechunks = 0;
+    double* d_partials = nullptr;
+    int* d_done = nullptr;
+    int* h_done = nullptr;
+    double* d_hist = nullptr;
+    int hist_cap = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_iters = 0;
+};
+
+namespace {
+
+std::mutex g_batch_mu;
+std::map<std::vector<cdft_plan*>, Batch*> g_batches;
+
+int upload_constants()
+{
+    std::call_once(g_const_once, []() {
+        if (cudaMemcpyToSymbol(c_pcsaft_a, kPCSAFT_A, sizeof(kPCSAFT_A)) != cudaSuccess ||
+            cudaMemcpyToSymbol(c_pcsaft_b, kPCSAFT_B, sizeof(kPCSAFT_B)) != cudaSuccess)
+            g_const_status = 1;
+    });
+    if (g_const_status) return set_error(CDFT_E_CUDA, "uploading PC-SAFT constants failed");
+    return 0;
+}
+
+void free_batch(Batch* b)
+{
+    if (!b) return;
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    cudaFree(b->d_sys);
+    cudaFree(b->d_st);
+    cudaFree(b->d_tasks);
+    cudaFree(b->d_pchunks);
+    cudaFree(b->d_echunks);
+    cudaFree(b->d_partials);
+    cudaFree(b->d_done);
+    cudaFree(b->d_hist);
+    if (b->h_done) cudaFreeHost(b->h_done);
+    delete b;
+}
+
+// ---------------------------------------------------------------------------
+// plan construction
+// ---------------------------------------------------------------------------
+int validate_desc(const cdft_system_desc* d)
+{
+    if (!d) return set_error(CDFT_E_INVALID, "desc is NULL");
+    if (d->nd != 1) return set_error(CDFT_E_UNSUPPORTED, "nd=%d: this build converges 1D Cartesian systems", d->nd);
+    if (d->coord != CDFT_COORD_CART) return set_error(CDFT_E_UNSUPPORTED, "only Cartesian coordinates are implemented");
+    if (d->nc < 1 || d->nc > CDFT_MAX_NC) return set_error(CDFT_E_INVALID, "nc=%d out of [1,%d]", d->nc, CDFT_MAX_NC);
+    if (d->ngrid[0] < 2) return set_error(CDFT_E_INVALID, "ngrid[0]=%d < 2", d->ngrid[0]);
+    if (!(d->bounds[0][1] > d->bounds[0][0])) return set_error(CDFT_E_INVALID, "bounds must satisfy ub > lb");
+    if (!(d->L > 0) || !(d->T > 0)) return set_error(CDFT_E_INVALID, "L and T must be positive");
+    if (d->n_assoc < 0 || d->n_assoc > CDFT_MAX_ASSOC) return set_error(CDFT_E_UNSUPPORTED, "n_assoc=%d (one pair supported)", d->n_assoc);
+    for (int i = 0; i < d->nc; ++i)
+        if (!(d->hsd[i] > 0) || !(d->m[i] > 0)) return set_error(CDFT_E_INVALID, "component %d: hsd and m must be positive", i);
+    if (d->n_assoc == 1) {
+        const cdft_assoc_pair& a = d->assoc[0];
+        if (a.icomp < 0 || a.icomp >= d->nc || a.jcomp < 0 || a.jcomp >= d->nc)
+            return set_error(CDFT_E_INVALID, "association pair component out of range");
+    }
+    if (d->precision != CDFT_PREC_FP64 && d->precision != CDFT_PREC_MIXED)
+        return set_error(CDFT_E_INVALID, "precision=%d", d->precision);
+    return 0;
+}
+
+int plan_alloc_m(cdft_plan* p, int m)
+{
+    if (m <= p->m_cap) return 0;
+    cudaFree(p->d_Q);
+    cudaFree(p->d_DG);
+    p->d_Q = p->d_DG = nullptr;
+    const size_t ne = (size_t)p->sys.n_elem;
+    const size_t cols = (size_t)(m > 0 ? m : 1);
+    CU(cudaMalloc(&p->d_Q, ne * cols * sizeof(double)));
+    CU(cudaMalloc(&p->d_DG, ne * cols * sizeof(double)));
+    CU(cudaMemsetAsync(p->d_Q, 0, ne * cols * sizeof(double), p->stream));
+    CU(cudaMemsetAsync(p->d_DG, 0, ne * cols * sizeof(double), p->stream));
+    p->m_cap = m;
+    p->sys.Q = p->d_Q;
+    p->sys.DG = p->d_DG;
+    return 0;
+}
+
+int plan_build(cdft_plan* p)
+{
+    const cdft_system_desc& d = p->desc;
+    SysDev& S = p->sys;
+    memset(&S, 0, sizeof(S));
+    const int N = d.ngrid[0];
+    const int nc = d.nc;
+    p->N = N;
+    S.nd = d.nd;
+    S.N = N;
+    S.nc = nc;
+    S.NF = 6 + d.nd;
+    S.nconv = S.NF - 1;
+    S.ngrid[0] = N; S.ngrid[1] = 1; S.ngrid[2] = 1;
+    S.ksplit = (N + CONV_QC - 1) / CONV_QC;
+    S.n_elem = N * nc;
+    S.mixed = d.precision == CDFT_PREC_MIXED;
+    const double L = d.L, T = d.T;
+    S.NA = kNA * L * L * L;
+    p->dz[0] = (d.bounds[0][1] - d.bounds[0][0]) / N;
+    for (int i = 0; i < nc; ++i) S.cprd[i] = d.mu_res_plus_ln_rhob[i];
+    PhiParams& P = S.phi;
+    P.nc = nc;
+    P.nd = d.nd;
+    P.T = T;
+    for (int i = 0; i < nc; ++i) {
+        P.m[i] = d.m[i];
+        P.d[i] = d.hsd[i] / L;
+    }
+    for (int i = 0; i < nc; ++i)
+        for (int j = 0; j < nc; ++j) {
+            const double s = d.sigma[i * nc + j] / L;
+            const double e = d.eps[i * nc + j];
+            const double c1 = d.m[i] * d.m[j] * s * s * s * e / T;
+            P.c1[i * CDFT_MAX_NC + j] = c1;
+            P.c2[i * CDFT_MAX_NC + j] = c1 * e / T;
+        }
+    P.has_assoc = d.n_assoc;
+    if (d.n_assoc) {
+        const cdft_assoc_pair& a = d.assoc[0];
+        P.a_ic = a.icomp;
+        P.a_jc = a.jcomp;
+        P.a_nia = a.n_ia;
+        P.a_njb = a.n_jb;
+        const double di = P.d[a.icomp], dj = P.d[a.jcomp];
+        P.a_dij = di * dj / (di + dj);
+        const double s = d.sigma[a.icomp * nc + a.jcomp] / L;
+        P.a_K = s * s * s * (exp(a.eps_ab / T) - 1.0) * a.kappa_ab;
+    }
+
+    const size_t ne = (size_t)S.n_elem;
+    const size_t ntap = (size_t)S.nconv * nc * N;
+    const size_t esz = S.mixed ? sizeof(float) : sizeof(double);
+    CU(cudaMalloc(&p->d_taps_eval, ntap * sizeof(double)));
+    CU(cudaMalloc(&p->d_taps_int, ntap * sizeof(double)));
+    CU(cudaMalloc(&p->d_vec, ne * 6 * sizeof(double)));
+    CU(cudaMemsetAsync(p->d_vec, 0, ne * 6 * sizeof(double), p->stream));
+    CU(cudaMalloc(&p->d_part, ntap * S.ksplit * esz));
+    CU(cudaMalloc(&p->d_dfield, (size_t)S.NF * nc * N * esz));
+    CU(cudaMalloc(&p->d_fval, (size_t)N * sizeof(double)));
+    if (d.vext) {
+        CU(cudaMalloc(&p->d_vext, ne * sizeof(double)));
+        CU(cudaMemcpyAsync(p->d_vext, d.vext, ne * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    }
+    S.rho = p->d_vec;
+    S.sol = p->d_vec + ne;
+    S.gx = p->d_vec + 2 * ne;
+    S.res = p->d_vec + 3 * ne;
+    S.df = p->d_vec + 4 * ne;
+    S.out = p->d_vec + 5 * ne;
+    S.part = p->d_part;
+    S.dfield = p->d_dfield;
+    S.fval = p->d_fval;
+    S.vext = p->d_vext;
+    S.taps_eval = p->d_taps_eval;
+    S.taps_int = p->d_taps_int;
+
+    // kernels of get_fields(::PCSAFTModel) (PCSAFT.jl:55-61), fields 2..7 in 1D
+    const double psi = PSI_DISP;
+    const int types[6] = {1, 2, 3, 2, 1, 2};
+    const double wf[6] = {0.5, 0.5, 0.5, 1.0, 1.0, psi};
+    const double span = d.bounds[0][1] - d.bounds[0][0];
+    for (int i = 0; i < nc; ++i)
+        for (int f = 0; f < S.nconv; ++f) {
+            const size_t off = ((size_t)i * S.nconv + f) * N;
+            const double sign = types[f] == 3 ? -1.0 : 1.0;   // vector fields: δfδρ .-= (weighted_densities.jl:381)
+            taps1d_kernel<<<(N + 127) / 128, 128, 0, p->stream>>>(N, span, L, types[f], wf[f] * P.d[i], S.NA,
+                                                                   sign, p->d_taps_eval + off, p->d_taps_int + off);
+            CHECK_LAUNCH();
+        }
+    if (S.mixed) {
+        CU(cudaMalloc(&p->d_taps_eval32, ntap * sizeof(float)));
+        CU(cudaMalloc(&p->d_taps_int32, ntap * sizeof(float)));
+        to_float_kernel<<<(unsigned)((ntap + 255) / 256), 256, 0, p->stream>>>(p->d_taps_eval, p->d_taps_eval32, ntap);
+        to_float_kernel<<<(unsigned)((ntap + 255) / 256), 256, 0, p->stream>>>(p->d_taps_int, p->d_taps_int32, ntap);
+        CHECK_LAUNCH();
+        S.taps_eval32 = p->d_taps_eval32;
+        S.taps_int32 = p->d_taps_int32;
+    }
+    CU(cudaStreamSynchronize(p->stream));
+    return 0;
+}
+
+void plan_free(cdft_plan* p)
+{
+    cudaFree(p->d_taps_eval);
+    cudaFree(p->d_taps_int);
+    cudaFree(p->d_taps_eval32);
+    cudaFree(p->d_taps_int32);
+    cudaFree(p->d_vext);
+    cudaFree(p->d_vec);
+    cudaFree(p->d_Q);
+    cudaFree(p->d_DG);
+    cudaFree(p->d_part);
+    cudaFree(p->d_dfield);
+    cudaFree(p->d_fval);
+    if (p->stream) cudaStreamDestroy(p->stream);
+}
+
+// ---------------------------------------------------------------------------
+// batches
+// ---------------------------------------------------------------------------
+int batch_build(const std::vector<cdft_plan*>& plans, Batch** out)
+{
+    Batch* b = new Batch();
+    b->plans = plans;
+    b->nsys = (int)plans.size();
+    b->nc = plans[0]->desc.nc;
+    b->nd = plans[0]->desc.nd;
+    b->mixed = plans[0]->sys.mixed;
+    b->stream = plans[0]->stream;
+    for (auto* p : plans) {
+        if (p->desc.nc != b->nc || p->desc.nd != b->nd || p->sys.mixed != b->mixed) {
+            free_batch(b);
+            return set_error(CDFT_E_UNSUPPORTED, "systems of one batch must share nc, nd and precision");
+        }
+        if (p->device != plans[0]->device) {
+            free_batch(b);
+            return set_error(CDFT_E_INVALID, "systems of one batch must live on one device");
+        }
+    }
+    std::vector<ConvTask> tasks;
+    std::vector<Chunk> pch, ech;
+    for (int s = 0; s < b->nsys; ++s) {
+        SysDev& S = plans[s]->sys;
+        const int tiles = (S.N + CONV_TILE - 1) / CONV_TILE;
+        for (int i = 0; i < S.nc; ++i)
+            for (int f = 0; f < S.nconv; ++f)
+                for (int t = 0; t < tiles; ++t)
+                    for (int ks = 0; ks < S.ksplit; ++ks) tasks.push_back({s, i, f, t * S.ksplit + ks});
+        for (int j = 0; j < S.N; j += POINT_THREADS) pch.push_back({s, j});
+        S.chunk_begin = (int)ech.size();
+        for (int e = 0; e < S.n_elem; e += ELEM_CHUNK) ech.push_back({s, e});
+        S.chunk_count = (int)ech.size() - S.chunk_begin;
+    }
+    b->ntasks = (int)tasks.size();
+    b->npchunks = (int)pch.size();
+    b->nechunks = (int)ech.size();
+#define BCU(call)                      \
+    do {                               \
+        cudaError_t _e = (call);       \
+        if (_e != cudaSuccess) {       \
+            free_batch(b);             \
+            return set_error(CDFT_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(_e)); \
+        }                              \
+    } while (0)
+    BCU(cudaMalloc(&b->d_sys, sizeof(SysDev) * b->nsys));
+    BCU(cudaMalloc(&b->d_st, sizeof(AAState) * b->nsys));
+    BCU(cudaMalloc(&b->d_tasks, sizeof(ConvTask) * tasks.size()));
+    BCU(cudaMalloc(&b->d_pchunks, sizeof(Chunk) * pch.size()));
+    BCU(cudaMalloc(&b->d_echunks, sizeof(Chunk) * ech.size()));
+    BCU(cudaMalloc(&b->d_partials, sizeof(double) * RED_SLOTS * ech.size()));
+    BCU(cudaMalloc(&b->d_done, sizeof(int)));
+    BCU(cudaMallocHost(&b->h_done, sizeof(int)));
+    BCU(cudaMemcpy(b->d_tasks, tasks.data(), sizeof(ConvTask) * tasks.size(), cudaMemcpyHostToDevice));
+    BCU(cudaMemcpy(b->d_pchunks, pch.data(), sizeof(Chunk) * pch.size(), cudaMemcpyHostToDevice));
+    BCU(cudaMemcpy(b->d_echunks, ech.data(), sizeof(Chunk) * ech.size(), cudaMemcpyHostToDevice));
+#undef BCU
+    *out = b;
+    return 0;
+}
+
+int batch_upload_sys(Batch* b)
+{
+    std::vector<SysDev> h(b->nsys);
+    for (int s = 0; s < b->nsys; ++s) h[s] = b->plans[s]->sys;
+    CU(cudaMemcpyAsync(b->d_sys, h.data(), sizeof(SysDev) * b->nsys, cudaMemcpyHostToDevice, b->stream));
+    return 0;
+}
+
+template <typename T>
+int launch_phi(Batch* b, const AAState* st)
+{
+#define PHI_CASE(NC_, ND_)                                                                              \
+    if (b->nc == NC_ && b->nd == ND_) {                                                                 \
+        phi_kernel<T, NC_, ND_><<<b->npchunks, POINT_THREADS, 0, b->stream>>>(b->d_pchunks, b->d_sys, st); \
+        return 0;                                                                                       \
+    }
+    PHI_CASE(1, 1) PHI_CASE(2, 1) PHI_CASE(3, 1) PHI_CASE(4, 1)
+#undef PHI_CASE
+    return set_error(CDFT_E_UNSUPPORTED, "no Phi kernel for nc=%d nd=%d", b->nc, b->nd);
+}
+
+template <typename T>
+int launch_eval_stages(Batch* b, const AAState* st, bool with_int)
+{
+    const size_t smem = (size_t)(CONV_QC + CONV_TILE + CONV_QC + 31) * sizeof(T);
+    conv1d_kernel<T><<<b->ntasks, CONV_WARPS * 32, smem, b->stream>>>(b->d_tasks, b->d_sys, st, 0);
+    int rc = launch_phi<T>(b, st);
+    if (rc) return rc;
+    g_launches += 2;
+    if (with_int) {
+        conv1d_kernel<T><<<b->ntasks, CONV_WARPS * 32, smem, b->stream>>>(b->d_tasks, b->d_sys, st, 1);
+        g_launches += 1;
+    }
+    return 0;
+}
+
+template <typename T>
+int launch_iteration(Batch* b)
+{
+    int rc = launch_eval_stages<T>(b, b->d_st, true);
+    if (rc) return rc;
+    el_kernel<T><<<b->nechunks, ELEM_THREADS, 0, b->stream>>>(b->d_echunks, b->d_sys, b->d_st, b->d_partials);
+    const int ctl_blocks = (b->nsys * 32 + 127) / 128;
+    ctl_kernel<<<ctl_blocks, 128, 0, b->stream>>>(b->d_sys, b->d_st, b->d_partials, b->nsys, 0, b->d_done);
+    for (int slot = 1; slot <= N_VEC_SLOTS; ++slot) {
+        vec_kernel<<<b->nechunks, ELEM_THREADS, 0, b->stream>>>(b->d_echunks, b->d_sys, b->d_st, b->d_partials, slot);
+        if (slot < N_VEC_SLOTS)
+            ctl_kernel<<<ctl_blocks, 128, 0, b->stream>>>(b->d_sys, b->d_st, b->d_partials, b->nsys, slot, b->d_done);
+    }
+    g_launches += 2 * N_VEC_SLOTS;   // el, ctl0, 5 vec, 4 ctl (eval stages counted above)
+    CHECK_LAUNCH();
+    return 0;
+}
+
+int batch_capture(Batch* b, int iters)
+{
+    if (b->graph && b->graph_iters == iters) return 0;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    cudaGraph_t g;
+    CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    const long long before = g_launches;
+    int rc = 0;
+    for (int it = 0; it < iters && !rc; ++it) rc = b->mixed ? launch_iteration<float>(b) : launch_iteration<double>(b);
+    g_launches = before;
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return set_error(CDFT_E_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return set_error(CDFT_E_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+    b->graph_iters = iters;
+    return 0;
+}
+
+int get_batch(const std::vector<cdft_plan*>& plans, Batch** out)
+{
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    auto it = g_batches.find(plans);
+    if (it != g_batches.end()) {
+        *out = it->second;
+        return 0;
+    }
+    Batch* b = nullptr;
+    int rc = batch_build(plans, &b);
+    if (rc) return rc;
+    g_batches[plans] = b;
+    *out = b;
+    return 0;
+}
+
+void drop_batches_of(cdft_plan* p)
+{
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    for (auto it = g_batches.begin(); it != g_batches.end();) {
+        bool hit = false;
+        for (auto* q : it->first) hit |= (q == p);
+        if (hit) {
+            free_batch(it->second);
+            it = g_batches.erase(it);
+        } else {
+            ++it;
+        }
+    }
+}
+
+int validate_opts(const cdft_solver_opts* o)
+{
+    if (!o) return set_error(CDFT_E_INVALID, "opts is NULL");
+    if (o->m < 0 || o->m > CDFT_MAX_M) return set_error(CDFT_E_INVALID, "m=%d out of [0,%d]", o->m, CDFT_MAX_M);
+    if (!(std::fabs(o->beta) > 0 && std::fabs(o->beta) <= 1)) return set_error(CDFT_E_INVALID, "abs(beta) must be in (0,1]");
+    if (o->maxit < 0 || o->picard_maxit < 0) return set_error(CDFT_E_INVALID, "maxit and picard_maxit must be >= 0");
+    return 0;
+}
+
+// rho pointers: host (is_dev = false) or device arrays of n_elem doubles per system
+int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, bool is_dev,
+                   const cdft_solver_opts* opts, cdft_result* results)
+{
+    int rc = validate_opts(opts);
+    if (rc) return rc;
+    for (size_t s = 0; s < plans.size(); ++s) {
+        if (!plans[s]) return set_error(CDFT_E_INVALID, "plan %zu is NULL", s);
+        if (!rho || !rho[s]) return set_error(CDFT_E_INVALID, "rho %zu is NULL", s);
+    }
+    auto t0 = std::chrono::steady_clock::now();
+    Batch* b = nullptr;
+    rc = get_batch(plans, &b);
+    if (rc) return rc;
+    CU(cudaSetDevice(plans[0]->device));
+    for (auto* p : plans) {
+        rc = plan_alloc_m(p, opts->m);
+        if (rc) return rc;
+    }
+    rc = batch_upload_sys(b);
+    if (rc) return rc;
+    const long long max_evals = (long long)opts->maxit + 2LL * opts->picard_maxit + 4;
+    int hist_cap = (int)std::min<long long>(max_evals, 1 << 20);
+    if (b->hist_cap < hist_cap) {
+        cudaFree(b->d_hist);
+        b->d_hist = nullptr;
+        CU(cudaMalloc(&b->d_hist, sizeof(double) * (size_t)hist_cap * b->nsys));
+        b->hist_cap = hist_cap;
+    }
+    std::vector<AAState> st(b->nsys);
+    for (int s = 0; s < b->nsys; ++s) {
+        AAState& A = st[s];
+        memset(&A, 0, sizeof(A));
+        A.mode = MODE_EVAL_INIT;
+        A.m = opts->m;
+        A.maxit = opts->maxit;
+        A.picard_maxit = opts->picard_maxit;
+        A.beta = opts->beta;
+        A.picard_beta = opts->picard_beta;
+        A.rtol = opts->rtol;
+        A.atol = opts->atol;
+        A.picard_rtol = opts->picard_rtol;
+        A.picard_atol = opts->picard_atol;
+        A.history = b->d_hist + (size_t)s * b->hist_cap;
+        A.history_cap = b->hist_cap;
+    }
+    CU(cudaMemcpyAsync(b->d_st, st.data(), sizeof(AAState) * b->nsys, cudaMemcpyHostToDevice, b->stream));
+    CU(cudaMemsetAsync(b->d_done, 0, sizeof(int), b->stream));
+    for (int s = 0; s < b->nsys; ++s) {
+        cdft_plan* p = plans[s];
+        const size_t bytes = (size_t)p->sys.n_elem * sizeof(double);
+        CU(cudaMemcpyAsync(p->sys.rho, rho[s], bytes, is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->stream));
+    }
+    init_kernel<<<b->nechunks, ELEM_THREADS, 0, b->stream>>>(b->d_echunks, b->d_sys);
+    CHECK_LAUNCH();
+    g_launches += 1;
+    const int K = opts->iters_per_launch > 0 ? opts->iters_per_launch : 16;
+    rc = batch_capture(b, K);
+    if (rc) return rc;
+    const int per_iter = 3 + 2 * N_VEC_SLOTS;   // conv, phi, conv, el, ctl0, 5 vec, 4 ctl
+    long long launched_evals = 0;
+    bool budget_hit = false;
+    while (true) {
+        CU(cudaGraphLaunch(b->graph, b->stream));
+        g_launches += (long long)K * per_iter;
+        launched_evals += K;
+        CU(cudaMemcpyAsync(b->h_done, b->d_done, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+        CU(cudaStreamSynchronize(b->stream));
+        if (*b->h_done >= b->nsys) break;
+        if (launched_evals > max_evals + K) break;   // cannot happen: aasol's caps end every system
+        if (opts->time_budget_s > 0) {
+            const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            if (el > opts->time_budget_s) {
+                budget_hit = true;
+                break;
+            }
+        }
+    }
+    CU(cudaMemcpyAsync(st.data(), b->d_st, sizeof(AAState) * b->nsys, cudaMemcpyDeviceToHost, b->stream));
+    for (int s = 0; s < b->nsys; ++s) {
+        cdft_plan* p = plans[s];
+        const size_t bytes = (size_t)p->sys.n_elem * sizeof(double);
+        CU(cudaMemcpyAsync(rho[s], p->sys.rho, bytes, is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, b->stream));
+    }
+    CU(cudaStreamSynchronize(b->stream));
+    if (results) {
+        for (int s = 0; s < b->nsys; ++s) {
+            cdft_result& r = results[s];
+            const AAState& A = st[s];
+            r.idid = A.idid;
+            r.errcode = A.errcode;
+            r.iterations = A.k;
+            r.evaluations = A.nevals;
+            r.resnorm = A.resnorm;
+            r.tol = A.tol;
+            r.history_len = 0;
+            if (r.history && r.history_cap > 0) {
+                const int n = std::min(std::min(A.nevals, r.history_cap), b->hist_cap);
+                CU(cudaMemcpy(r.history, b->d_hist + (size_t)s * b->hist_cap, sizeof(double) * n, cudaMemcpyDeviceToHost));
+                r.history_len = n;
+            }
+        }
+    }
+    if (budget_hit) return set_error(CDFT_E_BUDGET, "time budget of %.3f s exhausted", opts->time_budget_s);
+    return 0;
+}
+
+int self_batch(cdft_plan* p, Batch** b)
+{
+    std::vector<cdft_plan*> v{p};
+    int rc = get_batch(v, b);
+    if (rc) return rc;
+    return batch_upload_sys(*b);
+}
+
+int functional_derivative(cdft_plan* p, const double* rho, double* out, bool is_dev)
+{
+    if (!p || !rho || !out) return set_error(CDFT_E_INVALID, "NULL argument");
+    CU(cudaSetDevice(p->device));
+    Batch* b = nullptr;
+    int rc = self_batch(p, &b);
+    if (rc) return rc;
+    const size_t bytes = (size_t)p->sys.n_elem * sizeof(double);
+    CU(cudaMemcpyAsync(p->sys.rho, rho, bytes, is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, p->stream));
+    rc = p->sys.mixed ? launch_eval_stages<float>(b, nullptr, true) : launch_eval_stages<double>(b, nullptr, true);
+    if (rc) return rc;
+    if (p->sys.mixed)
+        dfdrho_out_kernel<float><<<b->nechunks, ELEM_THREADS, 0, p->stream>>>(b->d_echunks, b->d_sys);
+    else
+        dfdrho_out_kernel<double><<<b->nechunks, ELEM_THREADS, 0, p->stream>>>(b->d_echunks, b->d_sys);
+    CHECK_LAUNCH();
+    g_launches += 1;
+    CU(cudaMemcpyAsync(out, p->sys.out, bytes, is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, p->stream));
+    CU(cudaStreamSynchronize(p->stream));
+    return 0;
+}
+
+// compensated (Neumaier) sum
+struct KSum {
+    double s = 0, c = 0;
+    void add(double x)
+    {
+        const double t = s + x;
+        if (std::fabs(s) >= std::fabs(x)) c += (s - t) + x;
+        else c += (x - t) + s;
+        s = t;
+    }
+    double value() const { return s + c; }
+};
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int cdft_plan_create(const cdft_system_desc* desc, cdft_plan** plan)
+{
+    g_err_code = 0;
+    if (!plan) return set_error(CDFT_E_INVALID, "plan output pointer is NULL");
+    *plan = nullptr;
+    int rc = validate_desc(desc);
+    if (rc) return rc;
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    rc = upload_constants();
+    if (rc) return rc;
+    cdft_plan* p = new cdft_plan();
+    p->device = dev;
+    p->desc = *desc;
+    p->desc.vext = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete p;
+        return set_error(CDFT_E_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    }
+    cdft_system_desc tmp = *desc;
+    p->desc = tmp;
+    rc = plan_build(p);
+    p->desc.vext = nullptr;
+    if (rc) {
+        plan_free(p);
+        delete p;
+        return rc;
+    }
+    *plan = p;
+    return 0;
+}
+
+int cdft_plan_destroy(cdft_plan* plan)
+{
+    if (!plan) return 0;
+    cudaSetDevice(plan->device);
+    drop_batches_of(plan);
+    plan_free(plan);
+    delete plan;
+    return 0;
+}
+
+int cdft_functional_derivative(cdft_plan* plan, const double* rho, double* dFdrho)
+{
+    g_err_code = 0;
+    return functional_derivative(plan, rho, dFdrho, false);
+}
+
+int cdft_functional_derivative_dev(cdft_plan* plan, const double* d_rho, double* d_dFdrho)
+{
+    g_err_code = 0;
+    return functional_derivative(plan, d_rho, d_dFdrho, true);
+}
+
+int cdft_free_energy_res(cdft_plan* plan, const double* rho, double* F)
+{
+    g_err_code = 0;
+    if (!plan || !rho || !F) return set_error(CDFT_E_INVALID, "NULL argument");
+    CU(cudaSetDevice(plan->device));
+    Batch* b = nullptr;
+    int rc = self_batch(plan, &b);
+    if (rc) return rc;
+    const size_t bytes = (size_t)plan->sys.n_elem * sizeof(double);
+    CU(cudaMemcpyAsync(plan->sys.rho, rho, bytes, cudaMemcpyHostToDevice, plan->stream));
+    rc = plan->sys.mixed ? launch_eval_stages<float>(b, nullptr, false) : launch_eval_stages<double>(b, nullptr, false);
+    if (rc) return rc;
+    std::vector<double> f(plan->N);
+    CU(cudaMemcpyAsync(f.data(), plan->sys.fval, sizeof(double) * plan->N, cudaMemcpyDeviceToHost, plan->stream));
+    CU(cudaStreamSynchronize(plan->stream));
+    // Simpson coefficients of _∫ (integrals.jl:28-41): 1, 4, 2, 4, ..., 1 times dz/3
+    const int N = plan->N;
+    KSum acc;
+    for (int k = 1; k <= N; ++k) {
+        const double c = (k == 1 || k == N) ? 1.0 : ((k % 2 == 0) ? 4.0 : 2.0);
+        acc.add(c * f[k - 1]);
+    }
+    const double L = plan->desc.L;
+    *F = acc.value() * (plan->dz[0] / 3.0) / (L * L * L);
+    return 0;
+}
+
+int cdft_phi_pointwise(cdft_plan* plan, const double* n, int npts, double* fval, double* dphi)
+{
+    g_err_code = 0;
+    if (!plan || !n || !fval || !dphi || npts <= 0) return set_error(CDFT_E_INVALID, "invalid argument");
+    CU(cudaSetDevice(plan->device));
+    const int nc = plan->desc.nc, NF = plan->sys.NF;
+    const size_t nin = (size_t)npts * NF * nc;
+    double *d_n = nullptr, *d_f = nullptr, *d_g = nullptr;
+    CU(cudaMalloc(&d_n, nin * sizeof(double)));
+    CU(cudaMalloc(&d_f, (size_t)npts * sizeof(double)));
+    CU(cudaMalloc(&d_g, nin * sizeof(double)));
+    CU(cudaMemcpyAsync(d_n, n, nin * sizeof(double), cudaMemcpyHostToDevice, plan->stream));
+    const int blocks = (npts + 127) / 128;
+    const PhiParams& P = plan->sys.phi;
+    int rc = 0;
+    if (plan->desc.nd == 1) {
+        switch (nc) {
+        case 1: phi_points_kernel<1, 1><<<blocks, 128, 0, plan->stream>>>(P, d_n, npts, d_f, d_g); break;
+        case 2: phi_points_kernel<2, 1><<<blocks, 128, 0, plan->stream>>>(P, d_n, npts, d_f, d_g); break;
+        case 3: phi_points_kernel<3, 1><<<blocks, 128, 0, plan->stream>>>(P, d_n, npts, d_f, d_g); break;
+        case 4: phi_points_kernel<4, 1><<<blocks, 128, 0, plan->stream>>>(P, d_n, npts, d_f, d_g); break;
+        default: rc = set_error(CDFT_E_UNSUPPORTED, "nc");
+        }
+    } else {
+        rc = set_error(CDFT_E_UNSUPPORTED, "nd");
+    }
+    g_launches += 1;
+    cudaError_t e = cudaGetLastError();
+    if (!rc && e != cudaSuccess) rc = set_error(CDFT_E_CUDA, "phi_points_kernel: %s", cudaGetErrorString(e));
+    if (!rc) {
+        cudaMemcpyAsync(fval, d_f, (size_t)npts * sizeof(double), cudaMemcpyDeviceToHost, plan->stream);
+        cudaMemcpyAsync(dphi, d_g, nin * sizeof(double), cudaMemcpyDeviceToHost, plan->stream);
+        e = cudaStreamSynchronize(plan->stream);
+        if (e != cudaSuccess) rc = set_error(CDFT_E_CUDA, "phi_pointwise: %s", cudaGetErrorString(e));
+    }
+    cudaFree(d_n);
+    cudaFree(d_f);
+    cudaFree(d_g);
+    return rc;
+}
+
+int cdft_converge(cdft_plan* plan, double* rho_inout, const cdft_solver_opts* opts, cdft_result* result)
+{
+    g_err_code = 0;
+    std::vector<cdft_plan*> v{plan};
+    double* r[1] = {rho_inout};
+    return batch_converge(v, r, false, opts, result);
+}
+
+int cdft_converge_dev(cdft_plan* plan, double* d_rho_inout, const cdft_solver_opts* opts, cdft_result* result)
+{
+    g_err_code = 0;
+    std::vector<cdft_plan*> v{plan};
+    double* r[1] = {d_rho_inout};
+    return batch_converge(v, r, true, opts, result);
+}
+
+int cdft_batch_converge(cdft_plan* const* plans, int nplans, double* const* rho_inout,
+                        const cdft_solver_opts* opts, cdft_result* results)
+{
+    g_err_code = 0;
+    if (!plans || nplans <= 0) return set_error(CDFT_E_INVALID, "no plans");
+    std::vector<cdft_plan*> v(plans, plans + nplans);
+    return batch_converge(v, rho_inout, false, opts, results);
+}
+
+int cdft_batch_converge_dev(cdft_plan* const* plans, int nplans, double* const* d_rho_inout,
+                            const cdft_solver_opts* opts, cdft_result* results)
+{
+    g_err_code = 0;
+    if (!plans || nplans <= 0) return set_error(CDFT_E_INVALID, "no plans");
+    std::vector<cdft_plan*> v(plans, plans + nplans);
+    return batch_converge(v, d_rho_inout, true, opts, results);
+}
+
+long long cdft_launch_count(int reset)
+{
+    const long long v = g_launches;
+    if (reset) g_launches = 0;
+    return v;
+}
+
+int cdft_last_error(char* buf, size_t len)
+{
+    if (buf && len) {
+        strncpy(buf, g_err_msg, len - 1);
+        buf[len - 1] = 0;
+    }
+    return g_err_code;
+}
+
+const char* cdft_version(void) { return "cdft_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

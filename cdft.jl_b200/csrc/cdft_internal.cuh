@@ -1,0 +1,108 @@
+// Internal device/host structures of libcdft_b200.
+//
+// Memory model: every system (one DFTSystem of the reference) owns contiguous
+// device buffers; a "batch" is a device array of SysDev records plus task and
+// chunk lists, so every kernel launch covers all systems of the batch.
+// Vectors follow the reference's Julia layout (grid fastest, then field,
+// then component): element e = i*N + j of component i at grid point j.
+#pragma once
+#include <cstdint>
+#include "../../include/cdft_b200.h"
+
+#define CDFT_NF_MAX 9          // 6 + nd fields, nd <= 3
+#define CDFT_NCONV_MAX 8       // NF - 1 convolved fields
+
+// 1D circulant convolution tiling (see conv1d_kernel)
+#define CONV_R 4               // outputs per thread (strided by 32)
+#define CONV_WARPS 4
+#define CONV_TILE (CONV_WARPS * 32 * CONV_R)   // outputs per block
+#define CONV_QC 1024           // taps per block (split-K chunk)
+
+// vector (Anderson) chunking
+#define ELEM_CHUNK 1024        // elements per block of the vector kernels
+#define ELEM_THREADS 256
+#define POINT_THREADS 128      // points per block of the pointwise Phi kernel
+#define RED_SLOTS (CDFT_MAX_M + 2)   // partial sums per chunk
+
+// solver modes (the phase of aasol a system is in when its next G evaluation runs)
+enum { MODE_EVAL_INIT = 0, MODE_EVAL_PICARD = 1, MODE_EVAL_AA = 2, MODE_DONE = 3 };
+
+// vector-slot operations between two fixed-point evaluations (see ctl_kernel)
+enum {
+    OP_NONE = 0,
+    OP_NORM_DF = 1,        // partial ||df||^2
+    OP_DOT_H1 = 2,         // [Q <- Q*Qx if downdate]; partial Q^T df
+    OP_SUB_DOT = 3,        // df -= Q h1; partial Q^T df
+    OP_SUB_NORM = 4,       // df -= Q h2; partial ||df||^2
+    OP_SETQ_DOT_TRES = 5,  // Q[:,kq] = df / r; partial Q[:, :mk]^T res
+    OP_SOL_AA = 6,         // sol = gx - DG theta; rho = exp(sol)
+    OP_SOL_COPY = 7        // sol = gx; rho = exp(sol)
+};
+#define N_VEC_SLOTS 5
+
+struct PhiParams {
+    int nc, nd;
+    double T;
+    double m[CDFT_MAX_NC];
+    double d[CDFT_MAX_NC];                       // reduced hard-sphere diameters d_i / L
+    double c1[CDFT_MAX_NC * CDFT_MAX_NC];        // m_i m_j (sigma_ij/L)^3 eps_ij/T
+    double c2[CDFT_MAX_NC * CDFT_MAX_NC];        // c1 * eps_ij/T
+    int has_assoc, a_ic, a_jc;
+    double a_nia, a_njb, a_dij, a_K;             // d_ij (reduced) and (sigma_ij/L)^3 (exp(eps/T)-1) kappa
+};
+
+struct SysDev {
+    int nd, N, nc, NF, nconv;
+    int ngrid[3];
+    int ksplit;                  // split-K factor of the 1D circulant convolutions
+    int n_elem;                  // N * nc
+    int mixed;                   // 1: FP32 convolution/Phi buffers
+    int chunk_begin, chunk_count;  // element chunks of this system (reductions)
+    double NA;                   // N_A L^3
+    double cprd[CDFT_MAX_NC];    // mu_res + ln rho_bulk
+    PhiParams phi;
+    // tables
+    const double* taps_eval;     // [(i*nconv+f)*N + q], scaled by N_A L^3
+    const double* taps_int;      // [(i*nconv+f)*N + q], sign of the adjoint folded in
+    const float* taps_eval32;
+    const float* taps_int32;
+    const double* vext;          // [e] or nullptr
+    // work buffers
+    double* rho;                 // exp(sol)
+    double* sol;
+    double* gx;
+    double* res;
+    double* df;
+    double* Q;                   // [c*n_elem + e]
+    double* DG;                  // [slot*n_elem + e]
+    void* part;                  // convolution partials [((i*nconv+f)*ksplit+ks)*N + j] (double or float)
+    void* dfield;                // dPhi/dn [(i*NF+a)*N + j] (double or float)
+    double* fval;                // Phi per point
+    double* out;                 // scratch output (functional derivative)
+};
+
+struct AAState {
+    int mode, k, picard_it, nevals;
+    int errcode, idid, toosoon, m;
+    int maxit, picard_maxit;
+    int head, dg_slot, kq, mk;
+    int downdate, pad0;
+    int op[N_VEC_SLOTS + 1];
+    double beta, picard_beta, rtol, atol, picard_rtol, picard_atol;
+    double resnorm, tol, picard_tol, up_bd;
+    double rnorm;                // norm of the vector being orthonormalised
+    double coef[CDFT_MAX_M];     // coefficients of the current slot op
+    double h1[CDFT_MAX_M];
+    double R[CDFT_MAX_M * CDFT_MAX_M];     // column-major m x m
+    double Qx[CDFT_MAX_M * CDFT_MAX_M];    // column-major m x (m-1)
+    double* history;
+    int history_cap, pad1;
+};
+
+struct ConvTask {
+    int sys, comp, field, tile_ks;   // tile_ks = tile * ksplit + ks
+};
+
+struct Chunk {
+    int sys, begin;
+};

@@ -1,0 +1,312 @@
+// Fused pointwise PC-SAFT free-energy density Phi(n) and its gradient dPhi/dn.
+//
+// Restates f_res (src/models/DFT/SAFT/PCSAFT/PCSAFT.jl:110-117):
+//   f_hs   White-Bear FMT            src/models/DFT/FMT.jl:17-46
+//   f_hc   Sauer-Gross chain          PCSAFT.jl:123-144
+//   f_disp weighted dispersion        PCSAFT.jl:150-211
+//   f_assoc one-pair analytic Wertheim  src/models/DFT/assoc.jl:159-168,702-769
+// The reference differentiates f_res with Enzyme (models.jl:355-411, NF*nc
+// forward passes by default).  Here the gradient is a hand-written reverse
+// sweep computed in the same pass as Phi: one evaluation per point gives all
+// NF*nc partial derivatives.
+//
+// Field order (get_fields, PCSAFT.jl:47-62): 0 rho, 1 int rho dz (d/2),
+// 2 int rho z^2 dz (d/2), 3..3+nd-1 vector int rho z dz (d/2), 3+nd
+// int rho z^2 dz (d), 4+nd int rho dz (d), 5+nd int rho z^2 dz (psi d).
+#pragma once
+#include "cdft_internal.cuh"
+
+__constant__ double c_pcsaft_a[21];   // Gross & Sadowski (2001) a_0i, a_1i, a_2i, i = 0..6
+__constant__ double c_pcsaft_b[21];   // b_0i, b_1i, b_2i
+
+#define PSI_DISP 1.3862   // PCSAFT.jl:53
+
+template <typename T>
+__device__ __forceinline__ T fabs_t(T x) { return x < T(0) ? -x : x; }
+
+// log|x| evaluated in double (the near-close-packing log(1 - n3) and the
+// association logs stay FP64 in the mixed mode).
+__device__ __forceinline__ double logabs64(double x) { return log(fabs(x)); }
+
+template <typename T, int NC, int ND>
+__device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + ND], T (&g)[NC][6 + ND])
+{
+    constexpr int NF = 6 + ND;
+    constexpr int F2 = 1, F3 = 2, FV = 3, IHC = 3 + ND, ILAM = 4 + ND, IDISP = 5 + ND;
+    const T pi = T(3.14159265358979323846);
+    const T two_pi = T(2.0) * pi;
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+        for (int a = 0; a < NF; ++a) g[i][a] = T(0);
+
+    // ---------------- hard sphere (FMT.jl:17-46) ----------------
+    T n0 = 0, n1 = 0, n2 = 0, n3 = 0;
+    T nv1[ND], nv2[ND];
+#pragma unroll
+    for (int k = 0; k < ND; ++k) { nv1[k] = 0; nv2[k] = 0; }
+#pragma unroll
+    for (int i = 0; i < NC; ++i) {
+        const T mi = T(P.m[i]), di = T(P.d[i]);
+        const T nim = n[i][F2] * mi;
+        n0 += nim / di;
+        n1 += T(0.5) * nim;
+        n2 += pi * nim * di;
+#pragma unroll
+        for (int k = 0; k < ND; ++k) {
+            const T nvi = n[i][FV + k];
+            nv1[k] += nvi * mi / di;
+            nv2[k] -= two_pi * nvi * mi;
+        }
+        n3 += n[i][F3] * mi;
+    }
+    T nv1v2 = 0, nv2sq = 0;
+#pragma unroll
+    for (int k = 0; k < ND; ++k) { nv1v2 += nv1[k] * nv2[k]; nv2sq += nv2[k] * nv2[k]; }
+    // log(1 - n3) and the White-Bear bracket in FP64
+    const double n3d = double(n3);
+    const double Dd = 1.0 - n3d;
+    const double Lg = logabs64(Dd);
+    const double invD = 1.0 / Dd;
+    const double c12 = 12.0 * 3.14159265358979323846;
+    const double Bd = Lg / (c12 * n3d * n3d) + 1.0 / (c12 * n3d * Dd * Dd);
+    const double dBd = -invD / (c12 * n3d * n3d) - 2.0 * Lg / (c12 * n3d * n3d * n3d)
+                       - 1.0 / (c12 * n3d * n3d * Dd * Dd) + 2.0 / (c12 * n3d * Dd * Dd * Dd);
+    const T A3 = n2 * n2 * n2 / T(3) - n2 * nv2sq;
+    const T A2 = n1 * n2 - nv1v2;
+    T phi = T(-double(n0) * Lg) + A2 * T(invD) + A3 * T(Bd);
+    {
+        const T g_n0 = T(-Lg);
+        const T g_n1 = n2 * T(invD);
+        const T g_n2 = n1 * T(invD) + (n2 * n2 - nv2sq) * T(Bd);
+        const T g_n3 = T(double(n0) * invD + double(A2) * invD * invD + double(A3) * dBd);
+        T g_nv1[ND], g_nv2[ND];
+#pragma unroll
+        for (int k = 0; k < ND; ++k) {
+            g_nv1[k] = -nv2[k] * T(invD);
+            g_nv2[k] = -nv1[k] * T(invD) - T(2) * n2 * nv2[k] * T(Bd);
+        }
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            const T mi = T(P.m[i]), di = T(P.d[i]);
+            g[i][F2] += mi * (g_n0 / di + T(0.5) * g_n1 + pi * di * g_n2);
+            g[i][F3] += mi * g_n3;
+#pragma unroll
+            for (int k = 0; k < ND; ++k) g[i][FV + k] += mi * (g_nv1[k] / di - two_pi * g_nv2[k]);
+        }
+    }
+
+    // ---------------- hard chain (PCSAFT.jl:123-144) ----------------
+    {
+        T z3 = 0, z2 = 0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            z3 += T(P.m[i]) * n[i][IHC];
+            z2 += T(P.m[i]) * n[i][IHC] / T(P.d[i]);
+        }
+        z3 /= T(8);
+        z2 /= T(8);
+        const T I = T(1) / (T(1) - z3);
+        const T I2 = I * I, I3 = I2 * I, I4 = I3 * I;
+        T gz3 = 0, gz2 = 0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            const T am1 = T(P.m[i]) - T(1);
+            if (am1 == T(0)) continue;   // exact zero contribution (m_i = 1)
+            const T di = T(P.d[i]);
+            const T rho = n[i][0];
+            const T lam = n[i][ILAM] / (T(2) * di);
+            const T y = I + T(1.5) * di * z2 * I2 + T(0.5) * di * di * z2 * z2 * I3;
+            const T lg = T(log(fabs(double(y * lam / rho))));
+            phi -= rho * am1 * lg;
+            g[i][0] += -am1 * (lg - T(1));
+            g[i][ILAM] += -rho * am1 / n[i][ILAM];
+            const T gy = -rho * am1 / y;
+            gz3 += gy * (I2 + T(3) * di * z2 * I3 + T(1.5) * di * di * z2 * z2 * I4);
+            gz2 += gy * (T(1.5) * di * I2 + di * di * z2 * I3);
+        }
+#pragma unroll
+        for (int i = 0; i < NC; ++i) g[i][IHC] += T(P.m[i]) / T(8) * (gz3 + gz2 / T(P.d[i]));
+    }
+
+    // ---------------- dispersion (PCSAFT.jl:150-211) ----------------
+    {
+        const T psi = T(PSI_DISP);
+        const T factor = T(3) / (T(4) * psi * psi * psi * pi);
+        T r[NC];
+        T S = 0, M = 0, eta = 0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            const T di = T(P.d[i]);
+            const T d3 = di * di * di;
+            r[i] = n[i][IDISP] * factor / d3;
+            S += r[i];
+            M += r[i] * T(P.m[i]);
+            eta += T(P.m[i]) * r[i] * d3;
+        }
+        const T mbar = M / S;
+        eta = eta * pi / T(6);
+        T s1 = 0, s2 = 0;
+        T rc1[NC], rc2[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            rc1[i] = 0; rc2[i] = 0;
+#pragma unroll
+            for (int j = 0; j < NC; ++j) {
+                rc1[i] += r[j] * T(P.c1[i * CDFT_MAX_NC + j]);
+                rc2[i] += r[j] * T(P.c2[i * CDFT_MAX_NC + j]);
+            }
+            s1 += r[i] * rc1[i];
+            s2 += r[i] * rc2[i];
+        }
+        const T e2 = eta * eta;
+        const T om = T(1) - eta;
+        const T om2 = om * om;
+        const T om4 = om2 * om2;
+        const T iv1 = T(1) / om;
+        const T iv2 = T(1) / (T(2) - eta);
+        const T Pp = (T(8) * eta - T(2) * e2) / om4;
+        const T Qn = T(20) * eta - T(27) * e2 + T(12) * (eta * e2) - T(2) * (e2 * e2);
+        const T Qq = Qn * iv1 * iv1 * iv2 * iv2;
+        const T C1 = T(1) + mbar * Pp + (T(1) - mbar) * Qq;
+        const T c1m = (mbar - T(1)) / mbar;
+        const T c2m = c1m * (mbar - T(2)) / mbar;
+        const T dc1 = T(1) / (mbar * mbar);
+        const T dc2 = (T(3) * mbar - T(4)) / (mbar * mbar * mbar);
+        // Horner for I1, I2 and their derivatives in eta and mbar
+        T I1 = 0, I2 = 0, dI1e = 0, dI2e = 0, dI1m = 0, dI2m = 0;
+#pragma unroll
+        for (int k = 6; k >= 0; --k) {
+            const T a = T(c_pcsaft_a[3 * k]) + c1m * T(c_pcsaft_a[3 * k + 1]) + c2m * T(c_pcsaft_a[3 * k + 2]);
+            const T b = T(c_pcsaft_b[3 * k]) + c1m * T(c_pcsaft_b[3 * k + 1]) + c2m * T(c_pcsaft_b[3 * k + 2]);
+            const T am = dc1 * T(c_pcsaft_a[3 * k + 1]) + dc2 * T(c_pcsaft_a[3 * k + 2]);
+            const T bm = dc1 * T(c_pcsaft_b[3 * k + 1]) + dc2 * T(c_pcsaft_b[3 * k + 2]);
+            dI1e = dI1e * eta + I1;
+            dI2e = dI2e * eta + I2;
+            I1 = I1 * eta + a;
+            I2 = I2 * eta + b;
+            dI1m = dI1m * eta + am;
+            dI2m = dI2m * eta + bm;
+        }
+        phi += -T(2) * (pi * I1 * s1) - pi * mbar * I2 * s2 / C1;
+        const T g_s1 = -T(2) * pi * I1;
+        const T g_s2 = -pi * mbar * I2 / C1;
+        const T g_I1 = -T(2) * pi * s1;
+        const T g_I2 = -pi * mbar * s2 / C1;
+        const T g_C1 = pi * mbar * I2 * s2 / (C1 * C1);
+        const T dP = (T(8) - T(4) * eta) / om4 + T(4) * (T(8) * eta - T(2) * e2) / (om4 * om);
+        const T dQn = T(20) - T(54) * eta + T(36) * e2 - T(8) * eta * e2;
+        const T Qd = om2 * (T(2) - eta) * (T(2) - eta);
+        const T dQd = -T(2) * om * (T(2) - eta) * (T(3) - T(2) * eta);
+        const T dQ = (dQn * Qd - Qn * dQd) / (Qd * Qd);
+        const T g_m = -pi * I2 * s2 / C1 + g_C1 * (Pp - Qq) + g_I1 * dI1m + g_I2 * dI2m;
+        const T g_e = g_C1 * (mbar * dP + (T(1) - mbar) * dQ) + g_I1 * dI1e + g_I2 * dI2e;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            const T di = T(P.d[i]);
+            const T d3 = di * di * di;
+            const T gr = g_m * (T(P.m[i]) - mbar) / S + g_e * pi / T(6) * T(P.m[i]) * d3
+                         + g_s1 * T(2) * rc1[i] + g_s2 * T(2) * rc2[i];
+            g[i][IDISP] += gr * factor / d3;
+        }
+    }
+
+    // ---------------- association, one pair (assoc.jl:702-769), FP64 ----------------
+    if (P.has_assoc) {
+        const double PI = 3.14159265358979323846, TWO_PI = 2.0 * PI;
+        double n2m = 0, n3m = 0, nv2m[ND];
+#pragma unroll
+        for (int k = 0; k < ND; ++k) nv2m[k] = 0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            n2m += PI * double(n[i][F2]) * P.m[i] * P.d[i];
+            n3m += double(n[i][F3]) * P.m[i];
+#pragma unroll
+            for (int k = 0; k < ND; ++k) nv2m[k] -= TWO_PI * double(n[i][FV + k]) * P.m[i];
+        }
+        double nv2sqm = 0;
+#pragma unroll
+        for (int k = 0; k < ND; ++k) nv2sqm += nv2m[k] * nv2m[k];
+        const double xim = 1.0 - nv2sqm / (n2m * n2m);
+        const double dij = P.a_dij;
+        const double I = 1.0 / (1.0 - n3m);
+        const double ghs = I + 0.5 * dij * xim * n2m * I * I + dij * dij * n2m * n2m * xim * (I * I * I) / 18.0;
+        const double Delta = ghs * P.a_K;
+        const int ic = P.a_ic, jc = P.a_jc;
+        double n0c[2], n2c[2], sqc[2], xic[2], uc[2];
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const int c = s == 0 ? ic : jc;
+            double nc_f2 = 0, vv[ND];
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                if (i == c) {
+                    nc_f2 = double(n[i][F2]);
+#pragma unroll
+                    for (int k = 0; k < ND; ++k) vv[k] = double(n[i][FV + k]);
+                }
+            n0c[s] = nc_f2 / P.d[c];
+            n2c[s] = PI * nc_f2 * P.d[c];
+            double sq = 0;
+#pragma unroll
+            for (int k = 0; k < ND; ++k) { const double t = -TWO_PI * vv[k]; sq += t * t; }
+            sqc[s] = sq;
+            xic[s] = 1.0 - sq / (n2c[s] * n2c[s]);
+            uc[s] = n0c[s] * xic[s];
+        }
+        const double nia = P.a_nia, njb = P.a_njb;
+        const double kia = nia * uc[0] * Delta;
+        const double kjb = njb * uc[1] * Delta;
+        const double b = 1.0 - kia + kjb;
+        const double sr = sqrt(b * b + 4.0 * kia);
+        const double Xa = 2.0 / (b + sr);
+        const double Xb = 1.0 / (1.0 + kia * Xa);
+        const double phA = logabs64(Xa) - 0.5 * Xa + 0.5;
+        const double phB = logabs64(Xb) - 0.5 * Xb + 0.5;
+        phi += T(uc[0] * nia * phA + uc[1] * njb * phB);
+        // reverse sweep
+        const double gXa = nia * uc[0] * (1.0 / Xa - 0.5);
+        const double gXb = njb * uc[1] * (1.0 / Xb - 0.5);
+        const double bs2 = (b + sr) * (b + sr);
+        const double dXa_db = -2.0 / bs2 * (1.0 + b / sr);
+        const double dXa_dks = -4.0 / (bs2 * sr);
+        const double dXa_dkia = -dXa_db + dXa_dks;
+        const double dXa_dkjb = dXa_db;
+        const double dXb_dkia = -Xb * Xb * (Xa + kia * dXa_dkia);
+        const double dXb_dkjb = -Xb * Xb * kia * dXa_dkjb;
+        const double gkia = gXa * dXa_dkia + gXb * dXb_dkia;
+        const double gkjb = gXa * dXa_dkjb + gXb * dXb_dkjb;
+        const double gu[2] = {nia * phA + gkia * nia * Delta, njb * phB + gkjb * njb * Delta};
+        const double gDelta = gkia * nia * uc[0] + gkjb * njb * uc[1];
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const int c = s == 0 ? ic : jc;
+            const double g_n0 = gu[s] * xic[s];
+            const double g_xi = gu[s] * n0c[s];
+            const double g_n2 = g_xi * 2.0 * sqc[s] / (n2c[s] * n2c[s] * n2c[s]);
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                if (i == c) {
+                    g[i][F2] += T(g_n0 / P.d[c] + g_n2 * PI * P.d[c]);
+#pragma unroll
+                    for (int k = 0; k < ND; ++k)
+                        g[i][FV + k] += T(g_xi * (-2.0 * TWO_PI * TWO_PI * double(n[i][FV + k]) / (n2c[s] * n2c[s])));
+                }
+        }
+        const double gg = gDelta * P.a_K;
+        const double dg_dI = 1.0 + dij * xim * n2m * I + dij * dij * n2m * n2m * xim * I * I / 6.0;
+        const double dg_dn2 = 0.5 * dij * xim * I * I + dij * dij * n2m * xim * I * I * I / 9.0;
+        const double dg_dxi = 0.5 * dij * n2m * I * I + dij * dij * n2m * n2m * I * I * I / 18.0;
+        const double g_n2m = gg * (dg_dn2 + dg_dxi * 2.0 * nv2sqm / (n2m * n2m * n2m));
+        const double g_n3m = gg * dg_dI * I * I;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            g[i][F2] += T(g_n2m * PI * P.m[i] * P.d[i]);
+            g[i][F3] += T(g_n3m * P.m[i]);
+#pragma unroll
+            for (int k = 0; k < ND; ++k)
+                g[i][FV + k] += T(gg * dg_dxi * (-2.0 * nv2m[k] / (n2m * n2m)) * (-TWO_PI * P.m[i]));
+        }
+    }
+    return phi;
+}

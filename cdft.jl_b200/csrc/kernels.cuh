@@ -1,0 +1,675 @@
+// Device kernels of the converge! path (1D Cartesian engine).
+//
+// One fixed-point evaluation G(x) (GFix!, src/methods/converge.jl:235-242) is
+//   conv1d_kernel(stage 0)  weighted densities n_alpha  (evaluate_field!, fields.jl:26-48)
+//   phi_kernel              dPhi/dn_alpha, Phi          (δFδρ_res! AD stage, models.jl:145-179)
+//   conv1d_kernel(stage 1)  adjoint convolutions        (integrate_field!, fields.jl:50-61)
+//   el_kernel               ln G = mu - dF/drho - Vext, clamp, Anderson bookkeeping
+//                           (get_new_profile!, converge.jl:108-153; aa_point!/betafix!,
+//                            anderson.jl:470-491)
+// followed by up to five vector slots (vec_kernel) interleaved with one-warp
+// control kernels (ctl_kernel) that run aasol's state machine
+// (anderson.jl:301-443) and the QR update/downdate (anderson.jl:498-583).
+#pragma once
+#include "cdft_internal.cuh"
+#include "functional.cuh"
+
+__device__ __forceinline__ bool sys_active(const AAState* st, int s)
+{
+    return st == nullptr || st[s].mode != MODE_DONE;
+}
+
+// ---------------------------------------------------------------------------
+// Circulant convolution  out[j] = sum_q taps[q] * in[(j - q) mod N].
+//
+// taps are Re(IDFT(omega_hat)) of the reference's sampled kernel, so this is
+// the same linear operator as real(ifft(fft(in) .* omega_hat))
+// (convolve!, src/utils/integrals.jl:88-96), evaluated without transforms.
+// Block = (system, component, field, output tile, tap chunk).  Each lane owns
+// CONV_R outputs strided by 32 and walks its tap chunk in stride-32 order so
+// that the input window slides by one register per step: per step one
+// broadcast tap load, one conflict-free window load, CONV_R FMAs.
+// Tap chunks (split-K) write separate partial sums, reduced by the consumer.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T conv_in(const SysDev& S, int stage, int comp, int field, int j)
+{
+    if (stage == 0) return T(S.rho[comp * S.N + j]);
+    return reinterpret_cast<const T*>(S.dfield)[(comp * S.NF + field + 1) * S.N + j];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(CONV_WARPS * 32)
+conv1d_kernel(const ConvTask* __restrict__ tasks, const SysDev* __restrict__ sys,
+              const AAState* __restrict__ st, int stage)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* staps = reinterpret_cast<T*>(smem_raw);
+    T* swin = staps + CONV_QC;
+    const ConvTask tk = tasks[blockIdx.x];
+    if (!sys_active(st, tk.sys)) return;
+    const SysDev& S = sys[tk.sys];
+    const int N = S.N;
+    const int ks = tk.tile_ks % S.ksplit;
+    const int tile = tk.tile_ks / S.ksplit;
+    const int slot = tk.comp * S.nconv + tk.field;
+    const T* taps;
+    if (sizeof(T) == 8)
+        taps = reinterpret_cast<const T*>(stage == 0 ? S.taps_eval : S.taps_int);
+    else
+        taps = reinterpret_cast<const T*>(stage == 0 ? S.taps_eval32 : S.taps_int32);
+    taps += (size_t)slot * N;
+
+    const int q_lo = ks * CONV_QC;
+    const int q_hi = min(N, q_lo + CONV_QC);
+    const int QN = q_hi - q_lo;
+    const int j_lo = tile * CONV_TILE;
+    const int u_lo = j_lo - q_hi + 1 - 32;
+    const int u_n = CONV_TILE + QN - 1 + 32;
+    for (int t = threadIdx.x; t < QN; t += blockDim.x) staps[t] = taps[q_lo + t];
+    for (int t = threadIdx.x; t < u_n; t += blockDim.x) {
+        int u = u_lo + t;
+        int idx = ((u % N) + N) % N;
+        swin[t] = conv_in<T>(S, stage, tk.comp, tk.field, idx);
+    }
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wbase = j_lo + warp * 32 * CONV_R;
+    if (wbase >= N) return;   // no further barriers below
+    const int j0 = wbase + lane;
+    T acc[CONV_R];
+#pragma unroll
+    for (int r = 0; r < CONV_R; ++r) acc[r] = T(0);
+    const int q0_end = min(32, QN);
+    for (int q0 = 0; q0 < q0_end; ++q0) {
+        T W[CONV_R];
+#pragma unroll
+        for (int r = 0; r < CONV_R; ++r) W[r] = swin[j0 + 32 * r - (q_lo + q0) - u_lo];
+        for (int q = q0; q < QN; q += 32) {
+            const T tp = staps[q];
+#pragma unroll
+            for (int r = 0; r < CONV_R; ++r) acc[r] = fma(tp, W[r], acc[r]);
+#pragma unroll
+            for (int r = CONV_R - 1; r > 0; --r) W[r] = W[r - 1];
+            W[0] = swin[j0 - (q_lo + q) - 32 - u_lo];
+        }
+    }
+    T* out = reinterpret_cast<T*>(S.part) + ((size_t)slot * S.ksplit + ks) * N;
+#pragma unroll
+    for (int r = 0; r < CONV_R; ++r) {
+        const int j = j0 + 32 * r;
+        if (j < N) out[j] = acc[r];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused Phi / dPhi/dn at every grid point (one thread per point).
+// ---------------------------------------------------------------------------
+template <typename T, int NC, int ND>
+__device__ __forceinline__ void load_n(const SysDev& S, int j, T (&n)[NC][6 + ND])
+{
+    const T* part = reinterpret_cast<const T*>(S.part);
+#pragma unroll
+    for (int i = 0; i < NC; ++i) {
+        n[i][0] = T(S.NA * S.rho[i * S.N + j]);
+#pragma unroll
+        for (int f = 0; f < 5 + ND; ++f) {
+            const T* p = part + ((size_t)(i * S.nconv + f) * S.ksplit) * S.N + j;
+            T v = p[0];
+            for (int ks = 1; ks < S.ksplit; ++ks) v += p[(size_t)ks * S.N];
+            n[i][f + 1] = v;
+        }
+    }
+}
+
+template <typename T, int NC, int ND>
+__global__ void __launch_bounds__(POINT_THREADS)
+phi_kernel(const Chunk* __restrict__ pchunks, const SysDev* __restrict__ sys, const AAState* __restrict__ st)
+{
+    const Chunk c = pchunks[blockIdx.x];
+    if (!sys_active(st, c.sys)) return;
+    const SysDev& S = sys[c.sys];
+    const int j = c.begin + threadIdx.x;
+    if (j >= S.N) return;
+    T n[NC][6 + ND], g[NC][6 + ND];
+    load_n<T, NC, ND>(S, j, n);
+    const T f = phi_grad<T, NC, ND>(S.phi, n, g);
+    T* df = reinterpret_cast<T*>(S.dfield);
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+        for (int a = 0; a < 6 + ND; ++a) df[(i * (6 + ND) + a) * S.N + j] = g[i][a];
+    S.fval[j] = double(f);
+}
+
+// standalone pointwise evaluation (cdft_phi_pointwise): n, dphi are (npts, NF, nc) column-major
+template <int NC, int ND>
+__global__ void phi_points_kernel(PhiParams P, const double* __restrict__ n_in, int npts,
+                                  double* __restrict__ fval, double* __restrict__ dphi)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npts) return;
+    double n[NC][6 + ND], g[NC][6 + ND];
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+        for (int a = 0; a < 6 + ND; ++a) n[i][a] = n_in[(size_t)(i * (6 + ND) + a) * npts + p];
+    fval[p] = phi_grad<double, NC, ND>(P, n, g);
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+        for (int a = 0; a < 6 + ND; ++a) dphi[(size_t)(i * (6 + ND) + a) * npts + p] = g[i][a];
+}
+
+// ---------------------------------------------------------------------------
+// Block reduction of K partial sums (deterministic order).
+// ---------------------------------------------------------------------------
+template <int BLOCK>
+__device__ __forceinline__ void block_reduce_store(double* vals, int K, double* out)
+{
+    __shared__ double red[BLOCK / 32][RED_SLOTS];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int c = 0; c < K; ++c) {
+        double v = vals[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][c] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < BLOCK / 32; ++w) s += red[w][threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// dF/drho + Vext (standalone functional derivative).
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ double dfdrho_elem(const SysDev& S, int e)
+{
+    const int i = e / S.N, j = e - i * S.N;
+    const T* df = reinterpret_cast<const T*>(S.dfield);
+    const T* part = reinterpret_cast<const T*>(S.part);
+    double v = double(df[(i * S.NF) * S.N + j]);   // rho field: δfδρ_res .= profile
+    for (int f = 0; f < S.nconv; ++f) {
+        const T* p = part + ((size_t)(i * S.nconv + f) * S.ksplit) * S.N + j;
+        T acc = p[0];
+        for (int ks = 1; ks < S.ksplit; ++ks) acc += p[(size_t)ks * S.N];
+        v += double(acc);
+    }
+    if (S.vext) v += S.vext[e];
+    return v;
+}
+
+template <typename T>
+__global__ void dfdrho_out_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys)
+{
+    const Chunk c = echunks[blockIdx.x];
+    const SysDev& S = sys[c.sys];
+    for (int t = threadIdx.x; t < ELEM_CHUNK; t += blockDim.x) {
+        const int e = c.begin + t;
+        if (e < S.n_elem) S.out[e] = dfdrho_elem<T>(S, e);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Euler-Lagrange step + aa_point!/betafix! bookkeeping + ||res||^2 partials.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(ELEM_THREADS)
+el_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
+          const AAState* __restrict__ st, double* __restrict__ partials)
+{
+    const Chunk c = echunks[blockIdx.x];
+    if (!sys_active(st, c.sys)) return;
+    const SysDev& S = sys[c.sys];
+    const AAState& A = st[c.sys];
+    const int mode = A.mode;
+    const double beta = (mode == MODE_EVAL_PICARD) ? A.picard_beta : A.beta;
+    const bool aa = (mode == MODE_EVAL_AA);
+    double* DGs = (aa && A.m > 0) ? S.DG + (size_t)A.dg_slot * S.n_elem : nullptr;
+    double ss = 0.0;
+    for (int t = threadIdx.x; t < ELEM_CHUNK; t += ELEM_THREADS) {
+        const int e = c.begin + t;
+        if (e >= S.n_elem) break;
+        const int i = e / S.N;
+        const double dF = dfdrho_elem<T>(S, e);
+        double lnG = S.cprd[i] - dF;
+        lnG = fmin(fmax(lnG, -100.0), 100.0);             // clamp!(ln_Gx, -100, 100)
+        const double s = S.sol[e];
+        const double gxn = (beta == 1.0) ? lnG : (1.0 - beta) * s + beta * lnG;  // betafix!
+        const double rn = gxn - s;
+        if (aa) {
+            const double dgv = gxn - S.gx[e];
+            const double dfv = -S.res[e] + rn;
+            S.df[e] = dfv;
+            if (DGs) DGs[e] = dgv;
+        }
+        S.res[e] = rn;
+        S.gx[e] = gxn;
+        ss += rn * rn;
+    }
+    double v[1] = {ss};
+    block_reduce_store<ELEM_THREADS>(v, 1, partials + (size_t)blockIdx.x * RED_SLOTS);
+}
+
+// ---------------------------------------------------------------------------
+// Vector slot operations of the Anderson step (see OP_* in cdft_internal.cuh).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(ELEM_THREADS)
+vec_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
+           const AAState* __restrict__ st, double* __restrict__ partials, int slot)
+{
+    const Chunk c = echunks[blockIdx.x];
+    const AAState& A = st[c.sys];
+    const int op = A.op[slot];
+    if (op == OP_NONE) return;
+    const SysDev& S = sys[c.sys];
+    const int n = S.n_elem;
+    const int m = A.m;
+    double acc[RED_SLOTS];
+#pragma unroll
+    for (int k = 0; k < RED_SLOTS; ++k) acc[k] = 0.0;
+    int K = 0;
+    switch (op) {
+    case OP_NORM_DF: {
+        K = 1;
+        for (int t = threadIdx.x; t < ELEM_CHUNK; t += ELEM_THREADS) {
+            const int e = c.begin + t;
+            if (e >= n) break;
+            const double v = S.df[e];
+            acc[0] += v * v;
+        }
+        break;
+    }
+    case OP_DOT_H1: {
+        K = A.kq;
+        for (int t = threadIdx.x; t < ELEM_CHUNK; t += ELEM_THREADS) {
+            const int e = c.begin + t;
+            if (e >= n) break;
+            if (A.downdate) {   // Q[:, 1:m-1] = Q * Qx; Q[:, m] = 0  (downdate_aaqr!)
+                double row[CDFT_MAX_M];
+                for (int r = 0; r < m; ++r) row[r] = S.Q[(size_t)r * n + e];
+                for (int cc = 0; cc < m - 1; ++cc) {
+                    double v = 0.0;
+                    for (int r = 0; r < m; ++r) v += row[r] * A.Qx[r + cc * m];
+                    S.Q[(size_t)cc * n + e] = v;
+                }
+                S.Q[(size_t)(m - 1) * n + e] = 0.0;
+            }
+            const double dv = S.df[e];
+            for (int cc = 0; cc < K; ++cc) acc[cc] += S.Q[(size_t)cc * n + e] * dv;
+        }
+        break;
+    }
+    case OP_SUB_DOT:
+    case OP_SUB_NORM: {
+        const int kq = A.kq;
+        K = (op == OP_SUB_DOT) ? kq : 1;
+        for (int t = threadIdx.x; t < ELEM_CHUNK; t += ELEM_THREADS) {
+            const int e = c.begin + t;
+            if (e >= n) break;
+            double v = S.df[e];
+            for (int cc = 0; cc < kq; ++cc) v += (-A.coef[cc]) * S.Q[(size_t)cc * n + e];  // gemv, alpha=-1
+            S.df[e] = v;
+            if (op == OP_SUB_DOT) {
+                for (int cc = 0; cc < kq; ++cc) acc[cc] += S.Q[(size_t)cc * n + e] * v;
+            } else {
+                acc[0] += v * v;
+            }
+        }
+        break;
+    }
+    case OP_SETQ_DOT_TRES: {
+        const int kq = A.kq;
+        K = A.mk;
+        const double r = A.rnorm;
+        for (int t = threadIdx.x; t < ELEM_CHUNK; t += ELEM_THREADS) {
+            const int e = c.begin + t;
+            if (e >= n) break;
+            const double q = S.df[e] / r;
+            S.Q[(size_t)kq * n + e] = q;
+            const double rv = S.res[e];
+            for (int cc = 0; cc < K; ++cc) acc[cc] += S.Q[(size_t)cc * n + e] * rv;
+        }
+        break;
+    }
+    case OP_SOL_AA: {
+        const int mk = A.mk;
+        for (int t = threadIdx.x; t < ELEM_CHUNK; t += ELEM_THREADS) {
+            const int e = c.begin + t;
+            if (e >= n) break;
+            double v = S.gx[e];
+            for (int cc = 0; cc < mk; ++cc) {
+                const int slotc = (A.head + cc) % m;
+                v += (-A.coef[cc]) * S.DG[(size_t)slotc * n + e];
+            }
+            S.sol[e] = v;
+            S.rho[e] = exp(v);
+        }
+        return;
+    }
+    case OP_SOL_COPY: {
+        for (int t = threadIdx.x; t < ELEM_CHUNK; t += ELEM_THREADS) {
+            const int e = c.begin + t;
+            if (e >= n) break;
+            const double v = S.gx[e];
+            S.sol[e] = v;
+            S.rho[e] = exp(v);
+        }
+        return;
+    }
+    default:
+        return;
+    }
+    block_reduce_store<ELEM_THREADS>(acc, K, partials + (size_t)blockIdx.x * RED_SLOTS);
+}
+
+// ---------------------------------------------------------------------------
+// Control: one warp per system.
+// ---------------------------------------------------------------------------
+__device__ void aa_finish(AAState& A, int* done_counter)
+{
+    // AndersonOK, anderson.jl:727-737
+    if (A.toosoon) { A.idid = 1; A.errcode = -1; }
+    else if (A.resnorm >= A.up_bd) { A.idid = 0; A.errcode = -2; }
+    else if (A.resnorm <= A.tol) { A.idid = 1; A.errcode = 0; }
+    else { A.idid = 0; A.errcode = 10; }
+    A.mode = MODE_DONE;
+    atomicAdd(done_counter, 1);
+}
+
+__device__ __forceinline__ int aa_next_dg_slot(const AAState& A)
+{
+    // BuildDG!(DG, m, k+1, dg), anderson.jl:450-461, as a ring: the next dg lands in
+    // the slot of the column that is dropped (the oldest) once the history is full.
+    if (A.m <= 1) return 0;
+    return (A.k > A.m) ? A.head : A.k - 1;
+}
+
+__device__ void aa_anderson_start(AAState& A)
+{
+    // copy!(sol, gx); k += 1; aa_point!  (anderson.jl:369-380)
+    A.op[1] = OP_SOL_COPY;
+    A.k = 1;
+    A.mode = MODE_EVAL_AA;
+    A.dg_slot = aa_next_dg_slot(A);
+}
+
+// Householder QR of R[:, 2:m] (m x (m-1)) with LAPACK dlarfg conventions;
+// downdate_aaqr!, anderson.jl:552-583.
+__device__ void aa_downdate(AAState& A)
+{
+    const int m = A.m, n = m - 1;
+    double Am[CDFT_MAX_M * CDFT_MAX_M];  // column-major m x n
+    for (int c = 0; c < n; ++c)
+        for (int r = 0; r < m; ++r) Am[r + c * m] = A.R[r + (c + 1) * m];
+    double tau[CDFT_MAX_M];
+    double V[CDFT_MAX_M * CDFT_MAX_M];
+    for (int j = 0; j < n; ++j) {
+        double alpha = Am[j + j * m];
+        double xn2 = 0.0;
+        for (int r = j + 1; r < m; ++r) xn2 += Am[r + j * m] * Am[r + j * m];
+        double xnorm = sqrt(xn2);
+        for (int r = 0; r < m; ++r) V[r + j * m] = 0.0;
+        V[j + j * m] = 1.0;
+        if (xnorm == 0.0) {
+            tau[j] = 0.0;
+        } else {
+            const double beta = -copysign(hypot(alpha, xnorm), alpha);
+            tau[j] = (beta - alpha) / beta;
+            const double sc = 1.0 / (alpha - beta);
+            for (int r = j + 1; r < m; ++r) V[r + j * m] = Am[r + j * m] * sc;
+            Am[j + j * m] = beta;
+            for (int r = j + 1; r < m; ++r) Am[r + j * m] = 0.0;
+            for (int c = j + 1; c < n; ++c) {
+                double w = 0.0;
+                for (int r = j; r < m; ++r) w += V[r + j * m] * Am[r + c * m];
+                for (int r = j; r < m; ++r) Am[r + c * m] -= tau[j] * V[r + j * m] * w;
+            }
+        }
+    }
+    // thin Q (m x n)
+    double Qm[CDFT_MAX_M * CDFT_MAX_M];
+    for (int c = 0; c < n; ++c)
+        for (int r = 0; r < m; ++r) Qm[r + c * m] = (r == c) ? 1.0 : 0.0;
+    for (int j = n - 1; j >= 0; --j) {
+        for (int c = 0; c < n; ++c) {
+            double w = 0.0;
+            for (int r = j; r < m; ++r) w += V[r + j * m] * Qm[r + c * m];
+            for (int r = j; r < m; ++r) Qm[r + c * m] -= tau[j] * V[r + j * m] * w;
+        }
+    }
+    for (int c = 0; c < n; ++c)
+        for (int r = 0; r < m; ++r) A.Qx[r + c * m] = Qm[r + c * m];
+    // R[1:m-1, 1:m-1] = Rd; R[:, m] = 0
+    for (int c = 0; c < n; ++c)
+        for (int r = 0; r < n; ++r) A.R[r + c * m] = (r <= c) ? Am[r + c * m] : 0.0;
+    for (int r = 0; r < m; ++r) A.R[r + (m - 1) * m] = 0.0;
+}
+
+__device__ void aa_after_eval(AAState& A, double r, int* done_counter)
+{
+    A.resnorm = r;
+    if (A.history && A.nevals < A.history_cap) A.history[A.nevals] = r;
+    A.nevals++;
+    for (int s = 1; s <= N_VEC_SLOTS; ++s) A.op[s] = OP_NONE;
+    switch (A.mode) {
+    case MODE_EVAL_INIT: {
+        A.up_bd = 1.0e4 * r;
+        A.tol = A.rtol * r + A.atol;
+        A.picard_tol = A.picard_rtol * r + A.picard_atol;
+        A.toosoon = (r <= A.tol);
+        if (A.toosoon) { aa_finish(A, done_counter); return; }
+        if (A.picard_maxit > 0) {
+            A.picard_it = 0;
+            if (A.picard_maxit - 1 > 0) {   // copy!(sol, gx); Picard loop
+                A.mode = MODE_EVAL_PICARD;
+                A.op[1] = OP_SOL_COPY;
+                return;
+            }
+        }
+        aa_anderson_start(A);
+        return;
+    }
+    case MODE_EVAL_PICARD: {
+        A.picard_it++;
+        if (r <= A.picard_tol || r >= A.up_bd) {   // break (sol keeps the previous iterate)
+            A.toosoon = (r <= A.tol);
+            if (A.toosoon) { aa_finish(A, done_counter); return; }
+            aa_anderson_start(A);
+            return;
+        }
+        // copy!(sol, gx)
+        A.op[1] = OP_SOL_COPY;
+        if (A.picard_it >= A.picard_maxit - 1) {   // loop exhausted
+            A.toosoon = (r <= A.tol);
+            if (A.toosoon) { aa_finish(A, done_counter); return; }   // pending copy still runs
+            aa_anderson_start(A);
+        }
+        return;
+    }
+    case MODE_EVAL_AA: {
+        if (!((A.k < A.maxit + A.picard_maxit) && (r > A.tol) && (r < A.up_bd))) {
+            aa_finish(A, done_counter);
+            return;
+        }
+        if (A.m == 0) {
+            A.op[1] = OP_SOL_COPY;
+            A.k++;
+            return;
+        }
+        if (A.m > 1 && A.k > A.m) A.head = (A.head + 1) % A.m;   // BuildDG! shift
+        const int kqr = A.k - 1;
+        A.mk = min(A.m, A.k);
+        if (kqr == 0 || A.m == 1) {
+            A.kq = 0;
+            A.downdate = 0;
+            A.op[1] = OP_NORM_DF;
+            return;
+        }
+        A.downdate = (kqr > A.m - 1) ? 1 : 0;
+        if (A.downdate) aa_downdate(A);
+        A.kq = min(kqr, A.m - 1);
+        A.op[1] = OP_DOT_H1;
+        return;
+    }
+    default:
+        return;
+    }
+}
+
+__global__ void ctl_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, const double* __restrict__ partials,
+                           int nsys, int slot_done, int* done_counter)
+{
+    const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp_global >= nsys) return;
+    const int s = warp_global;
+    AAState& A = st[s];
+    const SysDev& S = sys[s];
+    if (A.mode == MODE_DONE) {
+        if (slot_done == 0 && lane == 0)
+            for (int k = 1; k <= N_VEC_SLOTS; ++k) A.op[k] = OP_NONE;
+        return;
+    }
+    int op = (slot_done == 0) ? -1 : A.op[slot_done];
+    if (op == OP_NONE || op == OP_SOL_AA || op == OP_SOL_COPY) return;
+    int K;
+    switch (op) {
+    case -1: case OP_NORM_DF: case OP_SUB_NORM: K = 1; break;
+    case OP_DOT_H1: case OP_SUB_DOT: K = A.kq; break;
+    case OP_SETQ_DOT_TRES: K = A.mk; break;
+    default: K = 0;
+    }
+    double sums[RED_SLOTS];
+    for (int k = 0; k < RED_SLOTS; ++k) sums[k] = 0.0;
+    for (int ch = lane; ch < S.chunk_count; ch += 32) {
+        const double* p = partials + (size_t)(S.chunk_begin + ch) * RED_SLOTS;
+        for (int k = 0; k < K; ++k) sums[k] += p[k];
+    }
+    for (int k = 0; k < K; ++k) {
+        double v = sums[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        sums[k] = v;
+    }
+    if (lane != 0) return;
+    const int next = slot_done + 1;
+    switch (op) {
+    case -1:
+        aa_after_eval(A, sqrt(sums[0]), done_counter);
+        break;
+    case OP_NORM_DF: {   // k == 0 branch of aa_qr_update!: R[1,1] = norm(df)
+        const double r = sqrt(sums[0]);
+        A.R[0] = r;
+        A.rnorm = r;
+        A.kq = 0;
+        if (next <= N_VEC_SLOTS) A.op[next] = OP_SETQ_DOT_TRES;
+        break;
+    }
+    case OP_DOT_H1:
+        for (int k = 0; k < A.kq; ++k) { A.h1[k] = sums[k]; A.coef[k] = sums[k]; }
+        if (next <= N_VEC_SLOTS) A.op[next] = OP_SUB_DOT;
+        break;
+    case OP_SUB_DOT:
+        for (int k = 0; k < A.kq; ++k) {
+            A.R[k + A.kq * A.m] = A.h1[k] + sums[k];   // hv[1:k] = h1 + h2
+            A.coef[k] = sums[k];
+        }
+        if (next <= N_VEC_SLOTS) A.op[next] = OP_SUB_NORM;
+        break;
+    case OP_SUB_NORM: {
+        const double r = sqrt(sums[0]);
+        A.R[A.kq + A.kq * A.m] = r;
+        A.rnorm = r;
+        if (next <= N_VEC_SLOTS) A.op[next] = OP_SETQ_DOT_TRES;
+        break;
+    }
+    case OP_SETQ_DOT_TRES: {
+        // theta = R[1:mk,1:mk] \ tres (upper triangular back substitution)
+        const int mk = A.mk, m = A.m;
+        double th[CDFT_MAX_M];
+        for (int i = mk - 1; i >= 0; --i) {
+            double v = sums[i];
+            for (int j = i + 1; j < mk; ++j) v -= A.R[i + j * m] * th[j];
+            th[i] = v / A.R[i + i * m];
+        }
+        for (int i = 0; i < mk; ++i) A.coef[i] = th[i];
+        if (next <= N_VEC_SLOTS) A.op[next] = OP_SOL_AA;
+        A.k++;
+        A.mode = MODE_EVAL_AA;
+        A.dg_slot = aa_next_dg_slot(A);
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+// initial iterate: sol = log(rho0); rho = exp(sol)   (converge.jl:244, GFix! :236)
+__global__ void init_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys)
+{
+    const Chunk c = echunks[blockIdx.x];
+    const SysDev& S = sys[c.sys];
+    for (int t = threadIdx.x; t < ELEM_CHUNK; t += blockDim.x) {
+        const int e = c.begin + t;
+        if (e >= S.n_elem) break;
+        const double x = log(S.rho[e]);
+        S.sol[e] = x;
+        S.rho[e] = exp(x);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Circulant taps of the 1D kernels: t[q] = Re((1/N) sum_k Omega_k exp(2 pi i k q / N)).
+// Omega_k are the reference's closed forms (weighted_densities.jl:28-80,193-246)
+// sampled at the reduced FFT frequencies L * fftfreq(N, N/(ub-lb))
+// (structure_fftfreq/structure_ω, src/structure/structure.jl:153-185).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double kernel_hat_1d(int type, double w, double R, int vector_comp)
+{
+    // type: 1 int rho dz, 2 int rho z^2 dz, 3 vector int rho z dz (imaginary part returned)
+    const double PI = 3.14159265358979323846, TWO_PI = 2.0 * PI;
+    const double wb = fabs(w);
+    if (type == 1) return (wb == 0.0) ? 2.0 * R / TWO_PI : 2.0 * sin(wb * R) / wb / TWO_PI;
+    if (type == 2) {
+        if (wb == 0.0) return 4.0 * PI * R * R * R / 3.0 / (TWO_PI * TWO_PI * TWO_PI);
+        return 4.0 * PI / (wb * wb * wb) * (sin(wb * R) - R * wb * cos(wb * R)) / (TWO_PI * TWO_PI * TWO_PI);
+    }
+    if (wb == 0.0) return 4.0 * PI * R / (TWO_PI * TWO_PI * TWO_PI);
+    return 4.0 * PI * w / (wb * wb * wb) * (sin(wb * R) - R * wb * cos(wb * R)) / (TWO_PI * TWO_PI * TWO_PI);
+}
+
+__global__ void taps1d_kernel(int N, double span, double L, int type, double width_red,
+                              double scale_eval, double sign_int,
+                              double* __restrict__ taps_eval, double* __restrict__ taps_int)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= N) return;
+    const double R = 2.0 * 3.14159265358979323846 * width_red;
+    double acc = 0.0;
+    const int half = (N + 1) / 2;   // ceil(N/2)
+    for (int k = 0; k < N; ++k) {
+        const int kk = (k < half) ? k : k - N;
+        const double w = (double)kk / span * L;
+        const long long ph = ((long long)k * (long long)q) % N;
+        double sn, cs;
+        sincospi(2.0 * (double)ph / (double)N, &sn, &cs);
+        const double K = kernel_hat_1d(type, w, R, 0);
+        acc += (type == 3) ? -K * sn : K * cs;
+    }
+    const double t = acc / (double)N;
+    taps_eval[q] = t * scale_eval;
+    taps_int[q] = t * sign_int;
+}
+
+__global__ void to_float_kernel(const double* __restrict__ a, float* __restrict__ b, size_t n)
+{
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
+}

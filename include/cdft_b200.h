@@ -1,0 +1,172 @@
+/*
+ * cdft_b200.h -- C ABI of the B200 (sm_100a) implementation of cDFT.jl's
+ * converge! hot path for PC-SAFT weighted-density DFT.
+ *
+ * Every entry point replaces one call on the reference's Julia path
+ * (ClapeyronThermo/cDFT.jl); the replaced function is cited beside each
+ * declaration.  Julia reaches this library through ccall (see the shim
+ * cdft.jl_b200/julia/CDFTB200.jl); Python through ctypes.
+ *
+ * Conventions
+ *  - Host arrays are column-major with the grid fastest, exactly like the
+ *    reference's Julia arrays: a profile rho(ngrid..., nc) is stored as
+ *    rho[((i*Nz + z)*Ny + y)*Nx + x] for component i.
+ *  - Densities in mol/m^3, lengths in m, energies eps/k_B in K.
+ *  - Every call returns 0 on success or a negative CDFT_E* code; the message
+ *    of the last error of the calling thread is available from
+ *    cdft_last_error().  No exception or exit() crosses this boundary.
+ *  - A plan is bound to the CUDA device current at cdft_plan_create and to
+ *    one stream; it is not thread-safe.  Distinct plans may be used
+ *    concurrently from distinct host threads.
+ */
+#ifndef CDFT_B200_H
+#define CDFT_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CDFT_MAX_NC 4        /* components per system */
+#define CDFT_MAX_ASSOC 1     /* association pairs per system (one-pair analytic path) */
+#define CDFT_MAX_M 16        /* Anderson history depth */
+
+/* error codes */
+#define CDFT_OK 0
+#define CDFT_E_INVALID -1     /* invalid argument */
+#define CDFT_E_CUDA -2        /* CUDA runtime error */
+#define CDFT_E_UNSUPPORTED -3 /* valid request outside the implemented scope */
+#define CDFT_E_BUDGET -4      /* host wall-clock budget exhausted before the solver ended */
+#define CDFT_E_NOMEM -5
+
+/* coordinate systems (Structure{Dim,Coord}, src/base/structure.jl:116-130) */
+#define CDFT_COORD_CART 0
+#define CDFT_COORD_SPH 1
+#define CDFT_COORD_CYL 2
+
+/* arithmetic of the convolutions and of Phi (DFTOptions precision, src/base/devices.jl:29-40) */
+#define CDFT_PREC_FP64 0
+#define CDFT_PREC_MIXED 1    /* FP32 convolutions and Phi; FP64 Anderson, norms, integrals */
+
+/* One Wertheim association pair, as packed by pack_assoc_params
+ * (src/models/DFT/assoc.jl:18-56): site A on component icomp bonds with
+ * site B on component jcomp. */
+typedef struct {
+    int icomp, jcomp;          /* 0-based */
+    int n_ia, n_jb;            /* site multiplicities */
+    double eps_ab;             /* epsilon_assoc / k_B, K */
+    double kappa_ab;           /* bonding volume (dimensionless) */
+} cdft_assoc_pair;
+
+/* Everything the reference's DFTSystem (src/base/base.jl:50-73) carries into
+ * the hot path, as plain numbers: the structure, the PC-SAFT parameters, the
+ * species data of get_species (PCSAFT.jl:65-72) and the cached external
+ * potential of preallocate_external_potential (devices.jl:71-102). */
+typedef struct {
+    int nd;                          /* 1 or 3 */
+    int ngrid[3];                    /* points per dimension (unused entries ignored) */
+    double bounds[3][2];             /* [lb, ub] per dimension, m */
+    int coord;                       /* CDFT_COORD_* */
+    int nc;                          /* components (one bead each) */
+    double m[CDFT_MAX_NC];           /* segment numbers */
+    double hsd[CDFT_MAX_NC];         /* hard-sphere diameters d_i(T), m (species.size) */
+    double sigma[CDFT_MAX_NC * CDFT_MAX_NC]; /* sigma_ij, m, row-major nc x nc */
+    double eps[CDFT_MAX_NC * CDFT_MAX_NC];   /* eps_ij / k_B, K, row-major nc x nc */
+    double L;                        /* length scale, m (length_scale(model) = max sigma) */
+    double T;                        /* temperature, K */
+    int n_assoc;                     /* 0 or 1 */
+    cdft_assoc_pair assoc[CDFT_MAX_ASSOC];
+    double mu_res_plus_ln_rhob[CDFT_MAX_NC]; /* species.chempot_res + log(bulk_density), converge.jl:121 */
+    const double* vext;              /* external potential / k_B T, (ngrid..., nc); NULL = none */
+    int precision;                   /* CDFT_PREC_* */
+} cdft_system_desc;
+
+/* The AASol fields used by aasol (src/utils/anderson.jl:193-207).  The
+ * converge! keyword form maps onto it as __AASol does (converge.jl:3-9):
+ * rtol = atol = tol, picard_maxit = maxit, picard_beta = beta,
+ * picard_rtol = picard_atol = anderson_start. */
+typedef struct {
+    int m;                 /* Anderson depth, 0 <= m <= CDFT_MAX_M */
+    int maxit;
+    double rtol, atol, beta;
+    int picard_maxit;
+    double picard_beta, picard_rtol, picard_atol;
+    double time_budget_s;  /* host wall-clock cap for the whole call, <= 0: none */
+    int iters_per_launch;  /* fixed-point evaluations per CUDA-graph launch, <= 0: default */
+} cdft_solver_opts;
+
+/* The (idid, errcode, history) part of aasol's output (anderson.jl:81-103,727-757). */
+typedef struct {
+    int idid;              /* 1 converged, 0 not */
+    int errcode;           /* -1 initial iterate within tol, -2 divergence, 0 converged, 10 maxit */
+    int iterations;        /* Anderson counter k of aasol */
+    int evaluations;       /* fixed-point map evaluations */
+    double resnorm;        /* final ||beta (G(x) - x)||_2 */
+    double tol;            /* rtol * ||r0|| + atol */
+    double* history;       /* optional caller buffer for resnorm per evaluation, or NULL */
+    int history_cap;
+    int history_len;       /* entries written */
+} cdft_result;
+
+typedef struct cdft_plan cdft_plan;
+
+/* Build the device-side system: weighted-density kernels (get_fields,
+ * PCSAFT.jl:47-62; SWeightedDensity/VWeightedDensity, weighted_densities.jl:28-80,
+ * 193-246), reduced parameters (preallocate_params, PCSAFT.jl:213-285) and
+ * work buffers (preallocate / preallocate_model, devices.jl:51-68,
+ * models.jl:209-251). */
+int cdft_plan_create(const cdft_system_desc* desc, cdft_plan** plan);
+int cdft_plan_destroy(cdft_plan* plan);
+
+/* dF/drho for every component: residual functional derivative plus external
+ * field, in k_B T.  Replaces δFδρ_res(system, ρ), src/models/models.jl:194-200
+ * (δFδρ_res! :131-186 followed by evaluate_external_field!). */
+int cdft_functional_derivative(cdft_plan* plan, const double* rho, double* dFdrho);
+int cdft_functional_derivative_dev(cdft_plan* plan, const double* d_rho, double* d_dFdrho);
+
+/* Residual Helmholtz energy per unit area (1D) or total (3D) in units of k_B T
+ * (per m^2 in 1D).  Replaces F_res(system, ρ), src/models/models.jl:86-91
+ * (Simpson rule of src/utils/integrals.jl:17-41 on the device f_res values,
+ * compensated FP64 summation). */
+int cdft_free_energy_res(cdft_plan* plan, const double* rho, double* F);
+
+/* Pointwise fused Phi and dPhi/dn_alpha at npts points: n and dphi are
+ * (npts, NF, nc) column-major (point fastest), fval is (npts).  Replaces
+ * the Enzyme kernels δf_fwd_kernel!/δf_rev_kernel! (models.jl:355-411) that
+ * differentiate f_res (PCSAFT.jl:110-117). */
+int cdft_phi_pointwise(cdft_plan* plan, const double* n, int npts, double* fval, double* dphi);
+
+/* Converge rho in place.  Replaces converge!(prob::DFTProblem, method::AASol, ρ),
+ * src/methods/converge.jl:220-254, running aasol (src/utils/anderson.jl:301-443)
+ * on the device; rho_inout holds the initial profile on entry and
+ * exp(result.solution) on exit.  `result` may be NULL. */
+int cdft_converge(cdft_plan* plan, double* rho_inout, const cdft_solver_opts* opts, cdft_result* result);
+int cdft_converge_dev(cdft_plan* plan, double* d_rho_inout, const cdft_solver_opts* opts, cdft_result* result);
+
+/* Converge nplans independent systems (state points, pore widths; uneven grid
+ * sizes allowed) together, every kernel launch covering all of them.  The
+ * reference converges one system per converge! call; this replaces a loop of
+ * converge! calls over state points (e.g. an isotherm of adsorption(model,
+ * surface, p, T), src/methods/adsorption.jl:204-222). */
+int cdft_batch_converge(cdft_plan* const* plans, int nplans, double* const* rho_inout,
+                        const cdft_solver_opts* opts, cdft_result* results);
+int cdft_batch_converge_dev(cdft_plan* const* plans, int nplans, double* const* d_rho_inout,
+                            const cdft_solver_opts* opts, cdft_result* results);
+
+/* Number of our kernel launches issued by the calling thread since the last
+ * reset (instrumentation for benchmarks). */
+long long cdft_launch_count(int reset);
+
+/* Copy the last error message of the calling thread into buf (NUL-terminated);
+ * returns the code of that error (0 if none). */
+int cdft_last_error(char* buf, size_t len);
+
+/* Library version string. */
+const char* cdft_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CDFT_B200_H */

@@ -1,0 +1,69 @@
+"""CPU checks of the C-ABI boundary: the library loads, exports every symbol
+include/cdft_b200.h declares, and the ctypes struct layouts equal the C ones
+(checked by compiling a probe against the header with gcc)."""
+import ctypes
+import os
+import re
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "cdft_b200.h")
+
+
+def declared_functions():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(cdft_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_loads_and_exports_header_symbols():
+    from cdft_b200 import _lib
+    lib = _lib.load()
+    names = declared_functions()
+    assert len(names) >= 13
+    for n in names:
+        assert hasattr(lib, n), f"{n} declared in cdft_b200.h but not exported"
+    assert sorted(_lib.EXPORTED) == names
+    assert lib.cdft_version().startswith(b"cdft_b200")
+
+
+def test_last_error_without_gpu_work():
+    from cdft_b200 import _lib
+    lib = _lib.load()
+    buf = ctypes.create_string_buffer(64)
+    # invalid call: NULL plan output pointer -> CDFT_E_INVALID, no CUDA call made
+    rc = lib.cdft_plan_create(None, None)
+    assert rc == _lib.E_INVALID
+    assert lib.cdft_last_error(buf, 64) == _lib.E_INVALID
+    assert b"NULL" in buf.value
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="gcc missing")
+def test_struct_layout_matches_header(tmp_path):
+    from cdft_b200 import _lib
+    probe = tmp_path / "probe.c"
+    probe.write_text(f"""
+#include <stdio.h>
+#include <stddef.h>
+#include "{HEADER}"
+int main(void) {{
+  printf("%zu %zu %zu %zu\\n", sizeof(cdft_system_desc), sizeof(cdft_solver_opts), sizeof(cdft_result), sizeof(cdft_assoc_pair));
+  printf("%zu %zu %zu %zu %zu\\n", offsetof(cdft_system_desc, vext), offsetof(cdft_system_desc, precision),
+         offsetof(cdft_system_desc, mu_res_plus_ln_rhob), offsetof(cdft_solver_opts, iters_per_launch),
+         offsetof(cdft_result, history_len));
+  return 0;
+}}
+""")
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-std=c99", "-o", str(exe), str(probe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    sizes = list(map(int, out[0].split()))
+    offs = list(map(int, out[1].split()))
+    assert sizes == [ctypes.sizeof(_lib.SystemDesc), ctypes.sizeof(_lib.SolverOpts), ctypes.sizeof(_lib.Result),
+                     ctypes.sizeof(_lib.AssocPair)]
+    assert offs == [_lib.SystemDesc.vext.offset, _lib.SystemDesc.precision.offset,
+                    _lib.SystemDesc.mu_res_plus_ln_rhob.offset, _lib.SolverOpts.iters_per_launch.offset,
+                    _lib.Result.history_len.offset]

@@ -1,0 +1,176 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle on the
+same seeded inputs.  Tolerances (FP64 path): Phi/gradients and dF/drho 1e-10
+relative to the field's scale; converged profiles 1e-9 relative (the
+BASELINE bar), gamma 1e-9 relative."""
+import numpy as np
+import pytest
+
+import _systems as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+@pytest.mark.parametrize("case", ["methane", "water_octane", "octane"])
+def test_phi_pointwise_matches_complex_step(case):
+    import cdft_b200 as cd
+    rng = np.random.default_rng(1)
+    if case == "methane":
+        sp, so = S.methane_wall(N=64)
+    elif case == "octane":
+        sp, so = S.octane_vle(N=64)
+    else:
+        sp, so = S.water_octane_lle(N=64)
+    rho = S.random_smooth_profile(sp, rng)
+    n = so.weighted_densities(rho)                    # (nc, NF, N)
+    n = n * (1 + 0.05 * rng.standard_normal(n.shape))
+    f, g = cd.phi_pointwise(sp, n)
+    fo = so.phi(n)
+    go = so.dphi(n)
+    np.testing.assert_allclose(f, fo, rtol=1e-11, atol=1e-12 * np.max(np.abs(fo)))
+    for i in range(sp.nc):
+        for a in range(so.NF):
+            scale = np.max(np.abs(go[i, a])) + 1e-300
+            assert np.max(np.abs(g[i, a] - go[i, a])) <= 1e-10 * scale, (i, a)
+
+
+@pytest.mark.parametrize("case", ["methane_wall", "slit", "octane", "water_octane"])
+def test_functional_derivative_matches_oracle(case):
+    import cdft_b200 as cd
+    rng = np.random.default_rng(2)
+    if case == "methane_wall":
+        sp, so = S.methane_wall(N=201)
+        rho = cd.initialize_profiles(sp)
+    elif case == "slit":
+        sp, so = S.slit_pore(3e-9, 1e5, N=150)
+        rho = cd.initialize_profiles(sp)
+    elif case == "octane":
+        sp, so = S.octane_vle(N=256)
+        rho = S.random_smooth_profile(sp, rng)
+    else:
+        sp, so = S.water_octane_lle(N=256)
+        rho = S.random_smooth_profile(sp, rng)
+    d = cd.dFdrho_res(sp, rho)
+    do = so.dFdrho(rho)
+    for i in range(sp.nc):
+        assert _rel(d[i], do[i]) < 1e-10, (i, _rel(d[i], do[i]))
+
+
+def test_bulk_consistency_on_gpu():
+    import cdft_b200 as cd
+    from oracle import pcsaft_bulk as pb
+    for names, p, T, x in [(["methane"], 1e7, 150.0, [1.0]), (["water", "octane"], 1e5, 298.15, [0.5, 0.5])]:
+        pm, om = S.models(names)
+        x = np.asarray(x)
+        rho_b = x * pb.density(om, p, T, x)
+        L = om.length_scale()
+        sysp = cd.DFTSystem(pm, cd.Uniform1DCart((p, T), rho_b, [-10 * L, 10 * L], 3))
+        d = cd.dFdrho_res(sysp, cd.initialize_profiles(sysp))
+        np.testing.assert_allclose(d[:, 0], pb.mu_res(om, rho_b, T), rtol=1e-11)
+
+
+def test_free_energy_matches_oracle():
+    import cdft_b200 as cd
+    rng = np.random.default_rng(3)
+    sp, so = S.water_octane_lle(N=128)
+    rho = S.random_smooth_profile(sp, rng)
+    assert cd.F_res(sp, rho) == pytest.approx(so.F_res(rho), rel=1e-11)
+
+
+def test_converge_methane_wall_tight():
+    """Config-1 system (201 points, m=5, beta=0.1), converged to 1e-13: profiles agree to 1e-9."""
+    import cdft_b200 as cd
+    sp, so = S.methane_wall(N=201)
+    rho = cd.initialize_profiles(sp)
+    rho0 = rho.copy()
+    res = cd.converge(sp, rho, beta=0.1, tol=1e-13, anderson_m=5)
+    ro, out = so.converge(rho0, beta=0.1, tol=1e-13, anderson_m=5)
+    assert res.idid and res.errcode == 0 and out.errcode == 0
+    assert float(np.max(np.abs(rho / ro - 1))) < 1e-9
+    assert cd.adsorption(sp, rho)[0] == pytest.approx(so.adsorption(ro)[0], rel=1e-9)
+
+
+def test_converge_methane_wall_same_trajectory():
+    """At the configuration's own tolerance (1e-10) the GPU follows the oracle's
+    aasol trajectory: same phases, same iteration count, same residual history."""
+    import cdft_b200 as cd
+    sp, so = S.methane_wall(N=201)
+    rho = cd.initialize_profiles(sp)
+    rho0 = rho.copy()
+    res = cd.converge(sp, rho, beta=0.1, tol=1e-10, anderson_m=5)
+    ro, out = so.converge(rho0, beta=0.1, tol=1e-10, anderson_m=5)
+    assert res.errcode == out.errcode == 0
+    assert res.evaluations == len(out.history)
+    n = min(20, len(out.history))
+    np.testing.assert_allclose(res.history[:n], out.history[:n], rtol=1e-8)
+    assert float(np.max(np.abs(rho / ro - 1))) < 1e-8
+
+
+@pytest.mark.parametrize("case", ["octane", "water_octane"])
+def test_converge_interface_and_gamma(case):
+    import cdft_b200 as cd
+    sp, so = (S.octane_vle if case == "octane" else S.water_octane_lle)(N=256)
+    rho = cd.initialize_profiles(sp)
+    rho_o = so.initialize_profiles()
+    np.testing.assert_allclose(rho, rho_o, rtol=1e-12)
+    rho0 = rho.copy()
+    kw = dict(beta=0.05, tol=1e-12, anderson_m=5, maxit=3000)
+    res = cd.converge(sp, rho, **kw)
+    ro, out = so.converge(rho0, **kw)
+    assert res.idid and out.idid, (res, out.errcode)
+    assert float(np.max(np.abs(rho / ro - 1))) < 1e-9
+    g = cd.surface_tension(sp, rho) / 2
+    go = so.surface_tension(ro) / 2
+    assert g == pytest.approx(go, rel=1e-9)
+    assert g > 0
+
+
+def test_errcodes_match_oracle():
+    import cdft_b200 as cd
+    from oracle import pcsaft_bulk as pb
+    pm, om = S.models(["methane"])
+    rb = pb.density(om, 1e7, 150.0, [1.0])
+    L = om.length_scale()
+    # uniform bulk profile is already the fixed point -> -1
+    sysp = cd.DFTSystem(pm, cd.Uniform1DCart((1e7, 150.0), [rb], [-5 * L, 5 * L], 32))
+    rho = cd.initialize_profiles(sysp)
+    assert cd.converge(sysp, rho, beta=0.1, tol=1e-8).errcode == -1
+    # maxit exhausted -> 10
+    sp, so = S.methane_wall(N=101)
+    rho = cd.initialize_profiles(sp)
+    r0 = rho.copy()
+    res = cd.converge(sp, rho, beta=0.1, tol=1e-14, anderson_m=5, maxit=7)
+    _, out = so.converge(r0, beta=0.1, tol=1e-14, anderson_m=5, maxit=7)
+    assert res.errcode == out.errcode == 10
+    assert res.evaluations == len(out.history)
+    # pure damped Picard (m = 0)
+    rho = cd.initialize_profiles(sp)
+    res = cd.converge(sp, rho, beta=0.1, tol=1e-9, anderson_m=0, maxit=4000)
+    _, out = so.converge(r0, beta=0.1, tol=1e-9, anderson_m=0, maxit=4000)
+    assert res.errcode == out.errcode == 0
+    assert abs(res.evaluations - len(out.history)) <= 2
+
+
+def test_batch_equals_individual_bitwise():
+    """Uneven slit pores converged in one batch give bit-identical results to
+    converging each alone (deterministic reductions, per-system chunking)."""
+    import cdft_b200 as cd
+    cases = [(2e-9, 1e3, 100), (4e-9, 1e5, 180), (8e-9, 1e7, 400), (3e-9, 1e6, 137)]
+    systems, rhos = [], []
+    for H, p, N in cases:
+        sp, _ = S.slit_pore(H, p, N)
+        systems.append(sp)
+        rhos.append(cd.initialize_profiles(sp))
+    singles = []
+    for sp, r in zip(systems, rhos):
+        rr = r.copy()
+        singles.append((rr, cd.converge(sp, rr, beta=0.1, tol=1e-10, anderson_m=5)))
+    batch = [r.copy() for r in rhos]
+    results = cd.batch_converge(systems, batch, beta=0.1, tol=1e-10, anderson_m=5)
+    for (rr, rs), rb, res in zip(singles, batch, results):
+        assert res.errcode == rs.errcode == 0
+        assert res.evaluations == rs.evaluations
+        assert np.array_equal(rr, rb)
