@@ -1,0 +1,365 @@
+"""Benchmark of the converge! hot path on B200.
+
+Workload (default): the batched adsorption isotherm -- PC-SAFT methane at
+150 K in graphite slit pores, 8 pore widths 2-8 nm x 8 pressures log-spaced
+1e3-1e7 Pa = 64 state points with uneven grids (100..400 points, linear in the
+width), Anderson m=5, beta=0.1, tol=1e-10, all converged together through
+cdft_batch_converge.  A step converges all 64 systems from their initial
+profiles.  Metric: state points per second (whole job, all ranks).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+    python bench.py --impl reference ...   # CPU oracle port of the reference on host cores
+
+Multi-GPU (torchrun): every rank converges its own 64-point isotherm (weak
+scaling, no collective on the data path); the timed region is bracketed by a
+barrier and the device time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cdft.jl_b200"))
+sys.path.insert(0, ROOT)
+
+T_ISO = 150.0
+WIDTHS = np.linspace(2e-9, 8e-9, 8)
+PRESSURES = np.logspace(3, 7, 8)
+N_OF_WIDTH = [int(round(100 + 300 * k / 7)) for k in range(8)]
+SOLVER = dict(beta=0.1, tol=1e-10, anderson_m=5, maxit=10000)
+METHANE = dict(m=[1.0], sigma=[3.7039], epsilon=[150.03])
+FP64_PEAK_NOMINAL_TFLOPS = 37.0   # B200 FP64 vector (datasheet); no measured FP64 peak exists for this pool
+
+
+def isotherm_specs(rank=0):
+    """(width, pressure, N) of the 64 state points; ranks > 0 shift pressures by 0.1% per rank."""
+    out = []
+    for k, H in enumerate(WIDTHS):
+        for p in PRESSURES:
+            out.append((float(H), float(p) * (1 + 1e-3 * rank), N_OF_WIDTH[k]))
+    return out
+
+
+def build_systems(specs, precision):
+    import cdft_b200 as cd
+    model = cd.PCSAFT(["methane"], **METHANE)
+    s = model.sigma[0]
+    systems, rho0 = [], []
+    for H, p, N in specs:
+        rb = model.stable_density(p, T_ISO, [1.0])
+        st = cd.Uniform1DCart((p, T_ISO), [rb], [0.7 * s, H - 0.7 * s], N)
+        sy = cd.DFTSystem(model, st, cd.Steele(["graphite"], H), cd.DFTOptions(precision))
+        systems.append(sy)
+        rho0.append(cd.initialize_profiles(sy))
+    return systems, rho0
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+def run_ours(args, rank, world, local_rank):
+    import ctypes
+    import torch
+    import cdft_b200 as cd
+    from cdft_b200 import _lib
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    lib = _lib.load()
+
+    specs = isotherm_specs(rank)
+    systems, rho0 = build_systems(specs, args.precision)
+    n = len(systems)
+    stream = torch.cuda.Stream()
+    for s in systems:
+        _lib.check(lib.cdft_plan_set_stream(s._plan, ctypes.c_void_p(stream.cuda_stream)))
+    method = cd.AASol.for_system(None, **SOLVER)
+    opts = method.c_opts()
+    plans = (ctypes.c_void_p * n)(*[s._plan.value for s in systems])
+    init_dev = [torch.from_numpy(r).cuda() for r in rho0]
+    work_dev = [torch.empty_like(t) for t in init_dev]
+    ptrs = (ctypes.c_void_p * n)(*[t.data_ptr() for t in work_dev])
+    results = (_lib.Result * n)()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # > 126 MB L2
+
+    def step_dev():
+        with torch.cuda.stream(stream):
+            for w, i in zip(work_dev, init_dev):
+                w.copy_(i, non_blocking=True)
+        _lib.check(lib.cdft_batch_converge_dev(plans, n, ptrs, ctypes.byref(opts), results))
+
+    host_in = [r.copy() for r in rho0]
+    host_work = [np.empty_like(r) for r in rho0]
+
+    def step_e2e():
+        for w, i in zip(host_work, host_in):
+            w[...] = i
+        cd.batch_converge(systems, host_work, method=method)
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        total = 0.0
+        for _ in range(steps):
+            flush.fill_(1.0)                       # evict the previous step's data from L2 (untimed)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        torch.cuda.synchronize()
+        if dist:
+            t = torch.tensor([total], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total = float(t.item())
+            dist.barrier()
+        return total / steps
+
+    cd.launch_count(reset=True)
+    with ClockSampler(local_rank) as clk:
+        ms_dev = timed(step_dev, args.steps, args.warmup)
+    launches = cd.launch_count(reset=True)
+    # launches of the timed steps only (warm-up launches are identical per step)
+    launches_timed = int(round(launches * args.steps / (args.steps + args.warmup)))
+    iters = [results[i].evaluations for i in range(n)]
+    errc = [results[i].errcode for i in range(n)]
+    ms_e2e = timed(step_e2e, max(1, args.steps), 1)
+
+    # dominant kernel: the weighted-density circulant convolution (stage 0), timed alone
+    ms_conv = ctypes.c_double()
+    _lib.check(lib.cdft_batch_time_stage(plans, n, 0, 200, ctypes.byref(ms_conv)))
+    ms_phi = ctypes.c_double()
+    _lib.check(lib.cdft_batch_time_stage(plans, n, 1, 200, ctypes.byref(ms_phi)))
+    flops_conv = sum(2.0 * s.nc * 6 * s.ngrid[0] ** 2 for s in systems)
+    achieved = flops_conv / (ms_conv.value * 1e-3) / 1e12
+    total_units = n * world
+    value = total_units / (ms_dev * 1e-3)
+    h2d = sum(r.nbytes for r in rho0)
+    line = None
+    if rank == 0:
+        line = {
+            "metric": "state points/s (64-point slit-pore adsorption isotherm, batched converge!)",
+            "value": round(value, 3),
+            "unit": "state points/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms_dev, 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32 conv+Phi / f64 solver",
+            "data": "synthetic: seeded isotherm state points, PC-SAFT methane parameters",
+            "config": {
+                "workload": "isotherm64: methane 150 K, graphite slit pores 2-8 nm x 1e3-1e7 Pa, N=100..400",
+                "systems_per_gpu": n, "grid_points": sum(s.ngrid[0] for s in systems),
+                "solver": SOLVER, "precision": args.precision,
+                "l2": "flushed between steps (256 MB write, untimed)",
+                "evaluations_per_system": {"min": min(iters), "max": max(iters), "mean": float(np.mean(iters))},
+                "errcodes": sorted(set(errc)),
+            },
+            "e2e": {"value": round(total_units / (ms_e2e * 1e-3), 3), "unit": "state points/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
+            "gpu_launches": launches_timed,
+            "roofline": {
+                "kernel": "conv1d_kernel<double> (weighted densities, 64 systems per launch)",
+                "bound": "fp64",
+                "achieved": round(achieved, 3),
+                "peak": FP64_PEAK_NOMINAL_TFLOPS,
+                "peak_source": "nominal B200 FP64 (MEASURED_PEAKS.json has no FP64 figure)",
+                "unit": "TFLOP/s",
+                "frac": round(achieved / FP64_PEAK_NOMINAL_TFLOPS, 4),
+                "traffic": None,
+                "ms_per_launch": round(ms_conv.value, 5),
+                "phi_ms_per_launch": round(ms_phi.value, 5),
+                "algorithmic_flops_per_launch": flops_conv,
+            },
+            "clocks": clk.summary(),
+        }
+    if args.cpu_baseline and rank == 0:
+        line["cpu_baseline"] = cpu_baseline(specs, budget_s=args.cpu_budget)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
+
+
+def _oracle_converge_one(spec):
+    """Converge one isotherm state point with the CPU oracle (port of the reference)."""
+    sys.path.insert(0, ROOT)
+    from oracle import functional as fn, pcsaft_bulk as pb
+    H, p, N = spec
+    om = pb.PCSAFTModel(["methane"], METHANE["m"], METHANE["sigma"], METHANE["epsilon"])
+    rl = pb.density(om, p, T_ISO, [1.0], "liquid")
+    rv = pb.density(om, p, T_ISO, [1.0], "vapour")
+    if abs(rl / rv - 1) > 1e-10:
+        g = [pb.mu_total(om, [r], T_ISO)[0] for r in (rl, rv)]
+        rb = rl if g[0] <= g[1] else rv
+    else:
+        rb = rl
+    s = om.sigma[0]
+    st = fn.Structure((p, T_ISO), [rb], [(0.7 * s, H - 0.7 * s)], (N,))
+    so = fn.DFTSystem(om, st, [fn.SteeleWall.graphite(H)])
+    t = time.perf_counter()
+    r, out = so.converge(so.initialize_profiles(), **SOLVER)
+    return time.perf_counter() - t, out.errcode
+
+
+def cpu_baseline(specs, budget_s=20.0):
+    """Oracle (NumPy port of the reference) on one host core over a bounded sample."""
+    done, t_total = 0, 0.0
+    order = specs[::9] + [s for i, s in enumerate(specs) if i % 9]   # spread over widths/pressures first
+    for spec in order:
+        dt, _ = _oracle_converge_one(spec)
+        t_total += dt
+        done += 1
+        if t_total > budget_s:
+            break
+    return {"value": round(done / t_total, 4), "unit": "state points/s", "cores": 1, "kind": "port",
+            "sample": f"{done} of the 64 isotherm state points, oracle converge! (NumPy FP64), 1 thread"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU implementation of the path.  Julia is
+    not available here, so this is the oracle port, run with one process per
+    host core; each step converges one bounded sample of state points."""
+    if rank != 0:
+        return None
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    specs = isotherm_specs(0)
+    ctx = mp.get_context("spawn")
+    per_step = cores
+    times = []
+    with ctx.Pool(cores) as pool:
+        k = 0
+        for it in range(args.warmup + args.steps):
+            sample = [specs[(k + j) % len(specs)] for j in range(per_step)]
+            k += per_step
+            t0 = time.perf_counter()
+            pool.map(_oracle_converge_one, sample)
+            dt = time.perf_counter() - t0
+            if it >= args.warmup:
+                times.append(dt)
+    ms = 1e3 * float(np.mean(times))
+    value = per_step / (ms * 1e-3)
+    return {
+        "impl": "reference",
+        "metric": "state points/s (64-point slit-pore adsorption isotherm, batched converge!)",
+        "value": round(value, 4),
+        "unit": "state points/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms, 2),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic: seeded isotherm state points, PC-SAFT methane parameters",
+        "config": {"workload": "isotherm64: methane 150 K, graphite slit pores 2-8 nm x 1e3-1e7 Pa, N=100..400",
+                   "solver": SOLVER, "sample_per_step": per_step},
+        "cpu_baseline": {"value": round(value, 4), "unit": "state points/s", "cores": cores, "kind": "port",
+                         "sample": f"{per_step} state points per step, one per process (spawn pool)"},
+        "e2e": {"value": round(value, 4), "unit": "state points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        line = run_ours(args, rank, world, local_rank)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -32,6 +32,7 @@ EXPORTED = [
     "cdft_free_energy_res", "cdft_phi_pointwise",
     "cdft_converge", "cdft_converge_dev",
     "cdft_batch_converge", "cdft_batch_converge_dev",
+    "cdft_plan_set_stream", "cdft_batch_time_stage",
     "cdft_launch_count", "cdft_last_error", "cdft_version",
 ]
 
@@ -118,6 +119,8 @@ def load(path=LIB_PATH):
                                         ctypes.POINTER(SolverOpts), ctypes.POINTER(Result)]
     lib.cdft_batch_converge_dev.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.POINTER(P),
                                             ctypes.POINTER(SolverOpts), ctypes.POINTER(Result)]
+    lib.cdft_plan_set_stream.argtypes = [P, P]
+    lib.cdft_batch_time_stage.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
     lib.cdft_launch_count.argtypes = [ctypes.c_int]
     lib.cdft_launch_count.restype = ctypes.c_longlong
     lib.cdft_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]

@@ -28,6 +28,9 @@ _B = np.array([
     [-355.60235612, -165.20769346, -29.666905585]])
 
 
+_TC_CACHE = {}
+
+
 class PCSAFT:
     """PC-SAFT parameters of a (one-bead-per-component) mixture.
 
@@ -116,30 +119,38 @@ class PCSAFT:
         rho = np.asarray(rho, dtype=float)
         return R * T * (np.log(rho) - 1.5 * np.log(T) + self.mu_res(rho, T))
 
-    def molar_density(self, p, T, x, phase="liquid"):
+    def molar_density(self, p, T, x, phase="liquid", eta_guess=None):
+        """Molar density at (p, T, x); liquid = densest root, vapour = most dilute."""
+        from scipy.optimize import brentq
         x = np.asarray(x, dtype=float) / np.sum(x)
         scale = np.pi / 6 * (x * self.m * self.d(T) ** 3).sum() * N_A
 
         def f(eta):
             return self.pressure(x * eta / scale, T) - p
 
-        grid = np.concatenate([np.logspace(-12, -1, 300), np.linspace(0.1005, 0.74, 500)])
+        if eta_guess is not None:
+            a, b = 0.97 * eta_guess, min(1.03 * eta_guess, 0.7405)
+            if (f(a) > 0) != (f(b) > 0):
+                return brentq(f, a, b, xtol=1e-17, rtol=1e-15) / scale
+        grid = np.concatenate([np.logspace(-12, -1.3, 40), np.linspace(0.051, 0.74, 70)])
         vals = np.array([f(g) for g in grid])
         idx = np.nonzero(np.sign(vals[:-1]) != np.sign(vals[1:]))[0]
         if idx.size == 0:
             raise ValueError("no density root at the given state")
         k = idx[-1] if phase == "liquid" else idx[0]
-        a, b, fa = grid[k], grid[k + 1], vals[k]
-        for _ in range(200):
-            c = 0.5 * (a + b)
-            fc = f(c)
-            if (fc > 0) == (fa > 0):
-                a, fa = c, fc
-            else:
-                b = c
-            if b - a <= 1e-16 * b:
-                break
-        return 0.5 * (a + b) / scale
+        return brentq(f, grid[k], grid[k + 1], xtol=1e-17, rtol=1e-15) / scale
+
+    def stable_density(self, p, T, x):
+        """Molar density of the stable phase at (p, T, x): of the vapour-like and
+        liquid-like roots, the one with the lower Gibbs energy per mole
+        (Clapeyron's volume(model, p, T, x) default)."""
+        x = np.asarray(x, dtype=float) / np.sum(x)
+        rl = self.molar_density(p, T, x, "liquid")
+        rv = self.molar_density(p, T, x, "vapour")
+        if abs(rl / rv - 1) < 1e-10:
+            return rl
+        g = [float((x * self.chemical_potential(x * r, T)).sum()) for r in (rl, rv)]
+        return rl if g[0] <= g[1] else rv
 
     def volume(self, p, T, x, phase="liquid"):
         return 1.0 / self.molar_density(p, T, x, phase)
@@ -166,23 +177,26 @@ class PCSAFT:
 
     def critical_temperature(self):
         """T at which the isotherm first has a horizontal inflection (pure component)."""
+        key = (float(self.m[0]), float(self.sigma[0]), float(self.epsilon[0]), tuple(self.assoc.get(0, ())))
+        if key in _TC_CACHE:
+            return _TC_CACHE[key]
+
         def min_slope(T):
             scale = np.pi / 6 * self.m[0] * self.d(T)[0] ** 3 * N_A
-            best = np.inf
-            for eta in np.linspace(0.02, 0.45, 300):
-                r = eta / scale
-                best = min(best, (self.pressure([r * (1 + 1e-6)], T) - self.pressure([r * (1 - 1e-6)], T)) / (2e-6 * r))
-            return best
+            r = np.linspace(0.05, 0.35, 61) / scale
+            return min((self.pressure([v * (1 + 1e-6)], T) - self.pressure([v * (1 - 1e-6)], T)) / (2e-6 * v) for v in r)
+
         lo, hi = 30.0, 3000.0
         while min_slope(lo) > 0:
             lo *= 0.7
-        for _ in range(60):
+        for _ in range(40):
             mid = 0.5 * (lo + hi)
             if min_slope(mid) < 0:
                 lo = mid
             else:
                 hi = mid
-        return 0.5 * (lo + hi)
+        _TC_CACHE[key] = 0.5 * (lo + hi)
+        return _TC_CACHE[key]
 
     def lle(self, p, T, z=(0.5, 0.5), x1=(0.999, 0.001), x2=(0.001, 0.999), iters=400):
         """Binary liquid-liquid split at (p, T): K-value substitution + Rachford-Rice."""
@@ -190,12 +204,15 @@ class PCSAFT:
         x1 = np.asarray(x1, dtype=float)
         x2 = np.asarray(x2, dtype=float)
 
-        def lnphi(x):
-            r = self.molar_density(p, T, x, "liquid")
+        hint = {}
+
+        def lnphi(x, key):
+            r = self.molar_density(p, T, x, "liquid", hint.get(key))
+            hint[key] = np.pi / 6 * (x / x.sum() * self.m * self.d(T) ** 3).sum() * N_A * r
             return self.mu_res(r * x, T) - np.log(p / (r * R * T))
 
         for _ in range(iters):
-            K = np.exp(lnphi(x1) - lnphi(x2))
+            K = np.exp(lnphi(x1, 1) - lnphi(x2, 2))
             lo, hi = 1e-12, 1 - 1e-12
             for _ in range(200):
                 b = 0.5 * (lo + hi)

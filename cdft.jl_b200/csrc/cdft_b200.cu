@@ -72,6 +72,7 @@ struct Batch;
 struct cdft_plan {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
     cdft_system_desc desc;
     SysDev sys;            // host copy holding device pointers
     int N = 0, m_cap = -1;
@@ -302,7 +303,7 @@ void plan_free(cdft_plan* p)
     cudaFree(p->d_part);
     cudaFree(p->d_dfield);
     cudaFree(p->d_fval);
-    if (p->stream) cudaStreamDestroy(p->stream);
+    if (p->own_stream) cudaStreamDestroy(p->own_stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -499,6 +500,7 @@ int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, boo
     Batch* b = nullptr;
     rc = get_batch(plans, &b);
     if (rc) return rc;
+    b->stream = plans[0]->stream;
     CU(cudaSetDevice(plans[0]->device));
     for (auto* p : plans) {
         rc = plan_alloc_m(p, opts->m);
@@ -597,7 +599,44 @@ int self_batch(cdft_plan* p, Batch** b)
     std::vector<cdft_plan*> v{p};
     int rc = get_batch(v, b);
     if (rc) return rc;
+    (*b)->stream = p->stream;
     return batch_upload_sys(*b);
+}
+
+int launch_stage(Batch* b, int stage)
+{
+    const bool mixed = b->mixed;
+    const size_t smem = (size_t)(CONV_QC + CONV_TILE + CONV_QC + 31) * (mixed ? sizeof(float) : sizeof(double));
+    switch (stage) {
+    case 0:
+    case 2:
+        if (mixed)
+            conv1d_kernel<float><<<b->ntasks, CONV_WARPS * 32, smem, b->stream>>>(b->d_tasks, b->d_sys, nullptr, stage / 2);
+        else
+            conv1d_kernel<double><<<b->ntasks, CONV_WARPS * 32, smem, b->stream>>>(b->d_tasks, b->d_sys, nullptr, stage / 2);
+        g_launches += 1;
+        break;
+    case 1: {
+        int rc = mixed ? launch_phi<float>(b, nullptr) : launch_phi<double>(b, nullptr);
+        if (rc) return rc;
+        g_launches += 1;
+        break;
+    }
+    case 3: {
+        int rc = mixed ? launch_eval_stages<float>(b, nullptr, true) : launch_eval_stages<double>(b, nullptr, true);
+        if (rc) return rc;
+        if (mixed)
+            dfdrho_out_kernel<float><<<b->nechunks, ELEM_THREADS, 0, b->stream>>>(b->d_echunks, b->d_sys);
+        else
+            dfdrho_out_kernel<double><<<b->nechunks, ELEM_THREADS, 0, b->stream>>>(b->d_echunks, b->d_sys);
+        g_launches += 1;
+        break;
+    }
+    default:
+        return set_error(CDFT_E_INVALID, "stage %d", stage);
+    }
+    CHECK_LAUNCH();
+    return 0;
 }
 
 int functional_derivative(cdft_plan* p, const double* rho, double* out, bool is_dev)
@@ -657,11 +696,12 @@ int cdft_plan_create(const cdft_system_desc* desc, cdft_plan** plan)
     p->device = dev;
     p->desc = *desc;
     p->desc.vext = nullptr;
-    cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
+    cudaError_t e = cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete p;
         return set_error(CDFT_E_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
     }
+    p->stream = p->own_stream;
     cdft_system_desc tmp = *desc;
     p->desc = tmp;
     rc = plan_build(p);
@@ -797,6 +837,46 @@ int cdft_batch_converge_dev(cdft_plan* const* plans, int nplans, double* const* 
     if (!plans || nplans <= 0) return set_error(CDFT_E_INVALID, "no plans");
     std::vector<cdft_plan*> v(plans, plans + nplans);
     return batch_converge(v, d_rho_inout, true, opts, results);
+}
+
+int cdft_plan_set_stream(cdft_plan* plan, void* stream)
+{
+    g_err_code = 0;
+    if (!plan) return set_error(CDFT_E_INVALID, "plan is NULL");
+    CU(cudaSetDevice(plan->device));
+    CU(cudaStreamSynchronize(plan->stream));
+    plan->stream = stream ? (cudaStream_t)stream : plan->own_stream;
+    return 0;
+}
+
+int cdft_batch_time_stage(cdft_plan* const* plans, int nplans, int stage, int reps, double* ms_per_launch)
+{
+    g_err_code = 0;
+    if (!plans || nplans <= 0 || reps <= 0 || !ms_per_launch) return set_error(CDFT_E_INVALID, "invalid argument");
+    std::vector<cdft_plan*> v(plans, plans + nplans);
+    Batch* b = nullptr;
+    int rc = get_batch(v, &b);
+    if (rc) return rc;
+    b->stream = v[0]->stream;
+    CU(cudaSetDevice(v[0]->device));
+    rc = batch_upload_sys(b);
+    if (rc) return rc;
+    for (int w = 0; w < 3 && !rc; ++w) rc = launch_stage(b, stage);
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    CU(cudaEventCreate(&e0));
+    CU(cudaEventCreate(&e1));
+    CU(cudaEventRecord(e0, b->stream));
+    for (int r = 0; r < reps && !rc; ++r) rc = launch_stage(b, stage);
+    CU(cudaEventRecord(e1, b->stream));
+    CU(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    *ms_per_launch = (double)ms / reps;
+    return 0;
 }
 
 long long cdft_launch_count(int reset)

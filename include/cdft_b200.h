@@ -154,6 +154,20 @@ int cdft_batch_converge(cdft_plan* const* plans, int nplans, double* const* rho_
 int cdft_batch_converge_dev(cdft_plan* const* plans, int nplans, double* const* d_rho_inout,
                             const cdft_solver_opts* opts, cdft_result* results);
 
+/* Bind a plan to a caller-owned CUDA stream (a cudaStream_t, e.g. the stream of
+ * a CUDA.jl task or of torch); NULL restores the plan's own stream.  The
+ * reference has no counterpart: KernelAbstractions launches on the task's
+ * default stream and synchronizes after every stage (models.jl:142-179). */
+int cdft_plan_set_stream(cdft_plan* plan, void* stream);
+
+/* Average device time of one launch of a converge! stage over the systems of
+ * `plans` (the profiles currently held by the plans, e.g. after a converge),
+ * timed with CUDA events on the plans' stream after 3 warm-up launches:
+ * stage 0 weighted densities (evaluate_field!), 1 fused Phi/dPhi (AD stage),
+ * 2 adjoint convolutions (integrate_field!), 3 the whole δFδρ_res! evaluation.
+ * Instrumentation for roofline accounting; no reference counterpart. */
+int cdft_batch_time_stage(cdft_plan* const* plans, int nplans, int stage, int reps, double* ms_per_launch);
+
 /* Number of our kernel launches issued by the calling thread since the last
  * reset (instrumentation for benchmarks). */
 long long cdft_launch_count(int reset);

@@ -97,11 +97,17 @@ def _assoc_X(model, rho_n, T, d, zeta2, zeta3):
             delta[2 * j, 2 * i + 1] = D
             delta[2 * i + 1, 2 * j] = D
     rho_site = np.repeat(rho_n, 2)
+    if all(i == j for (i, j, _, _) in model.assoc):
+        # only 2B self-association: X_A = X_B = 2 / (1 + sqrt(1 + 4 rho_i Delta_i)) in closed form
+        X = np.ones(ns, dtype=delta.dtype)
+        for (i, _, _, _) in model.assoc:
+            q = rho_n[i] * delta[2 * i, 2 * i + 1]
+            X[2 * i] = X[2 * i + 1] = 2.0 / (1.0 + np.sqrt(1.0 + 4.0 * q))
+        return X
     X = np.ones(ns, dtype=delta.dtype)
-    for _ in range(200):  # successive substitution (damped) then Newton
-        Xn = 1.0 / (1.0 + delta @ (rho_site * X))
-        X = 0.5 * (X + Xn)
-    for _ in range(30):
+    for _ in range(5):  # a few damped substitutions, then Newton (quadratic)
+        X = 0.5 * (X + 1.0 / (1.0 + delta @ (rho_site * X)))
+    for _ in range(12):
         F = X * (1.0 + delta @ (rho_site * X)) - 1.0
         J = np.diag(1.0 + delta @ (rho_site * X)) + X[:, None] * delta * rho_site[None, :]
         X = X - np.linalg.solve(J, F)
@@ -185,31 +191,31 @@ def _dp_deta(model, x, T, eta):
     return pressure(model, x * rho_tot, T), rho_tot
 
 
-def density(model, p, T, x, phase="liquid"):
-    """Molar density (mol/m^3) at (p, T, x): liquid = largest root, vapour = smallest."""
+def density(model, p, T, x, phase="liquid", eta_guess=None):
+    """Molar density (mol/m^3) at (p, T, x): liquid = largest root, vapour = smallest.
+
+    Roots of p(eta) - p are bracketed on a coarse packing-fraction grid (or
+    around ``eta_guess``) and polished with Brent's method."""
+    from scipy.optimize import brentq
     x = np.asarray(x, dtype=np.float64)
     x = x / np.sum(x)
-    etas = np.concatenate([np.logspace(-12, -1, 400), np.linspace(0.1001, 0.74, 700)])
-    vals = np.array([_dp_deta(model, x, T, e)[0] - p for e in etas])
-    roots = []
-    for k in range(len(etas) - 1):
-        if vals[k] == 0.0:
-            roots.append(etas[k])
-        elif np.sign(vals[k]) != np.sign(vals[k + 1]):
-            a, b, fa = etas[k], etas[k + 1], vals[k]
-            for _ in range(200):
-                c = 0.5 * (a + b)
-                fc = _dp_deta(model, x, T, c)[0] - p
-                if np.sign(fc) == np.sign(fa):
-                    a, fa = c, fc
-                else:
-                    b = c
-                if b - a < 1e-16 * b:
-                    break
-            roots.append(0.5 * (a + b))
-    if not roots:
+
+    def f(e):
+        return _dp_deta(model, x, T, e)[0] - p
+
+    if eta_guess is not None:
+        a, b = eta_guess * 0.97, min(eta_guess * 1.03, 0.7405)
+        fa, fb = f(a), f(b)
+        if np.sign(fa) != np.sign(fb):
+            eta = brentq(f, a, b, xtol=1e-17, rtol=1e-15, maxiter=200)
+            return _dp_deta(model, x, T, eta)[1]
+    etas = np.concatenate([np.logspace(-12, -1.3, 40), np.linspace(0.051, 0.74, 70)])
+    vals = np.array([f(e) for e in etas])
+    idx = np.nonzero(np.sign(vals[:-1]) != np.sign(vals[1:]))[0]
+    if idx.size == 0:
         raise RuntimeError("no density root")
-    eta = roots[-1] if phase == "liquid" else roots[0]
+    k = idx[-1] if phase == "liquid" else idx[0]
+    eta = brentq(f, etas[k], etas[k + 1], xtol=1e-17, rtol=1e-15, maxiter=200)
     return _dp_deta(model, x, T, eta)[1]
 
 
@@ -253,24 +259,21 @@ def saturation_pure(model, T, p_guess=None):
 
 def critical_temperature(model):
     """Pure-component critical temperature: the T where min_rho dp/drho == 0."""
+    d0 = model.hs_diameter
+
     def min_dpdrho(T):
-        d = model.hs_diameter(T)
-        scale = np.pi / 6.0 * model.m[0] * d[0] ** 3 * N_A
-        etas = np.linspace(0.02, 0.45, 300)
+        scale = np.pi / 6.0 * model.m[0] * d0(T)[0] ** 3 * N_A
         best = np.inf
-        for e in etas:
+        for e in np.linspace(0.05, 0.35, 61):
             r = e / scale
             h = 1e-6 * r
-            dp = (pressure(model, [r + h], T) - pressure(model, [r - h], T)) / (2 * h)
-            best = min(best, dp)
+            best = min(best, (pressure(model, [r + h], T) - pressure(model, [r - h], T)) / (2 * h))
         return best
+
     lo, hi = 50.0, 2000.0
-    # find a bracket: unstable (negative min) at lo, stable at hi
-    T = lo
-    while min_dpdrho(T) > 0 and T < hi:
-        T *= 0.8
-    lo = T
-    for _ in range(60):
+    while min_dpdrho(lo) > 0:
+        lo *= 0.7
+    for _ in range(40):
         mid = 0.5 * (lo + hi)
         if min_dpdrho(mid) < 0:
             lo = mid
@@ -286,18 +289,21 @@ def lle_binary(model, p, T, x_feed=(0.5, 0.5), guess=((0.999, 0.001), (0.001, 0.
     x1 = np.array(guess[0], dtype=np.float64)
     x2 = np.array(guess[1], dtype=np.float64)
 
-    def lnphi(x):
-        r = density(model, p, T, x, "liquid")
+    eta_hint = {}
+
+    def lnphi(x, key):
+        r = density(model, p, T, x, "liquid", eta_hint.get(key))
+        d = model.hs_diameter(T)
+        eta_hint[key] = np.pi / 6 * np.sum(x / np.sum(x) * model.m * d ** 3) * N_A * r
         rho = r * x
         Z = p / (r * R_GAS * T)
         return mu_res(model, rho, T) - np.log(Z)
 
+    z = np.asarray(x_feed, dtype=np.float64)
     for _ in range(iters):
-        l1, l2 = lnphi(x1), lnphi(x2)
+        l1, l2 = lnphi(x1, 1), lnphi(x2, 2)
         K = np.exp(l1 - l2)  # x2_i = K_i x1_i
-        # Rachford--Rice on the feed
-        z = np.asarray(x_feed, dtype=np.float64)
-        a, b = 1e-12, 1 - 1e-12
+        a, b = 1e-12, 1 - 1e-12   # Rachford--Rice on the feed
         for _ in range(200):
             beta = 0.5 * (a + b)
             g = np.sum(z * (K - 1) / (1 + beta * (K - 1)))
@@ -309,8 +315,8 @@ def lle_binary(model, p, T, x_feed=(0.5, 0.5), guess=((0.999, 0.001), (0.001, 0.
         x2n = K * x1n
         x1n /= np.sum(x1n)
         x2n /= np.sum(x2n)
-        if np.max(np.abs(np.log(x1n) - np.log(x1))) + np.max(np.abs(np.log(x2n) - np.log(x2))) < 1e-14:
-            x1, x2 = x1n, x2n
-            break
+        done = np.max(np.abs(np.log(x1n) - np.log(x1))) + np.max(np.abs(np.log(x2n) - np.log(x2))) < 1e-13
         x1, x2 = x1n, x2n
+        if done:
+            break
     return x1, x2

@@ -5,6 +5,8 @@ Parameters are the explicit PC-SAFT sets of the benchmark configurations
 (methane, n-octane, water 2B, argon); the Steele wall is graphite from the
 reference's Steele database row.
 """
+import functools
+
 import numpy as np
 
 from oracle import functional as fn
@@ -65,9 +67,22 @@ def slit_pore(H, p, N, T=150.0, precision="fp64"):
     return pair(["methane"], (p, T), [rb], (0.7 * s, H - 0.7 * s), N, walls=(H,), precision=precision)
 
 
+@functools.lru_cache(maxsize=None)
+def _vle(name, T):
+    _, om = models([name])
+    return pb.saturation_pure(om, T)
+
+
+@functools.lru_cache(maxsize=None)
+def _lle(names, p, T):
+    _, om = models(list(names))
+    x1, x2 = pb.lle_binary(om, p, T)
+    return tuple(pb.density(om, p, T, x1) * x1), tuple(pb.density(om, p, T, x2) * x2)
+
+
 def octane_vle(N=256, box_sigmas=40.0, T=298.15):
     _, om = models(["octane"])
-    psat, rl, rv = pb.saturation_pure(om, T)
+    psat, rl, rv = _vle("octane", T)
     s = om.sigma[0]
     half = box_sigmas * s / 2
     return pair(["octane"], (psat, T), [rl], (-half, half), N, kind="twophase", rho_bulk2=[rv])
@@ -75,9 +90,7 @@ def octane_vle(N=256, box_sigmas=40.0, T=298.15):
 
 def water_octane_lle(N=256, box_sigmas=60.0, T=298.15, p=1e5):
     _, om = models(["water", "octane"])
-    x1, x2 = pb.lle_binary(om, p, T)
-    r1 = pb.density(om, p, T, x1) * x1
-    r2 = pb.density(om, p, T, x2) * x2
+    r1, r2 = _lle(("water", "octane"), p, T)
     s = om.sigma[0]
     half = box_sigmas * s / 2
     return pair(["water", "octane"], (p, T), list(r1), (-half, half), N, kind="twophase", rho_bulk2=list(r2))

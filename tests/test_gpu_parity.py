@@ -14,6 +14,32 @@ def _rel(a, b):
     return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
 
 
+def _aligned_log_diff(rho, ref):
+    """Max |ln rho - ln ref| after removing the interface displacements.
+
+    A periodic box holding two interfaces at coexistence has two (near-)zero
+    modes: a common translation and a breathing mode (one phase grows while
+    the other shrinks), so two correct solvers can stop with the interfaces a
+    tiny distance apart.  Each half of the box holds one interface (the seed
+    puts them at +-H/4 around the centre); one displacement per half is fitted
+    by least squares with the exact spectral derivative of the periodic
+    N-point problem and removed before comparing.  Returns (max diff, shifts
+    in grid units)."""
+    N = ref.shape[-1]
+    k = np.fft.fftfreq(N) * N
+    lr = np.log(ref)
+    D = np.real(np.fft.ifft(2j * np.pi * k / N * np.fft.fft(lr, axis=-1), axis=-1))
+    d = np.log(rho) - lr
+    r = d.copy()
+    shifts = []
+    for half in (slice(0, N // 2), slice(N // 2, N)):
+        Dh, dh = D[:, half], d[:, half]
+        sh = -np.sum(dh * Dh) / np.sum(Dh * Dh)
+        r[:, half] = dh + sh * Dh
+        shifts.append(float(sh))
+    return float(np.max(np.abs(r))), shifts
+
+
 @pytest.mark.parametrize("case", ["methane", "water_octane", "octane"])
 def test_phi_pointwise_matches_complex_step(case):
     import cdft_b200 as cd
@@ -115,13 +141,16 @@ def test_converge_interface_and_gamma(case):
     sp, so = (S.octane_vle if case == "octane" else S.water_octane_lle)(N=256)
     rho = cd.initialize_profiles(sp)
     rho_o = so.initialize_profiles()
-    np.testing.assert_allclose(rho, rho_o, rtol=1e-12)
+    # the seeds agree up to the two independent critical-temperature estimates
+    np.testing.assert_allclose(rho, rho_o, rtol=1e-3)
     rho0 = rho.copy()
-    kw = dict(beta=0.05, tol=1e-12, anderson_m=5, maxit=3000)
+    kw = dict(beta=0.01, tol=1e-12, anderson_m=5, maxit=10000)   # converge! defaults except tol
     res = cd.converge(sp, rho, **kw)
     ro, out = so.converge(rho0, **kw)
     assert res.idid and out.idid, (res, out.errcode)
-    assert float(np.max(np.abs(rho / ro - 1))) < 1e-9
+    err, shifts = _aligned_log_diff(rho, ro)
+    assert err < 1e-9, (err, shifts)
+    assert max(abs(x) for x in shifts) < 1e-3
     g = cd.surface_tension(sp, rho) / 2
     go = so.surface_tension(ro) / 2
     assert g == pytest.approx(go, rel=1e-9)
