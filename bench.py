@@ -142,7 +142,7 @@ def run_ours(args, rank, world, local_rank):
     for s in systems:
         _lib.check(lib.cdft_plan_set_stream(s._plan, ctypes.c_void_p(stream.cuda_stream)))
     method = cd.AASol.for_system(None, **SOLVER)
-    opts = method.c_opts()
+    opts = method.c_opts(engine=args.engine)
     plans = (ctypes.c_void_p * n)(*[s._plan.value for s in systems])
     init_dev = [torch.from_numpy(r).cuda() for r in rho0]
     work_dev = [torch.empty_like(t) for t in init_dev]
@@ -162,7 +162,7 @@ def run_ours(args, rank, world, local_rank):
     def step_e2e():
         for w, i in zip(host_work, host_in):
             w[...] = i
-        cd.batch_converge(systems, host_work, method=method)
+        cd.batch_converge(systems, host_work, method=method, engine=args.engine)
 
     def timed(fn, steps, warmup):
         for _ in range(warmup):
@@ -228,7 +228,7 @@ def run_ours(args, rank, world, local_rank):
             "config": {
                 "workload": "isotherm64: methane 150 K, graphite slit pores 2-8 nm x 1e3-1e7 Pa, N=100..400",
                 "systems_per_gpu": n, "grid_points": sum(s.ngrid[0] for s in systems),
-                "solver": SOLVER, "precision": args.precision,
+                "solver": SOLVER, "precision": args.precision, "engine": args.engine,
                 "l2": "flushed between steps (256 MB write, untimed)",
                 "evaluations_per_system": {"min": min(iters), "max": max(iters), "mean": float(np.mean(iters))},
                 "errcodes": sorted(set(errc)),
@@ -347,6 +347,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--engine", default="auto", choices=["auto", "grid", "persistent"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     args = ap.parse_args()

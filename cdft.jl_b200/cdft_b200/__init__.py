@@ -250,13 +250,14 @@ class AASol:
         return cls(anderson_m, maxit=maxit, rtol=tol, atol=tol, beta=beta, picard_maxit=maxit, picard_beta=beta,
                    picard_rtol=anderson_start, picard_atol=anderson_start, verbose=verbose)
 
-    def c_opts(self, time_budget_s=0.0, iters_per_launch=0):
+    def c_opts(self, time_budget_s=0.0, iters_per_launch=0, engine="auto"):
         o = _lib.SolverOpts()
         o.m, o.maxit, o.rtol, o.atol, o.beta = self.m, self.maxit, self.rtol, self.atol, self.beta
         o.picard_maxit, o.picard_beta = self.picard_maxit, self.picard_beta
         o.picard_rtol, o.picard_atol = self.picard_rtol, self.picard_atol
         o.time_budget_s = time_budget_s
         o.iters_per_launch = iters_per_launch
+        o.engine = {"auto": _lib.ENGINE_AUTO, "grid": _lib.ENGINE_GRID, "persistent": _lib.ENGINE_PERSISTENT}[engine]
         return o
 
 
@@ -282,9 +283,11 @@ def _check_rho(system, rho):
         raise ValueError(f"rho has shape {rho.shape}, expected {(system.nc,) + tuple(reversed(system.ngrid))}")
 
 
-def converge(system, rho, method=None, time_budget_s=0.0, iters_per_launch=0, keep_history=True, **kwargs):
+def converge(system, rho, method=None, time_budget_s=0.0, iters_per_launch=0, keep_history=True, engine="auto",
+             **kwargs):
     """converge!(system, ρ; kwargs...) / converge!(system, ρ, solver): converges
-    ``rho`` in place (converge.jl:214-254) and returns the aasol status."""
+    ``rho`` in place (converge.jl:214-254) and returns the aasol status.
+    ``engine``: "auto", "grid" (per-stage kernels) or "persistent" (one CTA per system)."""
     _check_rho(system, rho)
     method = method or AASol.for_system(system, **kwargs)
     res = _lib.Result()
@@ -294,7 +297,7 @@ def converge(system, rho, method=None, time_budget_s=0.0, iters_per_launch=0, ke
         hist = np.zeros(cap)
         res.history = _lib.dptr(hist)
         res.history_cap = cap
-    opts = method.c_opts(time_budget_s, iters_per_launch)
+    opts = method.c_opts(time_budget_s, iters_per_launch, engine)
     _lib.check(_LIB.cdft_converge(system._plan, _lib.dptr(rho), ctypes.byref(opts), ctypes.byref(res)))
     out = ConvergeResult(res, None if hist is None else hist[: res.history_len].copy())
     if method.verbose:
@@ -303,7 +306,7 @@ def converge(system, rho, method=None, time_budget_s=0.0, iters_per_launch=0, ke
     return out
 
 
-def batch_converge(systems, rhos, method=None, time_budget_s=0.0, iters_per_launch=0, **kwargs):
+def batch_converge(systems, rhos, method=None, time_budget_s=0.0, iters_per_launch=0, engine="auto", **kwargs):
     """Converge many independent systems (state points, pore widths) together."""
     n = len(systems)
     if n != len(rhos):
@@ -314,7 +317,7 @@ def batch_converge(systems, rhos, method=None, time_budget_s=0.0, iters_per_laun
     plans = (ctypes.c_void_p * n)(*[s._plan.value for s in systems])
     ptrs = (ctypes.POINTER(ctypes.c_double) * n)(*[_lib.dptr(r) for r in rhos])
     res = (_lib.Result * n)()
-    opts = method.c_opts(time_budget_s, iters_per_launch)
+    opts = method.c_opts(time_budget_s, iters_per_launch, engine)
     _lib.check(_LIB.cdft_batch_converge(plans, n, ptrs, ctypes.byref(opts), res))
     return [ConvergeResult(res[i], None) for i in range(n)]
 

@@ -21,6 +21,7 @@ E_BUDGET = -4
 
 COORD_CART, COORD_SPH, COORD_CYL = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
+ENGINE_AUTO, ENGINE_GRID, ENGINE_PERSISTENT = 0, 1, 2
 
 LIB_NAME = "libcdft_b200.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
@@ -75,6 +76,7 @@ class SolverOpts(ctypes.Structure):
         ("picard_beta", ctypes.c_double), ("picard_rtol", ctypes.c_double), ("picard_atol", ctypes.c_double),
         ("time_budget_s", ctypes.c_double),
         ("iters_per_launch", ctypes.c_int),
+        ("engine", ctypes.c_int),
     ]
 
 

@@ -16,7 +16,7 @@
 #include <string>
 #include <vector>
 
-#include "kernels.cuh"
+#include "persistent.cuh"
 
 namespace {
 
@@ -77,10 +77,8 @@ struct cdft_plan {
     SysDev sys;            // host copy holding device pointers
     int N = 0, m_cap = -1;
     double dz[3] = {0, 0, 0};
-    double* d_taps_eval = nullptr;
-    double* d_taps_int = nullptr;
-    float* d_taps_eval32 = nullptr;
-    float* d_taps_int32 = nullptr;
+    double* d_taps = nullptr;
+    float* d_taps32 = nullptr;
     double* d_vext = nullptr;
     double* d_vec = nullptr;      // rho, sol, gx, res, df, out
     double* d_Q = nullptr;
@@ -240,8 +238,7 @@ int plan_build(cdft_plan* p)
     const size_t ne = (size_t)S.n_elem;
     const size_t ntap = (size_t)S.nconv * nc * N;
     const size_t esz = S.mixed ? sizeof(float) : sizeof(double);
-    CU(cudaMalloc(&p->d_taps_eval, ntap * sizeof(double)));
-    CU(cudaMalloc(&p->d_taps_int, ntap * sizeof(double)));
+    CU(cudaMalloc(&p->d_taps, ntap * sizeof(double)));
     CU(cudaMalloc(&p->d_vec, ne * 6 * sizeof(double)));
     CU(cudaMemsetAsync(p->d_vec, 0, ne * 6 * sizeof(double), p->stream));
     CU(cudaMalloc(&p->d_part, ntap * S.ksplit * esz));
@@ -261,8 +258,7 @@ int plan_build(cdft_plan* p)
     S.dfield = p->d_dfield;
     S.fval = p->d_fval;
     S.vext = p->d_vext;
-    S.taps_eval = p->d_taps_eval;
-    S.taps_int = p->d_taps_int;
+    S.taps = p->d_taps;
 
     // kernels of get_fields(::PCSAFTModel) (PCSAFT.jl:55-61), fields 2..7 in 1D
     const double psi = PSI_DISP;
@@ -272,19 +268,14 @@ int plan_build(cdft_plan* p)
     for (int i = 0; i < nc; ++i)
         for (int f = 0; f < S.nconv; ++f) {
             const size_t off = ((size_t)i * S.nconv + f) * N;
-            const double sign = types[f] == 3 ? -1.0 : 1.0;   // vector fields: δfδρ .-= (weighted_densities.jl:381)
-            taps1d_kernel<<<(N + 127) / 128, 128, 0, p->stream>>>(N, span, L, types[f], wf[f] * P.d[i], S.NA,
-                                                                   sign, p->d_taps_eval + off, p->d_taps_int + off);
+            taps1d_kernel<<<(N + 127) / 128, 128, 0, p->stream>>>(N, span, L, types[f], wf[f] * P.d[i], p->d_taps + off);
             CHECK_LAUNCH();
         }
     if (S.mixed) {
-        CU(cudaMalloc(&p->d_taps_eval32, ntap * sizeof(float)));
-        CU(cudaMalloc(&p->d_taps_int32, ntap * sizeof(float)));
-        to_float_kernel<<<(unsigned)((ntap + 255) / 256), 256, 0, p->stream>>>(p->d_taps_eval, p->d_taps_eval32, ntap);
-        to_float_kernel<<<(unsigned)((ntap + 255) / 256), 256, 0, p->stream>>>(p->d_taps_int, p->d_taps_int32, ntap);
+        CU(cudaMalloc(&p->d_taps32, ntap * sizeof(float)));
+        to_float_kernel<<<(unsigned)((ntap + 255) / 256), 256, 0, p->stream>>>(p->d_taps, p->d_taps32, ntap);
         CHECK_LAUNCH();
-        S.taps_eval32 = p->d_taps_eval32;
-        S.taps_int32 = p->d_taps_int32;
+        S.taps32 = p->d_taps32;
     }
     CU(cudaStreamSynchronize(p->stream));
     return 0;
@@ -292,10 +283,8 @@ int plan_build(cdft_plan* p)
 
 void plan_free(cdft_plan* p)
 {
-    cudaFree(p->d_taps_eval);
-    cudaFree(p->d_taps_int);
-    cudaFree(p->d_taps_eval32);
-    cudaFree(p->d_taps_int32);
+    cudaFree(p->d_taps);
+    cudaFree(p->d_taps32);
     cudaFree(p->d_vext);
     cudaFree(p->d_vec);
     cudaFree(p->d_Q);
@@ -423,6 +412,65 @@ int launch_iteration(Batch* b)
     return 0;
 }
 
+template <typename T, int NC>
+int launch_persistent_nc(Batch* b, int max_evals, size_t smem)
+{
+    auto kern = persistent_kernel<T, NC, 1>;
+    CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<b->nsys, PERS_THREADS, smem, b->stream>>>(b->d_sys, b->d_st, b->d_done, max_evals);
+    CHECK_LAUNCH();
+    g_launches += 1;
+    return 0;
+}
+
+template <typename T>
+int launch_persistent(Batch* b, int max_evals, size_t smem)
+{
+    switch (b->nc) {
+    case 1: return launch_persistent_nc<T, 1>(b, max_evals, smem);
+    case 2: return launch_persistent_nc<T, 2>(b, max_evals, smem);
+    case 3: return launch_persistent_nc<T, 3>(b, max_evals, smem);
+    case 4: return launch_persistent_nc<T, 4>(b, max_evals, smem);
+    default: return set_error(CDFT_E_UNSUPPORTED, "nc=%d", b->nc);
+    }
+}
+
+// dynamic shared memory the persistent kernel needs for the largest system of the batch
+size_t persistent_smem_need(const Batch* b)
+{
+    int nmax = 0;
+    for (auto* p : b->plans) nmax = std::max(nmax, p->N);
+    const SysDev& S = b->plans[0]->sys;
+    return pers_smem_bytes(nmax, S.nc, S.nconv, S.NF, b->mixed ? sizeof(float) : sizeof(double));
+}
+
+template <typename T, int NC>
+size_t persistent_static_smem()
+{
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, persistent_kernel<T, NC, 1>) != cudaSuccess) return 1u << 30;
+    return a.sharedSizeBytes;
+}
+
+size_t persistent_smem_limit(const Batch* b)
+{
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->plans[0]->device);
+    size_t stat = 0;
+    switch ((b->mixed ? 10 : 0) + b->nc) {
+    case 1: stat = persistent_static_smem<double, 1>(); break;
+    case 2: stat = persistent_static_smem<double, 2>(); break;
+    case 3: stat = persistent_static_smem<double, 3>(); break;
+    case 4: stat = persistent_static_smem<double, 4>(); break;
+    case 11: stat = persistent_static_smem<float, 1>(); break;
+    case 12: stat = persistent_static_smem<float, 2>(); break;
+    case 13: stat = persistent_static_smem<float, 3>(); break;
+    case 14: stat = persistent_static_smem<float, 4>(); break;
+    default: return 0;
+    }
+    return (size_t)optin > stat ? (size_t)optin - stat : 0;
+}
+
 int batch_capture(Batch* b, int iters)
 {
     if (b->graph && b->graph_iters == iters) return 0;
@@ -543,13 +591,32 @@ int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, boo
     init_kernel<<<b->nechunks, ELEM_THREADS, 0, b->stream>>>(b->d_echunks, b->d_sys);
     CHECK_LAUNCH();
     g_launches += 1;
+    bool use_persistent = false;
+    if (opts->engine == CDFT_ENGINE_AUTO || opts->engine == CDFT_ENGINE_PERSISTENT) {
+        const size_t need = persistent_smem_need(b), limit = persistent_smem_limit(b);
+        use_persistent = need <= limit;
+        if (!use_persistent && opts->engine == CDFT_ENGINE_PERSISTENT)
+            return set_error(CDFT_E_UNSUPPORTED, "persistent engine needs %zu B of shared memory per system (limit %zu)",
+                             need, limit);
+    } else if (opts->engine != CDFT_ENGINE_GRID) {
+        return set_error(CDFT_E_INVALID, "engine=%d", opts->engine);
+    }
     const int K = opts->iters_per_launch > 0 ? opts->iters_per_launch : 16;
-    rc = batch_capture(b, K);
-    if (rc) return rc;
+    if (!use_persistent) {
+        rc = batch_capture(b, K);
+        if (rc) return rc;
+    }
     const int per_iter = 3 + 2 * N_VEC_SLOTS;   // conv, phi, conv, el, ctl0, 5 vec, 4 ctl
     long long launched_evals = 0;
     bool budget_hit = false;
-    while (true) {
+    if (use_persistent) {
+        // one launch: every block runs its system's aasol loop to the end (bounded by max_evals)
+        const size_t smem = persistent_smem_need(b);
+        rc = b->mixed ? launch_persistent<float>(b, (int)std::min<long long>(max_evals, 1 << 30), smem)
+                      : launch_persistent<double>(b, (int)std::min<long long>(max_evals, 1 << 30), smem);
+        if (rc) return rc;
+    }
+    while (!use_persistent) {
         CU(cudaGraphLaunch(b->graph, b->stream));
         g_launches += (long long)K * per_iter;
         launched_evals += K;

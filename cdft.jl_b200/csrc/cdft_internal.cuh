@@ -62,10 +62,8 @@ struct SysDev {
     double cprd[CDFT_MAX_NC];    // mu_res + ln rho_bulk
     PhiParams phi;
     // tables
-    const double* taps_eval;     // [(i*nconv+f)*N + q], scaled by N_A L^3
-    const double* taps_int;      // [(i*nconv+f)*N + q], sign of the adjoint folded in
-    const float* taps_eval32;
-    const float* taps_int32;
+    const double* taps;          // [(i*nconv+f)*N + q] = Re(IDFT(omega_hat))[q]
+    const float* taps32;
     const double* vext;          // [e] or nullptr
     // work buffers
     double* rho;                 // exp(sol)

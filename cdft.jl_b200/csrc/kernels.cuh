@@ -53,11 +53,7 @@ conv1d_kernel(const ConvTask* __restrict__ tasks, const SysDev* __restrict__ sys
     const int ks = tk.tile_ks % S.ksplit;
     const int tile = tk.tile_ks / S.ksplit;
     const int slot = tk.comp * S.nconv + tk.field;
-    const T* taps;
-    if (sizeof(T) == 8)
-        taps = reinterpret_cast<const T*>(stage == 0 ? S.taps_eval : S.taps_int);
-    else
-        taps = reinterpret_cast<const T*>(stage == 0 ? S.taps_eval32 : S.taps_int32);
+    const T* taps = (sizeof(T) == 8) ? reinterpret_cast<const T*>(S.taps) : reinterpret_cast<const T*>(S.taps32);
     taps += (size_t)slot * N;
 
     const int q_lo = ks * CONV_QC;
@@ -96,10 +92,11 @@ conv1d_kernel(const ConvTask* __restrict__ tasks, const SysDev* __restrict__ sys
         }
     }
     T* out = reinterpret_cast<T*>(S.part) + ((size_t)slot * S.ksplit + ks) * N;
+    const T scale = (stage == 0) ? T(S.NA) : T(1);   // n = real(conv) * N_A L^3 (weighted_densities.jl:137)
 #pragma unroll
     for (int r = 0; r < CONV_R; ++r) {
         const int j = j0 + 32 * r;
-        if (j < N) out[j] = acc[r];
+        if (j < N) out[j] = acc[r] * scale;
     }
 }
 
@@ -199,7 +196,9 @@ __device__ __forceinline__ double dfdrho_elem(const SysDev& S, int e)
         const T* p = part + ((size_t)(i * S.nconv + f) * S.ksplit) * S.N + j;
         T acc = p[0];
         for (int ks = 1; ks < S.ksplit; ++ks) acc += p[(size_t)ks * S.N];
-        v += double(acc);
+        // scalar fields accumulate, vector fields subtract (weighted_densities.jl:160,381)
+        if (f >= 2 && f < 2 + S.nd) v -= double(acc);
+        else v += double(acc);
     }
     if (S.vext) v += S.vext[e];
     return v;
@@ -220,6 +219,9 @@ __global__ void dfdrho_out_kernel(const Chunk* __restrict__ echunks, const SysDe
 // Euler-Lagrange step + aa_point!/betafix! bookkeeping + ||res||^2 partials.
 // ---------------------------------------------------------------------------
 template <typename T>
+__device__ __forceinline__ double el_range(const SysDev& S, const AAState& A, int e0, int e1, int stride);
+
+template <typename T>
 __global__ void __launch_bounds__(ELEM_THREADS)
 el_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
           const AAState* __restrict__ st, double* __restrict__ partials)
@@ -227,70 +229,32 @@ el_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
     const Chunk c = echunks[blockIdx.x];
     if (!sys_active(st, c.sys)) return;
     const SysDev& S = sys[c.sys];
-    const AAState& A = st[c.sys];
-    const int mode = A.mode;
-    const double beta = (mode == MODE_EVAL_PICARD) ? A.picard_beta : A.beta;
-    const bool aa = (mode == MODE_EVAL_AA);
-    double* DGs = (aa && A.m > 0) ? S.DG + (size_t)A.dg_slot * S.n_elem : nullptr;
-    double ss = 0.0;
-    for (int t = threadIdx.x; t < ELEM_CHUNK; t += ELEM_THREADS) {
-        const int e = c.begin + t;
-        if (e >= S.n_elem) break;
-        const int i = e / S.N;
-        const double dF = dfdrho_elem<T>(S, e);
-        double lnG = S.cprd[i] - dF;
-        lnG = fmin(fmax(lnG, -100.0), 100.0);             // clamp!(ln_Gx, -100, 100)
-        const double s = S.sol[e];
-        const double gxn = (beta == 1.0) ? lnG : (1.0 - beta) * s + beta * lnG;  // betafix!
-        const double rn = gxn - s;
-        if (aa) {
-            const double dgv = gxn - S.gx[e];
-            const double dfv = -S.res[e] + rn;
-            S.df[e] = dfv;
-            if (DGs) DGs[e] = dgv;
-        }
-        S.res[e] = rn;
-        S.gx[e] = gxn;
-        ss += rn * rn;
-    }
-    double v[1] = {ss};
+    const int e1 = min(c.begin + ELEM_CHUNK, S.n_elem);
+    double v[1] = {el_range<T>(S, st[c.sys], c.begin + threadIdx.x, e1, ELEM_THREADS)};
     block_reduce_store<ELEM_THREADS>(v, 1, partials + (size_t)blockIdx.x * RED_SLOTS);
 }
 
 // ---------------------------------------------------------------------------
 // Vector slot operations of the Anderson step (see OP_* in cdft_internal.cuh).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(ELEM_THREADS)
-vec_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
-           const AAState* __restrict__ st, double* __restrict__ partials, int slot)
+// Applies slot operation `op` to the elements e = e0, e0 + stride, ... < e1 of
+// one system and accumulates this thread's partial sums into acc[0..K).
+// Returns K (0 for the solution updates, which reduce nothing).
+__device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AAState& A, int e0, int e1, int stride,
+                                            double* acc)
 {
-    const Chunk c = echunks[blockIdx.x];
-    const AAState& A = st[c.sys];
-    const int op = A.op[slot];
-    if (op == OP_NONE) return;
-    const SysDev& S = sys[c.sys];
     const int n = S.n_elem;
     const int m = A.m;
-    double acc[RED_SLOTS];
-#pragma unroll
-    for (int k = 0; k < RED_SLOTS; ++k) acc[k] = 0.0;
-    int K = 0;
     switch (op) {
-    case OP_NORM_DF: {
-        K = 1;
-        for (int t = threadIdx.x; t < ELEM_CHUNK; t += ELEM_THREADS) {
-            const int e = c.begin + t;
-            if (e >= n) break;
+    case OP_NORM_DF:
+        for (int e = e0; e < e1; e += stride) {
             const double v = S.df[e];
             acc[0] += v * v;
         }
-        break;
-    }
+        return 1;
     case OP_DOT_H1: {
-        K = A.kq;
-        for (int t = threadIdx.x; t < ELEM_CHUNK; t += ELEM_THREADS) {
-            const int e = c.begin + t;
-            if (e >= n) break;
+        const int K = A.kq;
+        for (int e = e0; e < e1; e += stride) {
             if (A.downdate) {   // Q[:, 1:m-1] = Q * Qx; Q[:, m] = 0  (downdate_aaqr!)
                 double row[CDFT_MAX_M];
                 for (int r = 0; r < m; ++r) row[r] = S.Q[(size_t)r * n + e];
@@ -304,15 +268,12 @@ vec_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
             const double dv = S.df[e];
             for (int cc = 0; cc < K; ++cc) acc[cc] += S.Q[(size_t)cc * n + e] * dv;
         }
-        break;
+        return K;
     }
     case OP_SUB_DOT:
     case OP_SUB_NORM: {
         const int kq = A.kq;
-        K = (op == OP_SUB_DOT) ? kq : 1;
-        for (int t = threadIdx.x; t < ELEM_CHUNK; t += ELEM_THREADS) {
-            const int e = c.begin + t;
-            if (e >= n) break;
+        for (int e = e0; e < e1; e += stride) {
             double v = S.df[e];
             for (int cc = 0; cc < kq; ++cc) v += (-A.coef[cc]) * S.Q[(size_t)cc * n + e];  // gemv, alpha=-1
             S.df[e] = v;
@@ -322,27 +283,23 @@ vec_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
                 acc[0] += v * v;
             }
         }
-        break;
+        return (op == OP_SUB_DOT) ? kq : 1;
     }
     case OP_SETQ_DOT_TRES: {
         const int kq = A.kq;
-        K = A.mk;
+        const int K = A.mk;
         const double r = A.rnorm;
-        for (int t = threadIdx.x; t < ELEM_CHUNK; t += ELEM_THREADS) {
-            const int e = c.begin + t;
-            if (e >= n) break;
+        for (int e = e0; e < e1; e += stride) {
             const double q = S.df[e] / r;
             S.Q[(size_t)kq * n + e] = q;
             const double rv = S.res[e];
             for (int cc = 0; cc < K; ++cc) acc[cc] += S.Q[(size_t)cc * n + e] * rv;
         }
-        break;
+        return K;
     }
     case OP_SOL_AA: {
         const int mk = A.mk;
-        for (int t = threadIdx.x; t < ELEM_CHUNK; t += ELEM_THREADS) {
-            const int e = c.begin + t;
-            if (e >= n) break;
+        for (int e = e0; e < e1; e += stride) {
             double v = S.gx[e];
             for (int cc = 0; cc < mk; ++cc) {
                 const int slotc = (A.head + cc) % m;
@@ -351,22 +308,69 @@ vec_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
             S.sol[e] = v;
             S.rho[e] = exp(v);
         }
-        return;
+        return 0;
     }
-    case OP_SOL_COPY: {
-        for (int t = threadIdx.x; t < ELEM_CHUNK; t += ELEM_THREADS) {
-            const int e = c.begin + t;
-            if (e >= n) break;
+    case OP_SOL_COPY:
+        for (int e = e0; e < e1; e += stride) {
             const double v = S.gx[e];
             S.sol[e] = v;
             S.rho[e] = exp(v);
         }
-        return;
-    }
+        return 0;
     default:
-        return;
+        return 0;
     }
+}
+
+__global__ void __launch_bounds__(ELEM_THREADS)
+vec_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
+           const AAState* __restrict__ st, double* __restrict__ partials, int slot)
+{
+    const Chunk c = echunks[blockIdx.x];
+    const AAState& A = st[c.sys];
+    const int op = A.op[slot];
+    if (op == OP_NONE) return;
+    const SysDev& S = sys[c.sys];
+    double acc[RED_SLOTS];
+#pragma unroll
+    for (int k = 0; k < RED_SLOTS; ++k) acc[k] = 0.0;
+    const int e1 = min(c.begin + ELEM_CHUNK, S.n_elem);
+    const int K = vec_op_range(op, S, A, c.begin + threadIdx.x, e1, ELEM_THREADS, acc);
+    if (K == 0) return;   // block-uniform
     block_reduce_store<ELEM_THREADS>(acc, K, partials + (size_t)blockIdx.x * RED_SLOTS);
+}
+
+// Euler-Lagrange step on a range of elements: ln G = mu - dF/drho, clamp, betafix!,
+// aa_point! bookkeeping; returns this thread's sum of res^2.
+// One element of the Euler-Lagrange step given dF/drho + Vext; returns res^2.
+__device__ __forceinline__ double el_elem(const SysDev& S, int e, int i, double dF, double beta, bool aa, double* DGs)
+{
+    double lnG = S.cprd[i] - dF;
+    lnG = fmin(fmax(lnG, -100.0), 100.0);             // clamp!(ln_Gx, -100, 100)
+    const double s = S.sol[e];
+    const double gxn = (beta == 1.0) ? lnG : (1.0 - beta) * s + beta * lnG;  // betafix!
+    const double rn = gxn - s;
+    if (aa) {                                          // aa_point!: dg = G_new - G_old, df = res_new - res_old
+        const double dgv = gxn - S.gx[e];
+        const double dfv = -S.res[e] + rn;
+        S.df[e] = dfv;
+        if (DGs) DGs[e] = dgv;
+    }
+    S.res[e] = rn;
+    S.gx[e] = gxn;
+    return rn * rn;
+}
+
+template <typename T>
+__device__ __forceinline__ double el_range(const SysDev& S, const AAState& A, int e0, int e1, int stride)
+{
+    const int mode = A.mode;
+    const double beta = (mode == MODE_EVAL_PICARD) ? A.picard_beta : A.beta;
+    const bool aa = (mode == MODE_EVAL_AA);
+    double* DGs = (aa && A.m > 0) ? S.DG + (size_t)A.dg_slot * S.n_elem : nullptr;
+    double ss = 0.0;
+    for (int e = e0; e < e1; e += stride) ss += el_elem(S, e, e / S.N, dfdrho_elem<T>(S, e), beta, aa, DGs);
+    return ss;
 }
 
 // ---------------------------------------------------------------------------
@@ -523,42 +527,21 @@ __device__ void aa_after_eval(AAState& A, double r, int* done_counter)
     }
 }
 
-__global__ void ctl_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, const double* __restrict__ partials,
-                           int nsys, int slot_done, int* done_counter)
+// Number of partial sums that slot operation `op` produced (-1 = the EL stage).
+__device__ __forceinline__ int ctl_nsums(const AAState& A, int op)
 {
-    const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp_global >= nsys) return;
-    const int s = warp_global;
-    AAState& A = st[s];
-    const SysDev& S = sys[s];
-    if (A.mode == MODE_DONE) {
-        if (slot_done == 0 && lane == 0)
-            for (int k = 1; k <= N_VEC_SLOTS; ++k) A.op[k] = OP_NONE;
-        return;
-    }
-    int op = (slot_done == 0) ? -1 : A.op[slot_done];
-    if (op == OP_NONE || op == OP_SOL_AA || op == OP_SOL_COPY) return;
-    int K;
     switch (op) {
-    case -1: case OP_NORM_DF: case OP_SUB_NORM: K = 1; break;
-    case OP_DOT_H1: case OP_SUB_DOT: K = A.kq; break;
-    case OP_SETQ_DOT_TRES: K = A.mk; break;
-    default: K = 0;
+    case -1: case OP_NORM_DF: case OP_SUB_NORM: return 1;
+    case OP_DOT_H1: case OP_SUB_DOT: return A.kq;
+    case OP_SETQ_DOT_TRES: return A.mk;
+    default: return 0;
     }
-    double sums[RED_SLOTS];
-    for (int k = 0; k < RED_SLOTS; ++k) sums[k] = 0.0;
-    for (int ch = lane; ch < S.chunk_count; ch += 32) {
-        const double* p = partials + (size_t)(S.chunk_begin + ch) * RED_SLOTS;
-        for (int k = 0; k < K; ++k) sums[k] += p[k];
-    }
-    for (int k = 0; k < K; ++k) {
-        double v = sums[k];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        sums[k] = v;
-    }
-    if (lane != 0) return;
+}
+
+// Finish slot `slot_done` (0 = EL) of a system given its reduced sums; sets the
+// operation of the next slot.  One thread.
+__device__ void ctl_apply(AAState& A, int op, int slot_done, const double* sums, int* done_counter)
+{
     const int next = slot_done + 1;
     switch (op) {
     case -1:
@@ -611,6 +594,39 @@ __global__ void ctl_kernel(const SysDev* __restrict__ sys, AAState* __restrict__
     }
 }
 
+__global__ void ctl_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, const double* __restrict__ partials,
+                           int nsys, int slot_done, int* done_counter)
+{
+    const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp_global >= nsys) return;
+    const int s = warp_global;
+    AAState& A = st[s];
+    const SysDev& S = sys[s];
+    if (A.mode == MODE_DONE) {
+        if (slot_done == 0 && lane == 0)
+            for (int k = 1; k <= N_VEC_SLOTS; ++k) A.op[k] = OP_NONE;
+        return;
+    }
+    const int op = (slot_done == 0) ? -1 : A.op[slot_done];
+    if (op == OP_NONE || op == OP_SOL_AA || op == OP_SOL_COPY) return;
+    const int K = ctl_nsums(A, op);
+    double sums[RED_SLOTS];
+    for (int k = 0; k < RED_SLOTS; ++k) sums[k] = 0.0;
+    for (int ch = lane; ch < S.chunk_count; ch += 32) {
+        const double* p = partials + (size_t)(S.chunk_begin + ch) * RED_SLOTS;
+        for (int k = 0; k < K; ++k) sums[k] += p[k];
+    }
+    for (int k = 0; k < K; ++k) {
+        double v = sums[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        sums[k] = v;
+    }
+    if (lane != 0) return;
+    ctl_apply(A, op, slot_done, sums, done_counter);
+}
+
 // initial iterate: sol = log(rho0); rho = exp(sol)   (converge.jl:244, GFix! :236)
 __global__ void init_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys)
 {
@@ -645,9 +661,7 @@ __device__ __forceinline__ double kernel_hat_1d(int type, double w, double R, in
     return 4.0 * PI * w / (wb * wb * wb) * (sin(wb * R) - R * wb * cos(wb * R)) / (TWO_PI * TWO_PI * TWO_PI);
 }
 
-__global__ void taps1d_kernel(int N, double span, double L, int type, double width_red,
-                              double scale_eval, double sign_int,
-                              double* __restrict__ taps_eval, double* __restrict__ taps_int)
+__global__ void taps1d_kernel(int N, double span, double L, int type, double width_red, double* __restrict__ taps)
 {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= N) return;
@@ -663,9 +677,7 @@ __global__ void taps1d_kernel(int N, double span, double L, int type, double wid
         const double K = kernel_hat_1d(type, w, R, 0);
         acc += (type == 3) ? -K * sn : K * cs;
     }
-    const double t = acc / (double)N;
-    taps_eval[q] = t * scale_eval;
-    taps_int[q] = t * sign_int;
+    taps[q] = acc / (double)N;
 }
 
 __global__ void to_float_kernel(const double* __restrict__ a, float* __restrict__ b, size_t n)

@@ -93,8 +93,14 @@ typedef struct {
     int picard_maxit;
     double picard_beta, picard_rtol, picard_atol;
     double time_budget_s;  /* host wall-clock cap for the whole call, <= 0: none */
-    int iters_per_launch;  /* fixed-point evaluations per CUDA-graph launch, <= 0: default */
+    int iters_per_launch;  /* fixed-point evaluations per CUDA-graph launch (grid engine), <= 0: default */
+    int engine;            /* CDFT_ENGINE_* */
 } cdft_solver_opts;
+
+/* execution engines of cdft_converge / cdft_batch_converge */
+#define CDFT_ENGINE_AUTO 0        /* persistent when every system fits one CTA's shared memory */
+#define CDFT_ENGINE_GRID 1        /* per-stage kernels over all systems, CUDA-graph iterations */
+#define CDFT_ENGINE_PERSISTENT 2  /* one CTA per system runs the whole aasol loop, one launch */
 
 /* The (idid, errcode, history) part of aasol's output (anderson.jl:81-103,727-757). */
 typedef struct {

@@ -52,7 +52,7 @@ def test_struct_layout_matches_header(tmp_path):
 int main(void) {{
   printf("%zu %zu %zu %zu\\n", sizeof(cdft_system_desc), sizeof(cdft_solver_opts), sizeof(cdft_result), sizeof(cdft_assoc_pair));
   printf("%zu %zu %zu %zu %zu\\n", offsetof(cdft_system_desc, vext), offsetof(cdft_system_desc, precision),
-         offsetof(cdft_system_desc, mu_res_plus_ln_rhob), offsetof(cdft_solver_opts, iters_per_launch),
+         offsetof(cdft_system_desc, mu_res_plus_ln_rhob), offsetof(cdft_solver_opts, engine),
          offsetof(cdft_result, history_len));
   return 0;
 }}
@@ -65,5 +65,5 @@ int main(void) {{
     assert sizes == [ctypes.sizeof(_lib.SystemDesc), ctypes.sizeof(_lib.SolverOpts), ctypes.sizeof(_lib.Result),
                      ctypes.sizeof(_lib.AssocPair)]
     assert offs == [_lib.SystemDesc.vext.offset, _lib.SystemDesc.precision.offset,
-                    _lib.SystemDesc.mu_res_plus_ln_rhob.offset, _lib.SolverOpts.iters_per_launch.offset,
+                    _lib.SystemDesc.mu_res_plus_ln_rhob.offset, _lib.SolverOpts.engine.offset,
                     _lib.Result.history_len.offset]
