@@ -62,8 +62,8 @@ const double kPCSAFT_B[21] = {
     26.855641363, 192.67226447, -38.804430052, 206.55133841, -161.82646165, 93.626774077,
     -355.60235612, -165.20769346, -29.666905585};
 
-std::once_flag g_const_once;
-int g_const_status = 0;
+std::mutex g_const_mu;
+bool g_const_done[64] = {false};   // per device: PC-SAFT constants uploaded to its __constant__ bank
 
 }  // namespace
 
@@ -115,14 +115,17 @@ namespace {
 std::mutex g_batch_mu;
 std::map<std::vector<cdft_plan*>, Batch*> g_batches;
 
+// Upload the dispersion constants to the __constant__ bank of the current device (once per device).
 int upload_constants()
 {
-    std::call_once(g_const_once, []() {
-        if (cudaMemcpyToSymbol(c_pcsaft_a, kPCSAFT_A, sizeof(kPCSAFT_A)) != cudaSuccess ||
-            cudaMemcpyToSymbol(c_pcsaft_b, kPCSAFT_B, sizeof(kPCSAFT_B)) != cudaSuccess)
-            g_const_status = 1;
-    });
-    if (g_const_status) return set_error(CDFT_E_CUDA, "uploading PC-SAFT constants failed");
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(CDFT_E_UNSUPPORTED, "device ordinal %d", dev);
+    std::lock_guard<std::mutex> lk(g_const_mu);
+    if (g_const_done[dev]) return 0;
+    CU(cudaMemcpyToSymbol(c_pcsaft_a, kPCSAFT_A, sizeof(kPCSAFT_A)));
+    CU(cudaMemcpyToSymbol(c_pcsaft_b, kPCSAFT_B, sizeof(kPCSAFT_B)));
+    g_const_done[dev] = true;
     return 0;
 }
 
