@@ -21,6 +21,8 @@ E_BUDGET = -4
 
 COORD_CART, COORD_SPH, COORD_CYL = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
+NOALLOC_MAX_N = 4096
+NOALLOC_MAX_ELEM = 8192
 ENGINE_AUTO, ENGINE_GRID, ENGINE_PERSISTENT = 0, 1, 2
 
 LIB_NAME = "libcdft_b200.so"
@@ -33,7 +35,7 @@ EXPORTED = [
     "cdft_free_energy_res", "cdft_phi_pointwise",
     "cdft_converge", "cdft_converge_dev",
     "cdft_batch_converge", "cdft_batch_converge_dev",
-    "cdft_plan_set_stream", "cdft_batch_time_stage",
+    "cdft_plan_set_stream", "cdft_batch_time_stage", "cdft_functional_derivative_noalloc",
     "cdft_launch_count", "cdft_last_error", "cdft_version",
 ]
 
@@ -123,6 +125,7 @@ def load(path=LIB_PATH):
                                             ctypes.POINTER(SolverOpts), ctypes.POINTER(Result)]
     lib.cdft_plan_set_stream.argtypes = [P, P]
     lib.cdft_batch_time_stage.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
+    lib.cdft_functional_derivative_noalloc.argtypes = [ctypes.POINTER(SystemDesc), P, P, P]
     lib.cdft_launch_count.argtypes = [ctypes.c_int]
     lib.cdft_launch_count.restype = ctypes.c_longlong
     lib.cdft_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]

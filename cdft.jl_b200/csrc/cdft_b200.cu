@@ -968,3 +968,177 @@ int cdft_last_error(char* buf, size_t len)
 const char* cdft_version(void) { return "cdft_b200 0.1 (sm_100a)"; }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free functional derivative (cdft_functional_derivative_noalloc).
+//
+// For callers that cannot call cudaMalloc (see the header).  The scratch is a
+// file-scope device array; host code never dereferences its name (in host code
+// it is only a stand-in for the symbol): the device address is obtained once
+// per device with cudaGetSymbolAddress and handed to the kernels.
+// ===========================================================================
+static __device__ __align__(256) double g_noalloc_scratch[CDFT_NOALLOC_SCRATCH_BYTES / sizeof(double)];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[64] = {nullptr};
+
+// device address of the scratch array on the current device (looked up on first use)
+int noalloc_scratch_addr(double** out)
+{
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(CDFT_E_UNSUPPORTED, "device ordinal %d", dev);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        CU(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_addr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return 0;
+}
+
+size_t noalloc_align(size_t n) { return (n + 31) & ~size_t(31); }   // 256-byte steps, in doubles
+
+}  // namespace
+
+extern "C" int cdft_functional_derivative_noalloc(const cdft_system_desc* desc, const double* d_rho, double* d_dFdrho,
+                                                  void* stream_ptr)
+{
+    g_err_code = 0;
+    if (!d_rho || !d_dFdrho) return set_error(CDFT_E_INVALID, "NULL device array");
+    int rc = validate_desc(desc);
+    if (rc) return rc;
+    const cdft_system_desc& d = *desc;
+    if (d.precision != CDFT_PREC_FP64)
+        return set_error(CDFT_E_UNSUPPORTED, "the allocation-free entry point computes in FP64 only");
+    const int N = d.ngrid[0], nc = d.nc;
+    if (N > CDFT_NOALLOC_MAX_N || (long long)N * nc > CDFT_NOALLOC_MAX_ELEM)
+        return set_error(CDFT_E_UNSUPPORTED,
+                         "system too large for the allocation-free scratch: N=%d nc=%d (limits N<=%d, N*nc<=%d)",
+                         N, nc, CDFT_NOALLOC_MAX_N, CDFT_NOALLOC_MAX_ELEM);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    rc = upload_constants();
+    if (rc) return rc;
+    double* base = nullptr;
+    rc = noalloc_scratch_addr(&base);
+    if (rc) return rc;
+
+    // system record (reduced parameters as in plan creation), pointers into the scratch
+    SysDev S;
+    memset(&S, 0, sizeof(S));
+    S.nd = 1;
+    S.N = N;
+    S.nc = nc;
+    S.NF = 7;
+    S.nconv = 6;
+    S.ngrid[0] = N; S.ngrid[1] = 1; S.ngrid[2] = 1;
+    S.ksplit = (N + CONV_QC - 1) / CONV_QC;
+    S.n_elem = N * nc;
+    const double L = d.L, T = d.T;
+    S.NA = kNA * L * L * L;
+    for (int i = 0; i < nc; ++i) S.cprd[i] = d.mu_res_plus_ln_rhob[i];
+    PhiParams& P = S.phi;
+    P.nc = nc;
+    P.nd = 1;
+    P.T = T;
+    for (int i = 0; i < nc; ++i) {
+        P.m[i] = d.m[i];
+        P.d[i] = d.hsd[i] / L;
+    }
+    for (int i = 0; i < nc; ++i)
+        for (int j = 0; j < nc; ++j) {
+            const double sg = d.sigma[i * nc + j] / L;
+            const double e = d.eps[i * nc + j];
+            const double c1 = d.m[i] * d.m[j] * sg * sg * sg * e / T;
+            P.c1[i * CDFT_MAX_NC + j] = c1;
+            P.c2[i * CDFT_MAX_NC + j] = c1 * e / T;
+        }
+    P.has_assoc = d.n_assoc;
+    if (d.n_assoc) {
+        const cdft_assoc_pair& a = d.assoc[0];
+        P.a_ic = a.icomp;
+        P.a_jc = a.jcomp;
+        P.a_nia = a.n_ia;
+        P.a_njb = a.n_jb;
+        const double di = P.d[a.icomp], dj = P.d[a.jcomp];
+        P.a_dij = di * dj / (di + dj);
+        const double sg = d.sigma[a.icomp * nc + a.jcomp] / L;
+        P.a_K = sg * sg * sg * (exp(a.eps_ab / T) - 1.0) * a.kappa_ab;
+    }
+
+    // task and chunk lists on the host stack (bounded by the size limits)
+    ConvTask tasks[1024];
+    Chunk pch[(CDFT_NOALLOC_MAX_N + POINT_THREADS - 1) / POINT_THREADS];
+    Chunk ech[(CDFT_NOALLOC_MAX_ELEM + ELEM_CHUNK - 1) / ELEM_CHUNK];
+    int ntasks = 0, npch = 0, nech = 0;
+    const int tiles = (N + CONV_TILE - 1) / CONV_TILE;
+    for (int i = 0; i < nc; ++i)
+        for (int f = 0; f < S.nconv; ++f)
+            for (int t = 0; t < tiles; ++t)
+                for (int ks = 0; ks < S.ksplit; ++ks) {
+                    if (ntasks >= 1024) return set_error(CDFT_E_UNSUPPORTED, "task list overflow");
+                    tasks[ntasks++] = {0, i, f, t * S.ksplit + ks};
+                }
+    for (int j = 0; j < N; j += POINT_THREADS) pch[npch++] = {0, j};
+    for (int e = 0; e < S.n_elem; e += ELEM_CHUNK) ech[nech++] = {0, e};
+
+    // scratch layout (offsets in doubles, 256-byte aligned)
+    size_t off = 0;
+    const size_t o_sys = off;   off += noalloc_align((sizeof(SysDev) + 7) / 8);
+    const size_t o_task = off;  off += noalloc_align((sizeof(ConvTask) * ntasks + 7) / 8);
+    const size_t o_pch = off;   off += noalloc_align((sizeof(Chunk) * npch + 7) / 8);
+    const size_t o_ech = off;   off += noalloc_align((sizeof(Chunk) * nech + 7) / 8);
+    const size_t ntap = (size_t)S.nconv * nc * N;
+    const size_t o_taps = off;  off += noalloc_align(ntap);
+    const size_t o_part = off;  off += noalloc_align(ntap * S.ksplit);
+    const size_t o_df = off;    off += noalloc_align((size_t)S.NF * nc * N);
+    const size_t o_fval = off;  off += noalloc_align((size_t)N);
+    const size_t o_vext = off;  off += d.vext ? noalloc_align((size_t)S.n_elem) : 0;
+    if (off * sizeof(double) > CDFT_NOALLOC_SCRATCH_BYTES)
+        return set_error(CDFT_E_UNSUPPORTED, "scratch of %zu B exceeds %u B", off * sizeof(double),
+                         (unsigned)CDFT_NOALLOC_SCRATCH_BYTES);
+    S.taps = base + o_taps;
+    S.part = base + o_part;
+    S.dfield = base + o_df;
+    S.fval = base + o_fval;
+    S.vext = d.vext ? base + o_vext : nullptr;
+    S.rho = const_cast<double*>(d_rho);   // read only by the kernels below
+    S.out = d_dFdrho;
+    SysDev* d_sys = reinterpret_cast<SysDev*>(base + o_sys);
+    ConvTask* d_tasks = reinterpret_cast<ConvTask*>(base + o_task);
+    Chunk* d_pch = reinterpret_cast<Chunk*>(base + o_pch);
+    Chunk* d_ech = reinterpret_cast<Chunk*>(base + o_ech);
+    CU(cudaMemcpyAsync(d_sys, &S, sizeof(SysDev), cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(d_tasks, tasks, sizeof(ConvTask) * ntasks, cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(d_pch, pch, sizeof(Chunk) * npch, cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(d_ech, ech, sizeof(Chunk) * nech, cudaMemcpyHostToDevice, stream));
+    if (d.vext)
+        CU(cudaMemcpyAsync(base + o_vext, d.vext, sizeof(double) * S.n_elem, cudaMemcpyHostToDevice, stream));
+
+    // kernels of get_fields(::PCSAFTModel) in 1D (PCSAFT.jl:55-61), same tables as plan creation
+    const int types[6] = {1, 2, 3, 2, 1, 2};
+    const double wf[6] = {0.5, 0.5, 0.5, 1.0, 1.0, PSI_DISP};
+    const double span = d.bounds[0][1] - d.bounds[0][0];
+    for (int i = 0; i < nc; ++i)
+        for (int f = 0; f < S.nconv; ++f)
+            taps1d_kernel<<<(N + 127) / 128, 128, 0, stream>>>(N, span, L, types[f], wf[f] * P.d[i],
+                                                             base + o_taps + ((size_t)i * S.nconv + f) * N);
+    CHECK_LAUNCH();
+    const size_t smem = (size_t)(CONV_QC + CONV_TILE + CONV_QC + 31) * sizeof(double);
+    conv1d_kernel<double><<<ntasks, CONV_WARPS * 32, smem, stream>>>(d_tasks, d_sys, nullptr, 0);
+    switch (nc) {
+    case 1: phi_kernel<double, 1, 1><<<npch, POINT_THREADS, 0, stream>>>(d_pch, d_sys, nullptr); break;
+    case 2: phi_kernel<double, 2, 1><<<npch, POINT_THREADS, 0, stream>>>(d_pch, d_sys, nullptr); break;
+    case 3: phi_kernel<double, 3, 1><<<npch, POINT_THREADS, 0, stream>>>(d_pch, d_sys, nullptr); break;
+    default: phi_kernel<double, 4, 1><<<npch, POINT_THREADS, 0, stream>>>(d_pch, d_sys, nullptr); break;
+    }
+    conv1d_kernel<double><<<ntasks, CONV_WARPS * 32, smem, stream>>>(d_tasks, d_sys, nullptr, 1);
+    dfdrho_out_kernel<double><<<nech, ELEM_THREADS, 0, stream>>>(d_ech, d_sys);
+    CHECK_LAUNCH();
+    g_launches += 4 + (long long)nc * S.nconv;
+    CU(cudaStreamSynchronize(stream));
+    return 0;
+}

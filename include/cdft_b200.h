@@ -174,6 +174,34 @@ int cdft_plan_set_stream(cdft_plan* plan, void* stream);
  * Instrumentation for roofline accounting; no reference counterpart. */
 int cdft_batch_time_stage(cdft_plan* const* plans, int nplans, int stage, int reps, double* ms_per_launch);
 
+/* dF/drho (residual functional derivative plus external field) computed
+ * without allocating any device memory.  No counterpart in the reference: it
+ * exists for callers that cannot call cudaMalloc -- hosts whose device memory
+ * is owned entirely by a memory pool or caching allocator that must see every
+ * allocation (a CUDA.jl or PyTorch process running at its pool limit), or
+ * services that reserve their whole device budget at start-up and forbid
+ * allocations afterwards.  It takes no plan (plan creation allocates): the
+ * system comes as a descriptor, d_rho and d_dFdrho are caller-owned device
+ * arrays of N*nc doubles, desc->vext is a host array or NULL, stream is a
+ * cudaStream_t or NULL for the default stream; the call returns after the
+ * stream has finished its work.
+ *
+ * Scratch (kernel tables, weighted densities, partial sums) lives in one
+ * fixed array of CDFT_NOALLOC_SCRATCH_BYTES inside the library, which every
+ * GPU that loads the library holds until the process exits.  Limits: 1D
+ * Cartesian, FP64, N <= CDFT_NOALLOC_MAX_N and N*nc <= CDFT_NOALLOC_MAX_ELEM;
+ * larger systems are rejected with CDFT_E_UNSUPPORTED.  The first call on a
+ * device looks up the array's device address (once per device); make that
+ * first call before any stream capture.  All calls share the one array, so
+ * calls that overlap on the GPU (from two host threads or two streams) race
+ * and must be serialised by the caller.  Every value a call reads from the
+ * array is written earlier in the same call, so no clearing is needed. */
+#define CDFT_NOALLOC_SCRATCH_BYTES (4u * 1024u * 1024u)
+#define CDFT_NOALLOC_MAX_N 4096
+#define CDFT_NOALLOC_MAX_ELEM 8192
+int cdft_functional_derivative_noalloc(const cdft_system_desc* desc, const double* d_rho, double* d_dFdrho,
+                                       void* stream);
+
 /* Number of our kernel launches issued by the calling thread since the last
  * reset (instrumentation for benchmarks). */
 long long cdft_launch_count(int reset);
