@@ -200,13 +200,23 @@ def run_ours(args, rank, world, local_rank):
     errc = [results[i].errcode for i in range(n)]
     ms_e2e = timed(step_e2e, max(1, args.steps), 1)
 
-    # dominant kernel: the weighted-density circulant convolution (stage 0), timed alone
+    rho_out = [t.cpu().numpy() for t in work_dev]
+    accuracy = None
+    if args.precision == "mixed" and rank == 0:
+        accuracy = mixed_accuracy(specs, systems, rho_out, method)
+
+    # convolution stage alone (one launch covering all systems), timed with CUDA events
     ms_conv = ctypes.c_double()
     _lib.check(lib.cdft_batch_time_stage(plans, n, 0, 200, ctypes.byref(ms_conv)))
     ms_phi = ctypes.c_double()
     _lib.check(lib.cdft_batch_time_stage(plans, n, 1, 200, ctypes.byref(ms_phi)))
     flops_conv = sum(2.0 * s.nc * 6 * s.ngrid[0] ** 2 for s in systems)
-    achieved = flops_conv / (ms_conv.value * 1e-3) / 1e12
+    conv_tflops = flops_conv / (ms_conv.value * 1e-3) / 1e12
+    # the dominant kernel of a step: the persistent converge kernel (one launch per step) or,
+    # in the grid engine, the convolutions; algorithmic work = 2 convolution stages per evaluation
+    step_flops = sum(2.0 * 2.0 * s.nc * 6 * s.ngrid[0] ** 2 * ev for s, ev in zip(systems, iters))
+    achieved = step_flops / (ms_dev * 1e-3) / 1e12
+    plain = plain_fp64_gpu(specs) if (rank == 0 and args.plain) else None
     total_units = n * world
     value = total_units / (ms_dev * 1e-3)
     h2d = sum(r.nbytes for r in rho0)
@@ -237,26 +247,64 @@ def run_ours(args, rank, world, local_rank):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
             "gpu_launches": launches_timed,
             "roofline": {
-                "kernel": "conv1d_kernel<double> (weighted densities, 64 systems per launch)",
-                "bound": "fp64",
+                "kernel": ("persistent_kernel (whole batched converge, 1 launch per step)" if args.engine != "grid"
+                           else "grid engine (14 launches per evaluation)"),
+                "bound": "fp64" if args.precision == "fp64" else "fp32/fp64",
                 "achieved": round(achieved, 3),
                 "peak": FP64_PEAK_NOMINAL_TFLOPS,
                 "peak_source": "nominal B200 FP64 (MEASURED_PEAKS.json has no FP64 figure)",
                 "unit": "TFLOP/s",
                 "frac": round(achieved / FP64_PEAK_NOMINAL_TFLOPS, 4),
                 "traffic": None,
-                "ms_per_launch": round(ms_conv.value, 5),
-                "phi_ms_per_launch": round(ms_phi.value, 5),
-                "algorithmic_flops_per_launch": flops_conv,
+                "algorithmic_flops_per_launch": step_flops,
+                "stage_conv1d": {"ms_per_launch": round(ms_conv.value, 5), "tflops": round(conv_tflops, 3),
+                                 "algorithmic_flops_per_launch": flops_conv},
+                "stage_phi_ms_per_launch": round(ms_phi.value, 5),
             },
             "clocks": clk.summary(),
         }
+    if rank == 0 and accuracy is not None:
+        line["accuracy_vs_fp64"] = accuracy
+    if rank == 0 and plain is not None:
+        line["plain_fp64_gpu_path"] = plain
     if args.cpu_baseline and rank == 0:
         line["cpu_baseline"] = cpu_baseline(specs, budget_s=args.cpu_budget)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return line
+
+
+def mixed_accuracy(specs, systems_mixed, rho_mixed, method):
+    """Errors of the mixed-precision results against an FP64 batch of the same systems."""
+    import cdft_b200 as cd
+    s64, r64 = build_systems(specs, "fp64")
+    cd.batch_converge(s64, r64, method=method)
+    e_rho = max(float(np.max(np.abs(a / b - 1))) for a, b in zip(rho_mixed, r64))
+    e_ads = max(abs(cd.adsorption(a, ra)[0] / cd.adsorption(b, rb)[0] - 1)
+                for a, ra, b, rb in zip(systems_mixed, rho_mixed, s64, r64))
+    e_gam = max(abs(cd.surface_tension(a, ra) / cd.surface_tension(b, rb) - 1)
+                for a, ra, b, rb in zip(systems_mixed, rho_mixed, s64, r64))
+    return {"rho_rel_err_max": e_rho, "adsorption_rel_err_max": e_ads,
+            "surface_grand_potential_rel_err_max": e_gam}
+
+
+def plain_fp64_gpu(specs):
+    """The plain FP64 GPU path: the same 64 systems converged one converge! call at a
+    time with per-stage kernels (the reference's CUDA path structure), wall time."""
+    import torch
+    import cdft_b200 as cd
+    s64, r64 = build_systems(specs, "fp64")
+    method = cd.AASol.for_system(None, **SOLVER)
+    for s, r in zip(s64[:2], r64[:2]):   # warm-up (graph capture)
+        cd.converge(s, r.copy(), method=method, engine="grid")
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for s, r in zip(s64, r64):
+        cd.converge(s, r.copy(), method=method, engine="grid", keep_history=False)
+    dt = time.perf_counter() - t
+    return {"ms": round(dt * 1e3, 2), "value": round(len(s64) / dt, 3), "unit": "state points/s",
+            "how": "64 sequential cdft_converge calls, FP64, grid engine, host wall clock"}
 
 
 def _oracle_converge_one(spec):
@@ -350,6 +398,7 @@ def main():
     ap.add_argument("--engine", default="auto", choices=["auto", "grid", "persistent"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-plain", dest="plain", action="store_false", help="skip the sequential FP64 comparison")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

@@ -250,7 +250,7 @@ class AASol:
         return cls(anderson_m, maxit=maxit, rtol=tol, atol=tol, beta=beta, picard_maxit=maxit, picard_beta=beta,
                    picard_rtol=anderson_start, picard_atol=anderson_start, verbose=verbose)
 
-    def c_opts(self, time_budget_s=0.0, iters_per_launch=0, engine="auto"):
+    def c_opts(self, time_budget_s=0.0, iters_per_launch=0, engine="auto", mixed_switch_rtol=0.0):
         o = _lib.SolverOpts()
         o.m, o.maxit, o.rtol, o.atol, o.beta = self.m, self.maxit, self.rtol, self.atol, self.beta
         o.picard_maxit, o.picard_beta = self.picard_maxit, self.picard_beta
@@ -258,6 +258,7 @@ class AASol:
         o.time_budget_s = time_budget_s
         o.iters_per_launch = iters_per_launch
         o.engine = {"auto": _lib.ENGINE_AUTO, "grid": _lib.ENGINE_GRID, "persistent": _lib.ENGINE_PERSISTENT}[engine]
+        o.mixed_switch_rtol = mixed_switch_rtol
         return o
 
 
@@ -284,7 +285,7 @@ def _check_rho(system, rho):
 
 
 def converge(system, rho, method=None, time_budget_s=0.0, iters_per_launch=0, keep_history=True, engine="auto",
-             **kwargs):
+             mixed_switch_rtol=0.0, **kwargs):
     """converge!(system, ρ; kwargs...) / converge!(system, ρ, solver): converges
     ``rho`` in place (converge.jl:214-254) and returns the aasol status.
     ``engine``: "auto", "grid" (per-stage kernels) or "persistent" (one CTA per system)."""
@@ -293,11 +294,11 @@ def converge(system, rho, method=None, time_budget_s=0.0, iters_per_launch=0, ke
     res = _lib.Result()
     hist = None
     if keep_history:
-        cap = method.maxit + 2 * method.picard_maxit + 4
+        cap = 2 * (method.maxit + 2 * method.picard_maxit + 4)
         hist = np.zeros(cap)
         res.history = _lib.dptr(hist)
         res.history_cap = cap
-    opts = method.c_opts(time_budget_s, iters_per_launch, engine)
+    opts = method.c_opts(time_budget_s, iters_per_launch, engine, mixed_switch_rtol)
     _lib.check(_LIB.cdft_converge(system._plan, _lib.dptr(rho), ctypes.byref(opts), ctypes.byref(res)))
     out = ConvergeResult(res, None if hist is None else hist[: res.history_len].copy())
     if method.verbose:
@@ -306,7 +307,8 @@ def converge(system, rho, method=None, time_budget_s=0.0, iters_per_launch=0, ke
     return out
 
 
-def batch_converge(systems, rhos, method=None, time_budget_s=0.0, iters_per_launch=0, engine="auto", **kwargs):
+def batch_converge(systems, rhos, method=None, time_budget_s=0.0, iters_per_launch=0, engine="auto",
+                   mixed_switch_rtol=0.0, **kwargs):
     """Converge many independent systems (state points, pore widths) together."""
     n = len(systems)
     if n != len(rhos):
@@ -317,7 +319,7 @@ def batch_converge(systems, rhos, method=None, time_budget_s=0.0, iters_per_laun
     plans = (ctypes.c_void_p * n)(*[s._plan.value for s in systems])
     ptrs = (ctypes.POINTER(ctypes.c_double) * n)(*[_lib.dptr(r) for r in rhos])
     res = (_lib.Result * n)()
-    opts = method.c_opts(time_budget_s, iters_per_launch, engine)
+    opts = method.c_opts(time_budget_s, iters_per_launch, engine, mixed_switch_rtol)
     _lib.check(_LIB.cdft_batch_converge(plans, n, ptrs, ctypes.byref(opts), res))
     return [ConvergeResult(res[i], None) for i in range(n)]
 

@@ -79,6 +79,7 @@ class SolverOpts(ctypes.Structure):
         ("time_budget_s", ctypes.c_double),
         ("iters_per_launch", ctypes.c_int),
         ("engine", ctypes.c_int),
+        ("mixed_switch_rtol", ctypes.c_double),
     ]
 
 

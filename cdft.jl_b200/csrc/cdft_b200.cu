@@ -106,8 +106,9 @@ struct Batch {
     int* h_done = nullptr;
     double* d_hist = nullptr;
     int hist_cap = 0;
-    cudaGraphExec_t graph = nullptr;
-    int graph_iters = 0;
+    int cur32 = 0;                          // arithmetic of the running phase: 1 FP32, 0 FP64
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};   // indexed by cur32
+    int graph_iters[2] = {0, 0};
 };
 
 namespace {
@@ -132,7 +133,8 @@ int upload_constants()
 void free_batch(Batch* b)
 {
     if (!b) return;
-    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (int k = 0; k < 2; ++k)
+        if (b->graph[k]) cudaGraphExecDestroy(b->graph[k]);
     cudaFree(b->d_sys);
     cudaFree(b->d_st);
     cudaFree(b->d_tasks);
@@ -240,7 +242,7 @@ int plan_build(cdft_plan* p)
 
     const size_t ne = (size_t)S.n_elem;
     const size_t ntap = (size_t)S.nconv * nc * N;
-    const size_t esz = S.mixed ? sizeof(float) : sizeof(double);
+    const size_t esz = sizeof(double);   // mixed plans finish with an FP64 phase in the same buffers
     CU(cudaMalloc(&p->d_taps, ntap * sizeof(double)));
     CU(cudaMalloc(&p->d_vec, ne * 6 * sizeof(double)));
     CU(cudaMemsetAsync(p->d_vec, 0, ne * 6 * sizeof(double), p->stream));
@@ -309,6 +311,7 @@ int batch_build(const std::vector<cdft_plan*>& plans, Batch** out)
     b->nc = plans[0]->desc.nc;
     b->nd = plans[0]->desc.nd;
     b->mixed = plans[0]->sys.mixed;
+    b->cur32 = b->mixed;
     b->stream = plans[0]->stream;
     for (auto* p : plans) {
         if (p->desc.nc != b->nc || p->desc.nd != b->nd || p->sys.mixed != b->mixed) {
@@ -444,7 +447,7 @@ size_t persistent_smem_need(const Batch* b)
     int nmax = 0;
     for (auto* p : b->plans) nmax = std::max(nmax, p->N);
     const SysDev& S = b->plans[0]->sys;
-    return pers_smem_bytes(nmax, S.nc, S.nconv, S.NF, b->mixed ? sizeof(float) : sizeof(double));
+    return pers_smem_bytes(nmax, S.nc, S.nconv, S.NF, b->cur32 ? sizeof(float) : sizeof(double));
 }
 
 template <typename T, int NC>
@@ -460,7 +463,7 @@ size_t persistent_smem_limit(const Batch* b)
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->plans[0]->device);
     size_t stat = 0;
-    switch ((b->mixed ? 10 : 0) + b->nc) {
+    switch ((b->cur32 ? 10 : 0) + b->nc) {
     case 1: stat = persistent_static_smem<double, 1>(); break;
     case 2: stat = persistent_static_smem<double, 2>(); break;
     case 3: stat = persistent_static_smem<double, 3>(); break;
@@ -476,24 +479,25 @@ size_t persistent_smem_limit(const Batch* b)
 
 int batch_capture(Batch* b, int iters)
 {
-    if (b->graph && b->graph_iters == iters) return 0;
-    if (b->graph) {
-        cudaGraphExecDestroy(b->graph);
-        b->graph = nullptr;
+    const int g32 = b->cur32;
+    if (b->graph[g32] && b->graph_iters[g32] == iters) return 0;
+    if (b->graph[g32]) {
+        cudaGraphExecDestroy(b->graph[g32]);
+        b->graph[g32] = nullptr;
     }
     cudaGraph_t g;
     CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     const long long before = g_launches;
     int rc = 0;
-    for (int it = 0; it < iters && !rc; ++it) rc = b->mixed ? launch_iteration<float>(b) : launch_iteration<double>(b);
+    for (int it = 0; it < iters && !rc; ++it) rc = g32 ? launch_iteration<float>(b) : launch_iteration<double>(b);
     g_launches = before;
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (rc) return rc;
     if (e != cudaSuccess) return set_error(CDFT_E_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
-    e = cudaGraphInstantiate(&b->graph, g, 0);
+    e = cudaGraphInstantiate(&b->graph[g32], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return set_error(CDFT_E_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
-    b->graph_iters = iters;
+    b->graph_iters[g32] = iters;
     return 0;
 }
 
@@ -537,7 +541,85 @@ int validate_opts(const cdft_solver_opts* o)
     return 0;
 }
 
-// rho pointers: host (is_dev = false) or device arrays of n_elem doubles per system
+// One aasol run over the batch from the profiles currently in the plans' rho
+// buffers, with the arithmetic of b->cur32.  hist_off[s]: history entries already
+// written for system s by an earlier phase.
+int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, const std::vector<int>& hist_off,
+              std::vector<AAState>& st, std::chrono::steady_clock::time_point t0, bool* budget_hit)
+{
+    const long long max_evals = (long long)opts->maxit + 2LL * opts->picard_maxit + 4;
+    for (int s = 0; s < b->nsys; ++s) {
+        AAState& A = st[s];
+        memset(&A, 0, sizeof(A));
+        A.mode = MODE_EVAL_INIT;
+        A.m = opts->m;
+        A.maxit = opts->maxit;
+        A.picard_maxit = opts->picard_maxit;
+        A.beta = opts->beta;
+        A.picard_beta = opts->picard_beta;
+        A.rtol = rtol;
+        A.atol = atol;
+        A.picard_rtol = opts->picard_rtol;
+        A.picard_atol = opts->picard_atol;
+        const int off = std::min(hist_off[s], b->hist_cap);
+        A.history = b->d_hist + (size_t)s * b->hist_cap + off;
+        A.history_cap = b->hist_cap - off;
+    }
+    CU(cudaMemcpyAsync(b->d_st, st.data(), sizeof(AAState) * b->nsys, cudaMemcpyHostToDevice, b->stream));
+    CU(cudaMemsetAsync(b->d_done, 0, sizeof(int), b->stream));
+    init_kernel<<<b->nechunks, ELEM_THREADS, 0, b->stream>>>(b->d_echunks, b->d_sys);
+    CHECK_LAUNCH();
+    g_launches += 1;
+    bool use_persistent = false;
+    if (opts->engine == CDFT_ENGINE_AUTO || opts->engine == CDFT_ENGINE_PERSISTENT) {
+        const size_t need = persistent_smem_need(b), limit = persistent_smem_limit(b);
+        use_persistent = need <= limit;
+        if (!use_persistent && opts->engine == CDFT_ENGINE_PERSISTENT)
+            return set_error(CDFT_E_UNSUPPORTED, "persistent engine needs %zu B of shared memory per system (limit %zu)",
+                             need, limit);
+    } else if (opts->engine != CDFT_ENGINE_GRID) {
+        return set_error(CDFT_E_INVALID, "engine=%d", opts->engine);
+    }
+    int rc = 0;
+    if (use_persistent) {
+        // one launch: every block runs its system's aasol loop to the end (bounded by max_evals)
+        const size_t smem = persistent_smem_need(b);
+        const int cap = (int)std::min<long long>(max_evals, 1 << 30);
+        rc = b->cur32 ? launch_persistent<float>(b, cap, smem) : launch_persistent<double>(b, cap, smem);
+        if (rc) return rc;
+    } else {
+        const int K = opts->iters_per_launch > 0 ? opts->iters_per_launch : 16;
+        rc = batch_capture(b, K);
+        if (rc) return rc;
+        const int per_iter = 3 + 2 * N_VEC_SLOTS;   // conv, phi, conv, el, ctl0, 5 vec, 4 ctl
+        long long launched_evals = 0;
+        while (true) {
+            CU(cudaGraphLaunch(b->graph[b->cur32], b->stream));
+            g_launches += (long long)K * per_iter;
+            launched_evals += K;
+            CU(cudaMemcpyAsync(b->h_done, b->d_done, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+            CU(cudaStreamSynchronize(b->stream));
+            if (*b->h_done >= b->nsys) break;
+            if (launched_evals > max_evals + K) break;   // cannot happen: aasol's caps end every system
+            if (opts->time_budget_s > 0) {
+                const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+                if (el > opts->time_budget_s) {
+                    *budget_hit = true;
+                    break;
+                }
+            }
+        }
+    }
+    CU(cudaMemcpyAsync(st.data(), b->d_st, sizeof(AAState) * b->nsys, cudaMemcpyDeviceToHost, b->stream));
+    CU(cudaStreamSynchronize(b->stream));
+    return 0;
+}
+
+// rho pointers: host (is_dev = false) or device arrays of n_elem doubles per system.
+// FP64 plans run one aasol.  Mixed plans run aasol with FP32 convolutions and Phi
+// until ||r|| <= max(rtol, s) ||r0|| + atol (s = mixed_switch_rtol), then a
+// second aasol in FP64 from that profile to the requested tolerance (the
+// warm start a converge! call from a previous profile performs).
 int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, bool is_dev,
                    const cdft_solver_opts* opts, cdft_result* results)
 {
@@ -560,82 +642,42 @@ int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, boo
     rc = batch_upload_sys(b);
     if (rc) return rc;
     const long long max_evals = (long long)opts->maxit + 2LL * opts->picard_maxit + 4;
-    int hist_cap = (int)std::min<long long>(max_evals, 1 << 20);
+    const int phases = b->mixed ? 2 : 1;
+    int hist_cap = (int)std::min<long long>(phases * max_evals, 1 << 20);
     if (b->hist_cap < hist_cap) {
         cudaFree(b->d_hist);
         b->d_hist = nullptr;
         CU(cudaMalloc(&b->d_hist, sizeof(double) * (size_t)hist_cap * b->nsys));
         b->hist_cap = hist_cap;
     }
-    std::vector<AAState> st(b->nsys);
-    for (int s = 0; s < b->nsys; ++s) {
-        AAState& A = st[s];
-        memset(&A, 0, sizeof(A));
-        A.mode = MODE_EVAL_INIT;
-        A.m = opts->m;
-        A.maxit = opts->maxit;
-        A.picard_maxit = opts->picard_maxit;
-        A.beta = opts->beta;
-        A.picard_beta = opts->picard_beta;
-        A.rtol = opts->rtol;
-        A.atol = opts->atol;
-        A.picard_rtol = opts->picard_rtol;
-        A.picard_atol = opts->picard_atol;
-        A.history = b->d_hist + (size_t)s * b->hist_cap;
-        A.history_cap = b->hist_cap;
-    }
-    CU(cudaMemcpyAsync(b->d_st, st.data(), sizeof(AAState) * b->nsys, cudaMemcpyHostToDevice, b->stream));
-    CU(cudaMemsetAsync(b->d_done, 0, sizeof(int), b->stream));
     for (int s = 0; s < b->nsys; ++s) {
         cdft_plan* p = plans[s];
         const size_t bytes = (size_t)p->sys.n_elem * sizeof(double);
         CU(cudaMemcpyAsync(p->sys.rho, rho[s], bytes, is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->stream));
     }
-    init_kernel<<<b->nechunks, ELEM_THREADS, 0, b->stream>>>(b->d_echunks, b->d_sys);
-    CHECK_LAUNCH();
-    g_launches += 1;
-    bool use_persistent = false;
-    if (opts->engine == CDFT_ENGINE_AUTO || opts->engine == CDFT_ENGINE_PERSISTENT) {
-        const size_t need = persistent_smem_need(b), limit = persistent_smem_limit(b);
-        use_persistent = need <= limit;
-        if (!use_persistent && opts->engine == CDFT_ENGINE_PERSISTENT)
-            return set_error(CDFT_E_UNSUPPORTED, "persistent engine needs %zu B of shared memory per system (limit %zu)",
-                             need, limit);
-    } else if (opts->engine != CDFT_ENGINE_GRID) {
-        return set_error(CDFT_E_INVALID, "engine=%d", opts->engine);
-    }
-    const int K = opts->iters_per_launch > 0 ? opts->iters_per_launch : 16;
-    if (!use_persistent) {
-        rc = batch_capture(b, K);
-        if (rc) return rc;
-    }
-    const int per_iter = 3 + 2 * N_VEC_SLOTS;   // conv, phi, conv, el, ctl0, 5 vec, 4 ctl
-    long long launched_evals = 0;
+    std::vector<AAState> st(b->nsys), st1;
+    std::vector<int> hist_off(b->nsys, 0);
     bool budget_hit = false;
-    if (use_persistent) {
-        // one launch: every block runs its system's aasol loop to the end (bounded by max_evals)
-        const size_t smem = persistent_smem_need(b);
-        rc = b->mixed ? launch_persistent<float>(b, (int)std::min<long long>(max_evals, 1 << 30), smem)
-                      : launch_persistent<double>(b, (int)std::min<long long>(max_evals, 1 << 30), smem);
+    if (b->mixed) {
+        const double sw = opts->mixed_switch_rtol > 0 ? opts->mixed_switch_rtol : 1e-5;
+        b->cur32 = 1;
+        rc = run_phase(b, opts, std::max(opts->rtol, sw), opts->atol, hist_off, st, t0, &budget_hit);
+        if (rc) return rc;
+        st1 = st;
+        for (int s = 0; s < b->nsys; ++s) hist_off[s] = st1[s].nevals;
+        bool diverged = false;
+        for (int s = 0; s < b->nsys; ++s) diverged |= (st1[s].errcode == -2);
+        if (!budget_hit && !diverged) {
+            b->cur32 = 0;
+            rc = run_phase(b, opts, opts->rtol, opts->atol, hist_off, st, t0, &budget_hit);
+            b->cur32 = 1;
+            if (rc) return rc;
+        }
+    } else {
+        b->cur32 = 0;
+        rc = run_phase(b, opts, opts->rtol, opts->atol, hist_off, st, t0, &budget_hit);
         if (rc) return rc;
     }
-    while (!use_persistent) {
-        CU(cudaGraphLaunch(b->graph, b->stream));
-        g_launches += (long long)K * per_iter;
-        launched_evals += K;
-        CU(cudaMemcpyAsync(b->h_done, b->d_done, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
-        CU(cudaStreamSynchronize(b->stream));
-        if (*b->h_done >= b->nsys) break;
-        if (launched_evals > max_evals + K) break;   // cannot happen: aasol's caps end every system
-        if (opts->time_budget_s > 0) {
-            const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-            if (el > opts->time_budget_s) {
-                budget_hit = true;
-                break;
-            }
-        }
-    }
-    CU(cudaMemcpyAsync(st.data(), b->d_st, sizeof(AAState) * b->nsys, cudaMemcpyDeviceToHost, b->stream));
     for (int s = 0; s < b->nsys; ++s) {
         cdft_plan* p = plans[s];
         const size_t bytes = (size_t)p->sys.n_elem * sizeof(double);
@@ -645,16 +687,19 @@ int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, boo
     if (results) {
         for (int s = 0; s < b->nsys; ++s) {
             cdft_result& r = results[s];
-            const AAState& A = st[s];
+            const AAState& A = (st1.empty() || st1[s].errcode != -2) ? st[s] : st1[s];
+            const int prev_evals = st1.empty() ? 0 : st1[s].nevals;
+            const int prev_k = st1.empty() ? 0 : st1[s].k;
+            const bool two = !st1.empty() && st1[s].errcode != -2;
             r.idid = A.idid;
             r.errcode = A.errcode;
-            r.iterations = A.k;
-            r.evaluations = A.nevals;
+            r.iterations = two ? prev_k + A.k : A.k;
+            r.evaluations = two ? prev_evals + A.nevals : A.nevals;
             r.resnorm = A.resnorm;
             r.tol = A.tol;
             r.history_len = 0;
             if (r.history && r.history_cap > 0) {
-                const int n = std::min(std::min(A.nevals, r.history_cap), b->hist_cap);
+                const int n = std::min(std::min(r.evaluations, r.history_cap), b->hist_cap);
                 CU(cudaMemcpy(r.history, b->d_hist + (size_t)s * b->hist_cap, sizeof(double) * n, cudaMemcpyDeviceToHost));
                 r.history_len = n;
             }
@@ -675,7 +720,7 @@ int self_batch(cdft_plan* p, Batch** b)
 
 int launch_stage(Batch* b, int stage)
 {
-    const bool mixed = b->mixed;
+    const bool mixed = b->cur32;
     const size_t smem = (size_t)(CONV_QC + CONV_TILE + CONV_QC + 31) * (mixed ? sizeof(float) : sizeof(double));
     switch (stage) {
     case 0:
@@ -817,7 +862,8 @@ int cdft_free_energy_res(cdft_plan* plan, const double* rho, double* F)
     if (rc) return rc;
     const size_t bytes = (size_t)plan->sys.n_elem * sizeof(double);
     CU(cudaMemcpyAsync(plan->sys.rho, rho, bytes, cudaMemcpyHostToDevice, plan->stream));
-    rc = plan->sys.mixed ? launch_eval_stages<float>(b, nullptr, false) : launch_eval_stages<double>(b, nullptr, false);
+    // the free-energy integral is FP64 in every precision mode
+    rc = launch_eval_stages<double>(b, nullptr, false);
     if (rc) return rc;
     std::vector<double> f(plan->N);
     CU(cudaMemcpyAsync(f.data(), plan->sys.fval, sizeof(double) * plan->N, cudaMemcpyDeviceToHost, plan->stream));

@@ -61,6 +61,7 @@ struct CDFTSolverOpts
     time_budget_s::Cdouble
     iters_per_launch::Cint
     engine::Cint
+    mixed_switch_rtol::Cdouble
 end
 
 mutable struct CDFTResult
@@ -158,7 +159,7 @@ const B200System = DFTSystem{<:PCSAFTModel,<:Any,<:Any,<:Any,<:Any,<:Any,<:DFTOp
 function cDFT.converge!(prob::DFTProblem{<:B200System}, method::AASol, ρ::Array{Float64})
     opts = CDFTSolverOpts(method.m, method.maxit, method.rtol, method.atol, method.beta,
                           method.picard_maxit, method.picard_beta, method.picard_rtol,
-                          method.picard_atol, 0.0, 0, 0)
+                          method.picard_atol, 0.0, 0, 0, 0.0)
     res = CDFTResult()
     check(ccall((:cdft_converge, LIB), Cint,
                 (Ptr{Cvoid}, Ptr{Float64}, Ref{CDFTSolverOpts}, Ref{CDFTResult}),

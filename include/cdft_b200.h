@@ -95,6 +95,8 @@ typedef struct {
     double time_budget_s;  /* host wall-clock cap for the whole call, <= 0: none */
     int iters_per_launch;  /* fixed-point evaluations per CUDA-graph launch (grid engine), <= 0: default */
     int engine;            /* CDFT_ENGINE_* */
+    double mixed_switch_rtol; /* mixed plans: FP32 phase until ||r|| <= max(rtol, this) ||r0|| + atol,
+                                 then FP64 to the requested tolerance; <= 0: 1e-5 */
 } cdft_solver_opts;
 
 /* execution engines of cdft_converge / cdft_batch_converge */
@@ -132,7 +134,7 @@ int cdft_functional_derivative(cdft_plan* plan, const double* rho, double* dFdrh
 int cdft_functional_derivative_dev(cdft_plan* plan, const double* d_rho, double* d_dFdrho);
 
 /* Residual Helmholtz energy per unit area (1D) or total (3D) in units of k_B T
- * (per m^2 in 1D).  Replaces F_res(system, ρ), src/models/models.jl:86-91
+ * (per m^2 in 1D), evaluated in FP64 whatever the plan's precision.  Replaces F_res(system, ρ), src/models/models.jl:86-91
  * (Simpson rule of src/utils/integrals.jl:17-41 on the device f_res values,
  * compensated FP64 summation). */
 int cdft_free_energy_res(cdft_plan* plan, const double* rho, double* F);

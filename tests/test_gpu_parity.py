@@ -224,3 +224,35 @@ def test_engines_agree():
         assert ra.errcode == rb.errcode == 0
         assert abs(ra.evaluations - rb.evaluations) <= 1
         assert float(np.max(np.abs(a / b - 1))) < 1e-9
+
+
+@pytest.mark.parametrize("engine", ["grid", "persistent"])
+def test_mixed_precision_reaches_fp64_fixed_point(engine):
+    """Mixed plans: FP32 convolutions/Phi until the residual fell by 1e-5, then an
+    FP64 polish.  The result is the FP64 fixed point: profiles 1e-9, adsorption
+    and the surface grand potential within 1e-9 of the FP64 path."""
+    import cdft_b200 as cd
+    for H, p, N in [(3e-9, 1e5, 160), (6e-9, 2.7e6, 310)]:
+        s64, _ = S.slit_pore(H, p, N)
+        s32, _ = S.slit_pore(H, p, N, precision="mixed")
+        r0 = cd.initialize_profiles(s64)
+        a, b = r0.copy(), r0.copy()
+        ra = cd.converge(s64, a, beta=0.1, tol=1e-10, anderson_m=5, engine=engine)
+        rb = cd.converge(s32, b, beta=0.1, tol=1e-10, anderson_m=5, engine=engine)
+        assert ra.errcode == 0 and rb.errcode == 0
+        assert float(np.max(np.abs(a / b - 1))) < 1e-8
+        assert cd.adsorption(s32, b)[0] == pytest.approx(cd.adsorption(s64, a)[0], rel=1e-9)
+        assert cd.surface_tension(s32, b) == pytest.approx(cd.surface_tension(s64, a), rel=1e-8)
+
+
+def test_mixed_dfdrho_close_to_fp64():
+    """FP32 convolutions and Phi: dF/drho within FP32 accuracy of the FP64 path."""
+    import cdft_b200 as cd
+    rng = np.random.default_rng(5)
+    s64, so = S.water_octane_lle(N=256)
+    s32 = cd.DFTSystem(s64.model, s64.structure, None, cd.DFTOptions("mixed"))
+    rho = S.random_smooth_profile(s64, rng)
+    d64 = cd.dFdrho_res(s64, rho)
+    d32 = cd.dFdrho_res(s32, rho)
+    for i in range(2):
+        assert _rel(d32[i], d64[i]) < 2e-5, _rel(d32[i], d64[i])
