@@ -2,6 +2,7 @@
 
     python cdft.jl_b200/build.py
 """
+import glob
 import os
 import subprocess
 import sys
@@ -9,7 +10,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc", "cdft_b200.cu")
 OUT = os.path.join(HERE, "cdft_b200", "libcdft_b200.so")
-DEPS = [os.path.join(HERE, "csrc", f) for f in ("cdft_b200.cu", "kernels.cuh", "functional.cuh", "cdft_internal.cuh")] + [
+# every CUDA source and header of the library, plus the C ABI header
+DEPS = sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")) + glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + [
     os.path.join(HERE, "..", "include", "cdft_b200.h")]
 
 NVCC_FLAGS = [

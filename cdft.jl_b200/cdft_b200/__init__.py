@@ -24,7 +24,8 @@ from .thermo import PCSAFT, N_A, K_B, R
 _LIB = _lib.load()
 
 __all__ = [
-    "PCSAFT", "Steele", "Uniform1DCart", "TwoPhase1DCart", "DFTOptions", "DFTSystem", "AASol",
+    "PCSAFT", "Steele", "HardSphereSolutes", "Uniform1DCart", "Uniform3DCart", "TwoPhase1DCart", "DFTOptions",
+    "DFTSystem", "AASol",
     "initialize_profiles", "converge", "batch_converge", "dFdrho_res", "F_res", "F_ideal",
     "free_energy", "surface_tension", "interfacial_tension", "adsorption", "integrate",
     "CDFTError", "launch_count",
@@ -68,6 +69,53 @@ class Steele:
         return V / T
 
 
+class HardSphereSolutes:
+    """Hard spherical solutes in a periodic box (an external field the reference does
+    not have; defined here for the 3D configuration): V_ext = `height` k_B T for fluid
+    centres closer than `radius` to a solute centre (minimum image), 0 elsewhere.
+    The height only has to saturate the clamp of ln G (converge.jl:150)."""
+
+    def __init__(self, centres, radius, height=100.0):
+        self.centres = np.asarray(centres, dtype=float).reshape(-1, 3)
+        self.radius = float(radius)
+        self.height = float(height)
+
+    @staticmethod
+    def seeded(n, radius, box, min_gap, seed=0):
+        """n non-overlapping centres in [0, box)^3 by rejection sampling with
+        numpy.random.default_rng(seed); centre distances >= 2 radius + min_gap."""
+        rng = np.random.default_rng(seed)
+        pts = []
+        while len(pts) < n:
+            c = rng.random(3) * box
+            ok = True
+            for q in pts:
+                dv = c - q
+                dv -= box * np.round(dv / box)
+                if np.sqrt(dv @ dv) < 2 * radius + min_gap:
+                    ok = False
+                    break
+            if ok:
+                pts.append(c)
+        return np.array(pts)
+
+    def potential(self, model, structure):
+        coords = [structure.coords(d) for d in range(3)]
+        X, Y, Z = coords[0][None, None, :], coords[1][None, :, None], coords[2][:, None, None]
+        box = [ub - lb for (lb, ub) in structure.bounds]
+        inside = np.zeros(structure.grid_shape, dtype=bool)
+        for c in self.centres:
+            dx = X - c[0]
+            dx = dx - box[0] * np.round(dx / box[0])
+            dy = Y - c[1]
+            dy = dy - box[1] * np.round(dy / box[1])
+            dz = Z - c[2]
+            dz = dz - box[2] * np.round(dz / box[2])
+            inside |= dx * dx + dy * dy + dz * dz < self.radius ** 2
+        V = np.where(inside, self.height, 0.0)
+        return np.repeat(V[None], len(model), axis=0)
+
+
 class Structure:
     def __init__(self, conditions, rho_bulk, bounds, ngrid, kind, rho_bulk2=None):
         self.conditions = (float(conditions[0]), float(conditions[1]))
@@ -85,6 +133,10 @@ class Structure:
     def nd(self):
         return len(self.ngrid)
 
+    @property
+    def grid_shape(self):
+        return tuple(reversed(self.ngrid))   # (..., Nz, Ny, Nx): memory order of Julia's (Nx, Ny, Nz)
+
     def coords(self, d=0):
         lb, ub = self.bounds[d]
         return np.linspace(lb, ub, self.ngrid[d])   # LinRange(lb, ub, N)
@@ -96,6 +148,15 @@ class Structure:
 def Uniform1DCart(conditions, rho_bulk, bounds, ngrid):
     """src/base/structure.jl:310-312"""
     return Structure(conditions, rho_bulk, bounds, ngrid, "uniform")
+
+
+def Uniform3DCart(conditions, rho_bulk, bounds, ngrid):
+    """src/base/structure.jl:352 (cubic periodic boxes with N in {32, 64, 128, 256} on the GPU)."""
+    b = np.asarray(bounds, dtype=float)
+    if b.size == 2:
+        b = np.tile(b.reshape(1, 2), (3, 1))
+    ng = ngrid if isinstance(ngrid, (tuple, list)) else (ngrid,) * 3
+    return Structure(conditions, rho_bulk, b, ng, "uniform")
 
 
 def TwoPhase1DCart(conditions, rho_bulk, rho_bulk2, bounds, ngrid):
@@ -121,8 +182,8 @@ class DFTSystem:
     structure, external fields and options; owns one device plan."""
 
     def __init__(self, model, structure, external_field=None, options=None):
-        if structure.nd != 1:
-            raise NotImplementedError("this build converges 1D Cartesian structures")
+        if structure.nd not in (1, 3):
+            raise NotImplementedError("1D and 3D Cartesian structures are supported")
         self.model = model
         self.structure = structure
         if external_field is None:
@@ -137,15 +198,19 @@ class DFTSystem:
         self.size = model.d(T)                                   # species.size
         self.chempot_res = model.mu_res(structure.rho_bulk, T)   # species.chempot_res
         nc = len(model)
-        N = structure.ngrid[0]
+        nd = structure.nd
         self.vext = None
         if self.external_field:
-            z = structure.coords(0)
-            self.vext = sum(f.potential(model, z, T) for f in self.external_field)
+            if nd == 1:
+                z = structure.coords(0)
+                self.vext = sum(f.potential(model, z, T) for f in self.external_field)
+            else:
+                self.vext = sum(f.potential(model, structure) for f in self.external_field)
         d = _lib.SystemDesc()
-        d.nd = 1
-        d.ngrid[0] = N
-        d.bounds[0][0], d.bounds[0][1] = structure.bounds[0]
+        d.nd = nd
+        for k in range(nd):
+            d.ngrid[k] = structure.ngrid[k]
+            d.bounds[k][0], d.bounds[k][1] = structure.bounds[k]
         d.coord = _lib.COORD_CART
         d.nc = nc
         for i in range(nc):
@@ -204,10 +269,9 @@ def initialize_profiles(system, noise=0.0, rng=None):
     s = system.structure
     p, T = s.conditions
     nc = system.nc
-    N = s.ngrid[0]
-    rho = np.empty((nc, N))
+    rho = np.empty((nc,) + s.grid_shape)
     if s.kind == "uniform":
-        rho[:] = s.rho_bulk[:, None]
+        rho[:] = s.rho_bulk.reshape((nc,) + (1,) * s.nd)
     else:
         lb, ub = s.bounds[0]
         H = ub - lb
@@ -361,16 +425,25 @@ class _KSum:
 
 
 def integrate(f, structure):
-    """``∫(f, structure)`` (integrals.jl:17,28-41): Simpson weights 1,4,2,...,1,
-    dz = (ub-lb)/N, compensated FP64 summation."""
+    """``∫(f, structure)`` (integrals.jl:17,28-41): Simpson weights 1,4,2,...,1 per
+    dimension (outer product), dz = (ub-lb)/N, compensated FP64 summation."""
     f = np.asarray(f, dtype=float)
-    n = f.shape[-1]
-    k = np.arange(1, n + 1)
-    w = np.where((k == 1) | (k == n), 1.0, np.where(k % 2 == 0, 4.0, 2.0))
-    acc = _KSum()
-    for v in (w * f).ravel():
-        acc.add(float(v))
-    return acc.value() * structure.dz()[0] / 3
+    w = np.ones(())
+    for ax, n in enumerate(f.shape):
+        k = np.arange(1, n + 1)
+        c = np.where((k == 1) | (k == n), 1.0, np.where(k % 2 == 0, 4.0, 2.0))
+        shape = [1] * f.ndim
+        shape[ax] = n
+        w = w * c.reshape(shape)
+    terms = (w * f).ravel()
+    if terms.size > 100000:          # large 3D grids: pairwise (NumPy) summation
+        total = float(np.sum(terms))
+    else:
+        acc = _KSum()
+        for v in terms:
+            acc.add(float(v))
+        total = acc.value()
+    return total * float(np.prod(np.array(structure.dz()) / 3))
 
 
 def F_res(system, rho):
@@ -385,7 +458,7 @@ def F_ideal(system, rho):
     """F_ideal(system, ρ) (BasicIdeal.jl:10-38)."""
     T = system.structure.conditions[1]
     f = (N_A * rho * (np.log(rho) - 1.5 * np.log(T) - 1)).sum(axis=0)
-    return integrate(f, system.structure)
+    return integrate(f, system.structure)   # (nc, grid...) summed over components
 
 
 def free_energy(system, rho):
@@ -401,7 +474,7 @@ def surface_tension(system, rho):
     F = free_energy(system, rho)
     mu = system.model.chemical_potential(s.rho_bulk, T)
     chem = sum(mu[i] * integrate(rho[i], s) for i in range(system.nc))
-    return F * K_B * T - chem + p * integrate(np.ones(s.ngrid[0]), s)
+    return F * K_B * T - chem + p * integrate(np.ones(s.grid_shape), s)
 
 
 def interfacial_tension(system, rho):

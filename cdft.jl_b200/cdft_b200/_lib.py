@@ -26,7 +26,8 @@ NOALLOC_MAX_ELEM = 8192
 ENGINE_AUTO, ENGINE_GRID, ENGINE_PERSISTENT = 0, 1, 2
 
 LIB_NAME = "libcdft_b200.so"
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
+# CDFT_B200_LIB selects another build of the library (the Julia shim honours the same variable)
+LIB_PATH = os.environ.get("CDFT_B200_LIB") or os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
 # every symbol declared in include/cdft_b200.h
 EXPORTED = [

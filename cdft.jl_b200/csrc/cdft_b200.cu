@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "persistent.cuh"
+#include "fft3d.cuh"
 
 namespace {
 
@@ -86,6 +87,12 @@ struct cdft_plan {
     void* d_part = nullptr;
     void* d_dfield = nullptr;
     double* d_fval = nullptr;
+    void* d_spec = nullptr;       // 3D: convolved-field spectra [comp][field][z][y][kx]
+    void* d_R = nullptr;          // 3D: spectrum of rho / accumulated adjoint spectrum
+    void* d_adj = nullptr;        // 3D: adjoint sum in real space
+    double* d_ktab = nullptr;     // 3D: kernel tables by |k|^2
+    int L3 = 0, k2max = 0;        // 3D: points per dimension, max |k|^2 index
+    double w0 = 0.0;              // 3D: reduced frequency per index
     Batch* self = nullptr;        // batch of this plan alone
 };
 
@@ -153,7 +160,18 @@ void free_batch(Batch* b)
 int validate_desc(const cdft_system_desc* d)
 {
     if (!d) return set_error(CDFT_E_INVALID, "desc is NULL");
-    if (d->nd != 1) return set_error(CDFT_E_UNSUPPORTED, "nd=%d: this build converges 1D Cartesian systems", d->nd);
+    if (d->nd != 1 && d->nd != 3) return set_error(CDFT_E_UNSUPPORTED, "nd=%d: 1D and 3D Cartesian systems are supported", d->nd);
+    if (d->nd == 3) {
+        const int n = d->ngrid[0];
+        if (d->ngrid[1] != n || d->ngrid[2] != n || !(n == 32 || n == 64 || n == 128 || n == 256))
+            return set_error(CDFT_E_UNSUPPORTED, "3D grids must be cubic with N in {32, 64, 128, 256} points per side");
+        for (int k = 0; k < 3; ++k)
+            if (!(d->bounds[k][1] > d->bounds[k][0]) ||
+                std::fabs((d->bounds[k][1] - d->bounds[k][0]) - (d->bounds[0][1] - d->bounds[0][0])) >
+                    1e-12 * (d->bounds[0][1] - d->bounds[0][0]))
+                return set_error(CDFT_E_UNSUPPORTED, "3D boxes must be cubic (equal periods)");
+        if (d->nc > 2) return set_error(CDFT_E_UNSUPPORTED, "3D systems support nc <= 2");
+    }
     if (d->coord != CDFT_COORD_CART) return set_error(CDFT_E_UNSUPPORTED, "only Cartesian coordinates are implemented");
     if (d->nc < 1 || d->nc > CDFT_MAX_NC) return set_error(CDFT_E_INVALID, "nc=%d out of [1,%d]", d->nc, CDFT_MAX_NC);
     if (d->ngrid[0] < 2) return set_error(CDFT_E_INVALID, "ngrid[0]=%d < 2", d->ngrid[0]);
@@ -190,8 +208,11 @@ int plan_alloc_m(cdft_plan* p, int m)
     return 0;
 }
 
+int plan_build3d(cdft_plan* p);
+
 int plan_build(cdft_plan* p)
 {
+    if (p->desc.nd == 3) return plan_build3d(p);
     const cdft_system_desc& d = p->desc;
     SysDev& S = p->sys;
     memset(&S, 0, sizeof(S));
@@ -286,6 +307,119 @@ int plan_build(cdft_plan* p)
     return 0;
 }
 
+
+// Reduced PC-SAFT parameters of preallocate_params (PCSAFT.jl:213-285) for a system record.
+void fill_phi_params(const cdft_system_desc& d, SysDev& S)
+{
+    const double L = d.L, T = d.T;
+    const int nc = d.nc;
+    PhiParams& P = S.phi;
+    P.nc = nc;
+    P.nd = d.nd;
+    P.T = T;
+    for (int i = 0; i < nc; ++i) {
+        P.m[i] = d.m[i];
+        P.d[i] = d.hsd[i] / L;
+    }
+    for (int i = 0; i < nc; ++i)
+        for (int j = 0; j < nc; ++j) {
+            const double sg = d.sigma[i * nc + j] / L;
+            const double e = d.eps[i * nc + j];
+            const double c1 = d.m[i] * d.m[j] * sg * sg * sg * e / T;
+            P.c1[i * CDFT_MAX_NC + j] = c1;
+            P.c2[i * CDFT_MAX_NC + j] = c1 * e / T;
+        }
+    P.has_assoc = d.n_assoc;
+    if (d.n_assoc) {
+        const cdft_assoc_pair& a = d.assoc[0];
+        P.a_ic = a.icomp;
+        P.a_jc = a.jcomp;
+        P.a_nia = a.n_ia;
+        P.a_njb = a.n_jb;
+        const double di = P.d[a.icomp], dj = P.d[a.jcomp];
+        P.a_dij = di * dj / (di + dj);
+        const double sg = d.sigma[a.icomp * nc + a.jcomp] / L;
+        P.a_K = sg * sg * sg * (exp(a.eps_ab / T) - 1.0) * a.kappa_ab;
+    }
+}
+
+// omega_hat of SWeightedDensity (weighted_densities.jl:48-69) at reduced |omega|
+double kernel_hat(int type, double wb, double R)
+{
+    const double PI = 3.14159265358979323846, TWO_PI = 2.0 * PI;
+    if (type == 1) return (wb == 0.0) ? 2.0 * R / TWO_PI : 2.0 * std::sin(wb * R) / wb / TWO_PI;
+    if (wb == 0.0) return 4.0 * PI * R * R * R / 3.0 / (TWO_PI * TWO_PI * TWO_PI);
+    return 4.0 * PI / (wb * wb * wb) * (std::sin(wb * R) - R * wb * std::cos(wb * R)) / (TWO_PI * TWO_PI * TWO_PI);
+}
+
+// 3D periodic cubic box: FFT weighted densities (fft3d.cuh)
+int plan_build3d(cdft_plan* p)
+{
+    const cdft_system_desc& d = p->desc;
+    SysDev& S = p->sys;
+    memset(&S, 0, sizeof(S));
+    const int L3 = d.ngrid[0], nc = d.nc;
+    const size_t npts = (size_t)L3 * L3 * L3;
+    const size_t nspec = (size_t)(L3 / 2 + 1) * L3 * L3;
+    p->N = (int)npts;
+    p->L3 = L3;
+    S.nd = 3;
+    S.N = (int)npts;
+    S.nc = nc;
+    S.NF = 9;
+    S.nconv = 8;
+    S.ngrid[0] = S.ngrid[1] = S.ngrid[2] = L3;
+    S.ksplit = 1;
+    S.n_elem = (int)(npts * nc);
+    S.mixed = d.precision == CDFT_PREC_MIXED;
+    const double Lr = d.L;
+    S.NA = kNA * Lr * Lr * Lr;
+    for (int k = 0; k < 3; ++k) p->dz[k] = (d.bounds[k][1] - d.bounds[k][0]) / L3;
+    for (int i = 0; i < nc; ++i) S.cprd[i] = d.mu_res_plus_ln_rhob[i];
+    fill_phi_params(d, S);
+    const size_t ne = (size_t)S.n_elem;
+    CU(cudaMalloc(&p->d_vec, ne * 6 * sizeof(double)));
+    CU(cudaMemsetAsync(p->d_vec, 0, ne * 6 * sizeof(double), p->stream));
+    CU(cudaMalloc(&p->d_part, (size_t)S.nconv * nc * npts * sizeof(double)));
+    CU(cudaMalloc(&p->d_dfield, (size_t)S.NF * nc * npts * sizeof(double)));
+    CU(cudaMalloc(&p->d_adj, ne * sizeof(double)));
+    CU(cudaMalloc(&p->d_spec, (size_t)S.nconv * nc * nspec * 2 * sizeof(double)));
+    CU(cudaMalloc(&p->d_R, (size_t)nc * nspec * 2 * sizeof(double)));
+    CU(cudaMalloc(&p->d_fval, npts * sizeof(double)));
+    if (d.vext) {
+        CU(cudaMalloc(&p->d_vext, ne * sizeof(double)));
+        CU(cudaMemcpyAsync(p->d_vext, d.vext, ne * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    }
+    // kernel tables by integer |k|^2: omega_bar = sqrt(k2) * L / period (structure_ω + _scaled_ω)
+    const int half = L3 / 2;
+    p->k2max = 3 * half * half;
+    p->w0 = Lr / (d.bounds[0][1] - d.bounds[0][0]);
+    const int types[5] = {1, 2, 2, 1, 2};                 // n2(d/2), n3(d/2), n3(d), n2(d), n3(psi d)
+    const double wf[5] = {0.5, 0.5, 1.0, 1.0, PSI_DISP};
+    std::vector<double> tab((size_t)nc * 5 * (p->k2max + 1));
+    for (int i = 0; i < nc; ++i)
+        for (int t = 0; t < 5; ++t) {
+            const double R = 2.0 * 3.14159265358979323846 * wf[t] * S.phi.d[i];
+            for (int k2 = 0; k2 <= p->k2max; ++k2)
+                tab[((size_t)i * 5 + t) * (p->k2max + 1) + k2] = kernel_hat(types[t], std::sqrt((double)k2) * p->w0, R);
+        }
+    CU(cudaMalloc(&p->d_ktab, tab.size() * sizeof(double)));
+    CU(cudaMemcpyAsync(p->d_ktab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    S.rho = p->d_vec;
+    S.sol = p->d_vec + ne;
+    S.gx = p->d_vec + 2 * ne;
+    S.res = p->d_vec + 3 * ne;
+    S.df = p->d_vec + 4 * ne;
+    S.out = p->d_vec + 5 * ne;
+    S.part = p->d_part;
+    S.dfield = p->d_dfield;
+    S.adj = p->d_adj;
+    S.fval = p->d_fval;
+    S.vext = p->d_vext;
+    CU(cudaStreamSynchronize(p->stream));
+    return 0;
+}
+
 void plan_free(cdft_plan* p)
 {
     cudaFree(p->d_taps);
@@ -297,6 +431,10 @@ void plan_free(cdft_plan* p)
     cudaFree(p->d_part);
     cudaFree(p->d_dfield);
     cudaFree(p->d_fval);
+    cudaFree(p->d_spec);
+    cudaFree(p->d_R);
+    cudaFree(p->d_adj);
+    cudaFree(p->d_ktab);
     if (p->own_stream) cudaStreamDestroy(p->own_stream);
 }
 
@@ -323,15 +461,20 @@ int batch_build(const std::vector<cdft_plan*>& plans, Batch** out)
             return set_error(CDFT_E_INVALID, "systems of one batch must live on one device");
         }
     }
+    if (b->nd == 3 && b->nsys != 1) {
+        free_batch(b);
+        return set_error(CDFT_E_UNSUPPORTED, "3D systems are converged one per batch");
+    }
     std::vector<ConvTask> tasks;
     std::vector<Chunk> pch, ech;
     for (int s = 0; s < b->nsys; ++s) {
         SysDev& S = plans[s]->sys;
         const int tiles = (S.N + CONV_TILE - 1) / CONV_TILE;
-        for (int i = 0; i < S.nc; ++i)
-            for (int f = 0; f < S.nconv; ++f)
-                for (int t = 0; t < tiles; ++t)
-                    for (int ks = 0; ks < S.ksplit; ++ks) tasks.push_back({s, i, f, t * S.ksplit + ks});
+        if (b->nd == 1)
+            for (int i = 0; i < S.nc; ++i)
+                for (int f = 0; f < S.nconv; ++f)
+                    for (int t = 0; t < tiles; ++t)
+                        for (int ks = 0; ks < S.ksplit; ++ks) tasks.push_back({s, i, f, t * S.ksplit + ks});
         for (int j = 0; j < S.N; j += POINT_THREADS) pch.push_back({s, j});
         S.chunk_begin = (int)ech.size();
         for (int e = 0; e < S.n_elem; e += ELEM_CHUNK) ech.push_back({s, e});
@@ -350,13 +493,14 @@ int batch_build(const std::vector<cdft_plan*>& plans, Batch** out)
     } while (0)
     BCU(cudaMalloc(&b->d_sys, sizeof(SysDev) * b->nsys));
     BCU(cudaMalloc(&b->d_st, sizeof(AAState) * b->nsys));
-    BCU(cudaMalloc(&b->d_tasks, sizeof(ConvTask) * tasks.size()));
+    BCU(cudaMalloc(&b->d_tasks, sizeof(ConvTask) * std::max<size_t>(tasks.size(), 1)));
     BCU(cudaMalloc(&b->d_pchunks, sizeof(Chunk) * pch.size()));
     BCU(cudaMalloc(&b->d_echunks, sizeof(Chunk) * ech.size()));
     BCU(cudaMalloc(&b->d_partials, sizeof(double) * RED_SLOTS * ech.size()));
     BCU(cudaMalloc(&b->d_done, sizeof(int)));
     BCU(cudaMallocHost(&b->h_done, sizeof(int)));
-    BCU(cudaMemcpy(b->d_tasks, tasks.data(), sizeof(ConvTask) * tasks.size(), cudaMemcpyHostToDevice));
+    if (!tasks.empty())
+        BCU(cudaMemcpy(b->d_tasks, tasks.data(), sizeof(ConvTask) * tasks.size(), cudaMemcpyHostToDevice));
     BCU(cudaMemcpy(b->d_pchunks, pch.data(), sizeof(Chunk) * pch.size(), cudaMemcpyHostToDevice));
     BCU(cudaMemcpy(b->d_echunks, ech.data(), sizeof(Chunk) * ech.size(), cudaMemcpyHostToDevice));
 #undef BCU
@@ -380,14 +524,89 @@ int launch_phi(Batch* b, const AAState* st)
         phi_kernel<T, NC_, ND_><<<b->npchunks, POINT_THREADS, 0, b->stream>>>(b->d_pchunks, b->d_sys, st); \
         return 0;                                                                                       \
     }
-    PHI_CASE(1, 1) PHI_CASE(2, 1) PHI_CASE(3, 1) PHI_CASE(4, 1)
+    PHI_CASE(1, 1) PHI_CASE(2, 1) PHI_CASE(3, 1) PHI_CASE(4, 1) PHI_CASE(1, 3) PHI_CASE(2, 3)
 #undef PHI_CASE
     return set_error(CDFT_E_UNSUPPORTED, "no Phi kernel for nc=%d nd=%d", b->nc, b->nd);
+}
+
+template <typename K>
+int fft_attr(K kern, size_t smem)
+{
+    CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return 0;
+}
+
+// weighted densities, Phi and (with_int) the adjoint of a 3D system by FFT
+template <typename T, int L>
+int launch_eval3d_L(Batch* b, const AAState* st, bool with_int)
+{
+    typedef typename V2<T>::t C;
+    constexpr int LINES = FftLines<T, L>::value;
+    cdft_plan* p = b->plans[0];
+    const SysDev& S = p->sys;
+    const int nc = S.nc;
+    const int KX = L / 2 + 1;
+    const size_t npts = (size_t)L * L * L, nspec = (size_t)KX * L * L;
+    const int ntile = (KX + LINES - 1) / LINES;
+    const int xblocks = L * L / (2 * LINES);
+    const size_t smem2 = (size_t)(2 * L * (LINES + 1) + L / 2) * sizeof(C);
+    const size_t smem3 = (size_t)(3 * L * (LINES + 1) + L / 2) * sizeof(C);
+    int rc = 0;
+    if ((rc = fft_attr(fft_x_r2c<T, double, L, LINES>, smem2)) || (rc = fft_attr(fft_x_r2c<T, T, L, LINES>, smem2)) ||
+        (rc = fft_attr(fft_x_c2r<T, L, LINES>, smem2)) || (rc = fft_attr(fft_yz<T, L, LINES>, smem2)) ||
+        (rc = fft_attr(fft_z_eval<T, L, LINES>, smem3)) || (rc = fft_attr(fft_z_adjoint<T, L, LINES>, smem3)))
+        return rc;
+    C* R = reinterpret_cast<C*>(p->d_R);
+    C* spec = reinterpret_cast<C*>(p->d_spec);
+    T* part = reinterpret_cast<T*>(S.part);
+    T* dfield = reinterpret_cast<T*>(S.dfield);
+    T* adj = reinterpret_cast<T*>(S.adj);
+    KTab3 K;
+    K.tab = p->d_ktab;
+    K.k2max = p->k2max;
+    K.w0 = p->w0;
+    K.nconv = S.nconv;
+    cudaStream_t str = b->stream;
+    fft_x_r2c<T, double, L, LINES><<<dim3(xblocks, nc), FFT_THREADS, smem2, str>>>(S.rho, npts, R, nspec, st);
+    fft_yz<T, L, LINES><<<dim3(L * ntile, nc), FFT_THREADS, smem2, str>>>(R, nspec, 1, 0, st);
+    fft_z_eval<T, L, LINES><<<dim3(L * ntile, nc), FFT_THREADS, smem3, str>>>(R, nspec, spec, nspec, K, st);
+    fft_yz<T, L, LINES><<<dim3(L * ntile, nc * S.nconv), FFT_THREADS, smem2, str>>>(spec, nspec, 1, 1, st);
+    fft_x_c2r<T, L, LINES><<<dim3(xblocks, nc * S.nconv), FFT_THREADS, smem2, str>>>(spec, nspec, part, npts,
+                                                                                    T(S.NA / (double)npts), st);
+    rc = launch_phi<T>(b, st);
+    if (rc) return rc;
+    g_launches += 6;
+    if (with_int) {
+        for (int i = 0; i < nc; ++i)
+            fft_x_r2c<T, T, L, LINES><<<dim3(xblocks, S.nconv), FFT_THREADS, smem2, str>>>(
+                dfield + ((size_t)i * S.NF + 1) * npts, npts, spec + (size_t)i * S.nconv * nspec, nspec, st);
+        fft_yz<T, L, LINES><<<dim3(L * ntile, nc * S.nconv), FFT_THREADS, smem2, str>>>(spec, nspec, 1, 0, st);
+        fft_z_adjoint<T, L, LINES><<<dim3(L * ntile, nc), FFT_THREADS, smem3, str>>>(spec, nspec, R, nspec, K, st);
+        fft_yz<T, L, LINES><<<dim3(L * ntile, nc), FFT_THREADS, smem2, str>>>(R, nspec, 1, 1, st);
+        fft_x_c2r<T, L, LINES><<<dim3(xblocks, nc), FFT_THREADS, smem2, str>>>(R, nspec, adj, npts,
+                                                                              T(1.0 / (double)npts), st);
+        g_launches += nc + 4;
+    }
+    CHECK_LAUNCH();
+    return 0;
+}
+
+template <typename T>
+int launch_eval3d(Batch* b, const AAState* st, bool with_int)
+{
+    switch (b->plans[0]->L3) {
+    case 32: return launch_eval3d_L<T, 32>(b, st, with_int);
+    case 64: return launch_eval3d_L<T, 64>(b, st, with_int);
+    case 128: return launch_eval3d_L<T, 128>(b, st, with_int);
+    case 256: return launch_eval3d_L<T, 256>(b, st, with_int);
+    default: return set_error(CDFT_E_UNSUPPORTED, "3D grid size %d", b->plans[0]->L3);
+    }
 }
 
 template <typename T>
 int launch_eval_stages(Batch* b, const AAState* st, bool with_int)
 {
+    if (b->nd == 3) return launch_eval3d<T>(b, st, with_int);
     const size_t smem = (size_t)(CONV_QC + CONV_TILE + CONV_QC + 31) * sizeof(T);
     conv1d_kernel<T><<<b->ntasks, CONV_WARPS * 32, smem, b->stream>>>(b->d_tasks, b->d_sys, st, 0);
     int rc = launch_phi<T>(b, st);
@@ -544,8 +763,10 @@ int validate_opts(const cdft_solver_opts* o)
 // One aasol run over the batch from the profiles currently in the plans' rho
 // buffers, with the arithmetic of b->cur32.  hist_off[s]: history entries already
 // written for system s by an earlier phase.
+// atol_sys (optional): one absolute tolerance per system, replacing rtol/atol.
 int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, const std::vector<int>& hist_off,
-              std::vector<AAState>& st, std::chrono::steady_clock::time_point t0, bool* budget_hit)
+              std::vector<AAState>& st, std::chrono::steady_clock::time_point t0, bool* budget_hit,
+              const std::vector<double>* atol_sys = nullptr)
 {
     const long long max_evals = (long long)opts->maxit + 2LL * opts->picard_maxit + 4;
     for (int s = 0; s < b->nsys; ++s) {
@@ -557,8 +778,8 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
         A.picard_maxit = opts->picard_maxit;
         A.beta = opts->beta;
         A.picard_beta = opts->picard_beta;
-        A.rtol = rtol;
-        A.atol = atol;
+        A.rtol = atol_sys ? 0.0 : rtol;
+        A.atol = atol_sys ? (*atol_sys)[s] : atol;
         A.picard_rtol = opts->picard_rtol;
         A.picard_atol = opts->picard_atol;
         const int off = std::min(hist_off[s], b->hist_cap);
@@ -571,14 +792,16 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
     CHECK_LAUNCH();
     g_launches += 1;
     bool use_persistent = false;
-    if (opts->engine == CDFT_ENGINE_AUTO || opts->engine == CDFT_ENGINE_PERSISTENT) {
+    if (b->nd == 3 && opts->engine == CDFT_ENGINE_PERSISTENT)
+        return set_error(CDFT_E_UNSUPPORTED, "3D systems run on the grid engine");
+    if (opts->engine != CDFT_ENGINE_AUTO && opts->engine != CDFT_ENGINE_GRID && opts->engine != CDFT_ENGINE_PERSISTENT)
+        return set_error(CDFT_E_INVALID, "engine=%d", opts->engine);
+    if (b->nd == 1 && (opts->engine == CDFT_ENGINE_AUTO || opts->engine == CDFT_ENGINE_PERSISTENT)) {
         const size_t need = persistent_smem_need(b), limit = persistent_smem_limit(b);
         use_persistent = need <= limit;
         if (!use_persistent && opts->engine == CDFT_ENGINE_PERSISTENT)
             return set_error(CDFT_E_UNSUPPORTED, "persistent engine needs %zu B of shared memory per system (limit %zu)",
                              need, limit);
-    } else if (opts->engine != CDFT_ENGINE_GRID) {
-        return set_error(CDFT_E_INVALID, "engine=%d", opts->engine);
     }
     int rc = 0;
     if (use_persistent) {
@@ -618,8 +841,9 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
 // rho pointers: host (is_dev = false) or device arrays of n_elem doubles per system.
 // FP64 plans run one aasol.  Mixed plans run aasol with FP32 convolutions and Phi
 // until ||r|| <= max(rtol, s) ||r0|| + atol (s = mixed_switch_rtol), then a
-// second aasol in FP64 from that profile to the requested tolerance (the
-// warm start a converge! call from a previous profile performs).
+// second aasol in FP64 from that profile until the FP64 residual meets the
+// stopping test of a plain FP64 run, rtol ||r0|| + atol with r0 the residual
+// of the initial profile (taken from the first phase).
 int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, bool is_dev,
                    const cdft_solver_opts* opts, cdft_result* results)
 {
@@ -668,8 +892,13 @@ int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, boo
         bool diverged = false;
         for (int s = 0; s < b->nsys; ++s) diverged |= (st1[s].errcode == -2);
         if (!budget_hit && !diverged) {
+            // phase-1 tol = max(rtol, sw) ||r0|| + atol gives back ||r0||
+            const double r1 = std::max(opts->rtol, sw);
+            std::vector<double> target(b->nsys);
+            for (int s = 0; s < b->nsys; ++s)
+                target[s] = opts->rtol * ((st1[s].tol - opts->atol) / r1) + opts->atol;
             b->cur32 = 0;
-            rc = run_phase(b, opts, opts->rtol, opts->atol, hist_off, st, t0, &budget_hit);
+            rc = run_phase(b, opts, opts->rtol, opts->atol, hist_off, st, t0, &budget_hit, &target);
             b->cur32 = 1;
             if (rc) return rc;
         }
@@ -721,6 +950,7 @@ int self_batch(cdft_plan* p, Batch** b)
 int launch_stage(Batch* b, int stage)
 {
     const bool mixed = b->cur32;
+    if (b->nd == 3 && stage != 3) return set_error(CDFT_E_UNSUPPORTED, "3D systems time stage 3 only");
     const size_t smem = (size_t)(CONV_QC + CONV_TILE + CONV_QC + 31) * (mixed ? sizeof(float) : sizeof(double));
     switch (stage) {
     case 0:
@@ -868,15 +1098,25 @@ int cdft_free_energy_res(cdft_plan* plan, const double* rho, double* F)
     std::vector<double> f(plan->N);
     CU(cudaMemcpyAsync(f.data(), plan->sys.fval, sizeof(double) * plan->N, cudaMemcpyDeviceToHost, plan->stream));
     CU(cudaStreamSynchronize(plan->stream));
-    // Simpson coefficients of _∫ (integrals.jl:28-41): 1, 4, 2, 4, ..., 1 times dz/3
-    const int N = plan->N;
+    // Simpson coefficients of _∫ (integrals.jl:28-41): 1, 4, 2, 4, ..., 1 per dimension (outer
+    // product in nD), times prod(dz/3); compensated summation
+    auto coef = [](int k, int n) { return (k == 1 || k == n) ? 1.0 : ((k % 2 == 0) ? 4.0 : 2.0); };
     KSum acc;
-    for (int k = 1; k <= N; ++k) {
-        const double c = (k == 1 || k == N) ? 1.0 : ((k % 2 == 0) ? 4.0 : 2.0);
-        acc.add(c * f[k - 1]);
-    }
     const double L = plan->desc.L;
-    *F = acc.value() * (plan->dz[0] / 3.0) / (L * L * L);
+    if (plan->desc.nd == 1) {
+        const int N = plan->N;
+        for (int k = 1; k <= N; ++k) acc.add(coef(k, N) * f[k - 1]);
+        *F = acc.value() * (plan->dz[0] / 3.0) / (L * L * L);
+    } else {
+        const int n = plan->L3;
+        for (int z = 1; z <= n; ++z)
+            for (int y = 1; y <= n; ++y) {
+                const double cyz = coef(z, n) * coef(y, n);
+                for (int x = 1; x <= n; ++x)
+                    acc.add(cyz * coef(x, n) * f[((size_t)(z - 1) * n + (y - 1)) * n + (x - 1)]);
+            }
+        *F = acc.value() * (plan->dz[0] / 3.0) * (plan->dz[1] / 3.0) * (plan->dz[2] / 3.0) / (L * L * L);
+    }
     return 0;
 }
 
@@ -903,6 +1143,9 @@ int cdft_phi_pointwise(cdft_plan* plan, const double* n, int npts, double* fval,
         case 4: phi_points_kernel<4, 1><<<blocks, 128, 0, plan->stream>>>(P, d_n, npts, d_f, d_g); break;
         default: rc = set_error(CDFT_E_UNSUPPORTED, "nc");
         }
+    } else if (plan->desc.nd == 3 && nc <= 2) {
+        if (nc == 1) phi_points_kernel<1, 3><<<blocks, 128, 0, plan->stream>>>(P, d_n, npts, d_f, d_g);
+        else phi_points_kernel<2, 3><<<blocks, 128, 0, plan->stream>>>(P, d_n, npts, d_f, d_g);
     } else {
         rc = set_error(CDFT_E_UNSUPPORTED, "nd");
     }

@@ -77,6 +77,7 @@ struct SysDev {
     void* dfield;                // dPhi/dn [(i*NF+a)*N + j] (double or float)
     double* fval;                // Phi per point
     double* out;                 // scratch output (functional derivative)
+    void* adj;                   // 3D: adjoint sum sum_f ±omega_f * dPhi/dn_f per element (T), else nullptr
 };
 
 struct AAState {

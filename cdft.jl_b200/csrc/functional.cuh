@@ -28,6 +28,32 @@ __device__ __forceinline__ T fabs_t(T x) { return x < T(0) ? -x : x; }
 // association logs stay FP64 in the mixed mode).
 __device__ __forceinline__ double logabs64(double x) { return log(fabs(x)); }
 
+// White-Bear bracket B(n3) = [ln(1 - n3) / n3^2 + 1 / (n3 (1 - n3)^2)] / (12 pi) and
+// dB/dn3 (FMT.jl:39-43 writes B in this closed form).  For small |n3| the two
+// terms cancel from O(1/n3) to O(1) (from O(1/n3^3) in dB/dn3), which makes the
+// closed form lose all digits where n3 passes through zero: the ringing of the
+// sampled kernels next to hard solutes puts grid points there.  Below |n3| = 0.05
+// the Taylor series 12 pi B = sum_j (j+1)(j+3)/(j+2) n3^j is used instead; 16
+// terms reach the FP64 rounding level on that interval.
+__device__ __forceinline__ void wb_bracket(double n3, double D, double Lg, double invD, double& B, double& dB)
+{
+    const double c12 = 12.0 * 3.14159265358979323846;
+    if (fabs(n3) < 0.05) {
+        double b = 16.0 * 18.0 / 17.0, db = 0.0;   // j = 15
+#pragma unroll
+        for (int j = 14; j >= 0; --j) {
+            db = db * n3 + b;
+            b = b * n3 + (j + 1.0) * (j + 3.0) / (j + 2.0);
+        }
+        B = b / c12;
+        dB = db / c12;
+        return;
+    }
+    B = Lg / (c12 * n3 * n3) + 1.0 / (c12 * n3 * D * D);
+    dB = -invD / (c12 * n3 * n3) - 2.0 * Lg / (c12 * n3 * n3 * n3)
+         - 1.0 / (c12 * n3 * n3 * D * D) + 2.0 / (c12 * n3 * D * D * D);
+}
+
 template <typename T, int NC, int ND>
 __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + ND], T (&g)[NC][6 + ND])
 {
@@ -68,10 +94,8 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
     const double Dd = 1.0 - n3d;
     const double Lg = logabs64(Dd);
     const double invD = 1.0 / Dd;
-    const double c12 = 12.0 * 3.14159265358979323846;
-    const double Bd = Lg / (c12 * n3d * n3d) + 1.0 / (c12 * n3d * Dd * Dd);
-    const double dBd = -invD / (c12 * n3d * n3d) - 2.0 * Lg / (c12 * n3d * n3d * n3d)
-                       - 1.0 / (c12 * n3d * n3d * Dd * Dd) + 2.0 / (c12 * n3d * Dd * Dd * Dd);
+    double Bd, dBd;
+    wb_bracket(n3d, Dd, Lg, invD, Bd, dBd);
     const T A3 = n2 * n2 * n2 / T(3) - n2 * nv2sq;
     const T A2 = n1 * n2 - nv1v2;
     T phi = T(-double(n0) * Lg) + A2 * T(invD) + A3 * T(Bd);

@@ -192,6 +192,11 @@ __device__ __forceinline__ double dfdrho_elem(const SysDev& S, int e)
     const T* df = reinterpret_cast<const T*>(S.dfield);
     const T* part = reinterpret_cast<const T*>(S.part);
     double v = double(df[(i * S.NF) * S.N + j]);   // rho field: δfδρ_res .= profile
+    if (S.adj) {   // 3D: the adjoint convolutions were summed in the spectral domain
+        v += double(reinterpret_cast<const T*>(S.adj)[e]);
+        if (S.vext) v += S.vext[e];
+        return v;
+    }
     for (int f = 0; f < S.nconv; ++f) {
         const T* p = part + ((size_t)(i * S.nconv + f) * S.ksplit) * S.N + j;
         T acc = p[0];

@@ -96,7 +96,8 @@ typedef struct {
     int iters_per_launch;  /* fixed-point evaluations per CUDA-graph launch (grid engine), <= 0: default */
     int engine;            /* CDFT_ENGINE_* */
     double mixed_switch_rtol; /* mixed plans: FP32 phase until ||r|| <= max(rtol, this) ||r0|| + atol,
-                                 then FP64 to the requested tolerance; <= 0: 1e-5 */
+                                 then FP64 until ||r|| <= rtol ||r0|| + atol, the stopping test of an
+                                 FP64 run (r0 of the initial profile); <= 0: 1e-5 */
 } cdft_solver_opts;
 
 /* execution engines of cdft_converge / cdft_batch_converge */

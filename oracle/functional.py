@@ -92,10 +92,11 @@ def fftfreq(n, fs):
 class DFTSystem:
     """PC-SAFT DFT system (base.jl:50-90 ``DFTSystem`` / ``build_DFT_system``)."""
 
-    def __init__(self, model, structure, walls=None):
+    def __init__(self, model, structure, walls=None, vext=None):
         self.model = model
         self.structure = structure
         self.walls = list(walls or [])
+        self._vext_given = None if vext is None else np.asarray(vext, dtype=np.float64)
         T = structure.T
         self.nc = model.nc
         self.nd = structure.nd
@@ -174,6 +175,8 @@ class DFTSystem:
 
     # ---- external field (steele.jl:49-81) ---------------------------------------
     def _build_vext(self):
+        if self._vext_given is not None:
+            return self._vext_given   # e.g. hard spherical solutes in 3D (no counterpart in the reference)
         if not self.walls:
             return None
         if self.nd != 1:
@@ -371,6 +374,30 @@ def _logabs(z):
     return np.log(z * np.sign(np.real(z)))
 
 
+# Taylor coefficients of 12 pi B(n3), B the White-Bear bracket below: (j+1)(j+3)/(j+2)
+_WB_SERIES = [(j + 1.0) * (j + 3.0) / (j + 2.0) for j in range(16)]
+_WB_SMALL = 0.05
+
+
+def _wb_bracket(n3, dn, log1dn):
+    """B(n3) = ln(1-n3)/(12 pi n3^2) + 1/(12 pi n3 (1-n3)^2) (FMT.jl:42-43).
+
+    The closed form cancels from O(1/n3) to O(1) as n3 -> 0 (its derivative from
+    O(1/n3^3)), which loses every digit where the kernels' ringing next to a hard
+    solute takes n3 through zero; for |Re n3| < 0.05 the Taylor series
+    12 pi B = sum_j (j+1)(j+3)/(j+2) n3^j (16 terms, FP64 rounding level there) is
+    used instead.  Polynomial in n3, so the complex step differentiates it."""
+    with np.errstate(all="ignore"):
+        closed = log1dn / (12 * np.pi * n3 * n3) + 1.0 / (12 * np.pi * n3 * dn * dn)
+    small = np.abs(np.real(n3)) < _WB_SMALL
+    if not np.any(small):
+        return closed
+    ser = _WB_SERIES[-1] + 0 * n3
+    for c in _WB_SERIES[-2::-1]:
+        ser = ser * n3 + c
+    return np.where(small, ser / (12 * np.pi), closed)
+
+
 def f_res(n, sys):
     """Pointwise PC-SAFT residual free-energy density (PCSAFT.jl:110-117).
 
@@ -399,7 +426,7 @@ def f_res(n, sys):
     nv2sq = sum(nv2[k] * nv2[k] for k in range(nd))
     dn = 1.0 - n3
     log1dn = _logabs(dn)
-    bkt = log1dn / (12 * pi * n3 * n3) + 1.0 / (12 * pi * n3 * dn * dn)
+    bkt = _wb_bracket(n3, dn, log1dn)
     res_hs = -n0 * log1dn + (n1 * n2 - nv1v2) / dn + (n2 * n2 * n2 / 3 - n2 * nv2sq) * bkt
     # --- f_hc (PCSAFT.jl:123-144) ---
     z3 = z2 = 0.0

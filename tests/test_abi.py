@@ -67,3 +67,13 @@ int main(void) {{
     assert offs == [_lib.SystemDesc.vext.offset, _lib.SystemDesc.precision.offset,
                     _lib.SystemDesc.mu_res_plus_ln_rhob.offset, _lib.SolverOpts.engine.offset,
                     _lib.Result.history_len.offset]
+
+
+def test_library_is_not_older_than_its_sources():
+    """The in-tree library must be rebuilt after any change to its CUDA sources or the ABI header."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("cdft_build", os.path.join(ROOT, "cdft.jl_b200", "build.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    assert len(mod.DEPS) >= 7
+    assert mod.up_to_date(), "libcdft_b200.so is older than its sources: run cdft.jl_b200/build.py"
