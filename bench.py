@@ -268,7 +268,7 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and plain is not None:
         line["plain_fp64_gpu_path"] = plain
     if rank == 0 and args.with3d:
-        line["solutes3d"] = solutes3d(args.grid3d, args.precision)
+        line["solutes3d"] = {str(N): solutes3d(N) for N in args.grid3d}
     if args.cpu_baseline and rank == 0:
         line["cpu_baseline"] = cpu_baseline(specs, budget_s=args.cpu_budget)
     if dist:
@@ -282,31 +282,48 @@ T_3D = 100.0
 SOLVER_3D = dict(beta=0.1, tol=1e-10, anderson_m=10, maxit=2000)
 
 
-def solutes3d(N=128, precision="fp64", reps=2):
-    """3D configuration: PC-SAFT argon, 100 K, rho_b = 0.021 A^-3, periodic cubic box of
-    edge 16 sigma on N^3 points, 27 hard spherical solutes of radius 1.5 sigma at
-    non-overlapping positions (numpy default_rng(0), centre gaps >= 3 sigma + 2 cells),
-    Anderson m = 10.  Converged from the initial profile; metric: iterations/s."""
-    import ctypes
-    import torch
+def _solutes3d_system(N, precision):
     import cdft_b200 as cd
-    from cdft_b200 import _lib
     model = cd.PCSAFT(["argon"], **ARGON)
     s = model.sigma[0]
     box = 16 * s
     rb = 0.021e30 / cd.N_A
     st = cd.Uniform3DCart((1e5, T_3D), [rb], [0.0, box], N)
     centres = cd.HardSphereSolutes.seeded(27, 1.5 * s, box, 2 * box / N, seed=0)
-    sy = cd.DFTSystem(model, st, cd.HardSphereSolutes(centres, 1.5 * s), cd.DFTOptions(precision))
+    return cd.DFTSystem(model, st, cd.HardSphereSolutes(centres, 1.5 * s), cd.DFTOptions(precision))
+
+
+# HBM bytes per grid point of one functional-derivative evaluation of the 3D
+# pipeline, FP64 (8 B reals; the half spectrum holds 16 B per (N/2+1)/N point,
+# counted as 8 B per real point):
+#   forward rho: x 8+8, y 16, z + multiply 8+64                    = 104
+#   inverse of the 8 convolved fields: y 128, x 64+64              = 256
+#   Phi: read 9 fields 72, write 8 gradients 64                    = 136
+#   forward of the 8 gradients: x 64+64, y 128                     = 256
+#   z adjoint 64+8, inverse y 16, x 8+8                            = 104
+#   Euler-Lagrange output: rho, V_ext, adjoint in, G(rho) out      =  32
+# total 888 B/point; mixed: the FFT and Phi arrays in FP32 (half), rho, V_ext,
+# adjoint and G in FP64.
+BYTES_3D = {"fp64": 888, "mixed": (104 + 256 + 136 + 256 + 104) // 2 + 32}
+
+
+def solutes3d_run(N, precision, reps=2):
+    """One precision of the 3D configuration at N^3: converged from the initial
+    profile through cdft_converge_dev (device-resident rho), CUDA-event timed."""
+    import ctypes
+    import torch
+    import cdft_b200 as cd
+    from cdft_b200 import _lib
+    sy = _solutes3d_system(N, precision)
     rho0 = cd.initialize_profiles(sy)
     stream = torch.cuda.Stream()
-    _lib.check(_lib.load().cdft_plan_set_stream(sy._plan, ctypes.c_void_p(stream.cuda_stream)))
+    lib = _lib.load()
+    _lib.check(lib.cdft_plan_set_stream(sy._plan, ctypes.c_void_p(stream.cuda_stream)))
     method = cd.AASol.for_system(None, **SOLVER_3D)
     opts = method.c_opts(engine="grid")
     init = torch.from_numpy(rho0).cuda()
     work = torch.empty_like(init)
     res = _lib.Result()
-    lib = _lib.load()
 
     def run():
         with torch.cuda.stream(stream):
@@ -316,6 +333,7 @@ def solutes3d(N=128, precision="fp64", reps=2):
 
     run()   # warm-up (graph capture)
     torch.cuda.synchronize()
+    cd.launch_count(reset=True)
     times = []
     for _ in range(reps):
         e0 = torch.cuda.Event(enable_timing=True)
@@ -325,30 +343,68 @@ def solutes3d(N=128, precision="fp64", reps=2):
         e1.record(stream)
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
+    launches = cd.launch_count(reset=True) // reps
     ms = float(np.mean(times))
     evals = res.evaluations
     ips = evals / (ms * 1e-3)
-    npts = N ** 3
-    bytes_per_point = 512 if precision == "fp64" else 364   # algorithmic bytes per point per iteration
-    achieved = bytes_per_point * npts * ips / 1e9
-    peaks = measured_peaks()
-    peak = peaks["hbm_gbs"] if peaks else 6650.0
     ms_eval = ctypes.c_double()
     plans = (ctypes.c_void_p * 1)(sy._plan.value)
     _lib.check(lib.cdft_batch_time_stage(plans, 1, 3, 20, ctypes.byref(ms_eval)))
-    out = {
-        "workload": f"solutes3d: argon 100 K, {N}^3 periodic box edge 16 sigma, 27 hard solutes r=1.5 sigma",
-        "precision": precision, "solver": SOLVER_3D,
-        "iterations_per_s": round(ips, 2), "ms_per_converge": round(ms, 3), "evaluations": evals,
-        "errcode": res.errcode, "ms_per_iteration": round(ms / evals, 4),
-        "functional_derivative_ms": round(ms_eval.value, 4),
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s",
-                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
-                     "algorithmic_bytes_per_point_iteration": bytes_per_point},
-    }
+    rho = work.cpu().numpy()
+    omega = cd.surface_tension(sy, rho)   # F k_B T - sum mu int rho + p V: excess grand potential, J
+    fluid = sy.vext == 0
     sy.close()
-    return out
+    peaks = measured_peaks()
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    achieved = BYTES_3D[precision] * N ** 3 / (ms_eval.value * 1e-3) / 1e9
+    out = {
+        "iterations_per_s": round(ips, 2), "ms_per_converge": round(ms, 3), "evaluations": evals,
+        "errcode": res.errcode, "ms_per_iteration": round(ms / evals, 4), "gpu_launches_per_converge": launches,
+        "functional_derivative_ms": round(ms_eval.value, 4),
+        "roofline_functional_derivative": {
+            "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s",
+            "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "algorithmic_bytes_per_point": BYTES_3D[precision]},
+    }
+    return out, rho, omega, fluid
+
+
+def solutes3d(N=128, reps=2):
+    """3D configuration: PC-SAFT argon, 100 K, rho_b = 0.021 A^-3, periodic cubic box of
+    edge 16 sigma on N^3 points, 27 hard spherical solutes of radius 1.5 sigma at
+    non-overlapping positions (numpy default_rng(0), centre gaps >= 3 sigma + 2 cells),
+    Anderson m = 10, beta = 0.1, tol = 1e-10.  FP64 and mixed, each converged from the
+    initial profile; the mixed profile and excess grand potential are compared with
+    the FP64 ones (relative errors; rho over the fluid, V_ext = 0)."""
+    r64, rho64, om64, fluid = solutes3d_run(N, "fp64", reps)
+    r32, rho32, om32, _ = solutes3d_run(N, "mixed", reps)
+    return {
+        "workload": f"solutes3d: argon 100 K, {N}^3 periodic box edge 16 sigma, 27 hard solutes r=1.5 sigma",
+        "solver": SOLVER_3D, "fp64": r64, "mixed": r32,
+        "mixed_vs_fp64": {
+            "rho_rel_err_max_fluid": float(np.max(np.abs(rho32[fluid] / rho64[fluid] - 1))),
+            "omega_rel_err": abs(om32 / om64 - 1),
+            "speedup_converge": round(r64["ms_per_converge"] / r32["ms_per_converge"], 3),
+            "speedup_per_iteration": round(r64["ms_per_iteration"] / r32["ms_per_iteration"], 3),
+        },
+    }
+
+
+def run_3d_only(args):
+    """--only3d: the 3D configuration alone at one size and precision (profiling runs)."""
+    import torch
+    torch.cuda.set_device(0)
+    N = args.grid3d[0]
+    for _ in range(max(0, args.warmup - 1)):
+        solutes3d_run(N, args.precision, reps=1)
+    r, _, _, _ = solutes3d_run(N, args.precision, reps=max(1, args.steps))
+    return {"metric": "3D iterations/s (solutes3d)", "value": r["iterations_per_s"], "unit": "iterations/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_converge"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32 FFT+Phi / f64 solver",
+            "data": "synthetic: seeded solute positions",
+            "config": {"workload": f"solutes3d {N}^3", "solver": SOLVER_3D}, "solutes3d": r}
 
 
 def mixed_accuracy(specs, systems_mixed, rho_mixed, method):
@@ -476,13 +532,17 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-plain", dest="plain", action="store_false", help="skip the sequential FP64 comparison")
     ap.add_argument("--no-3d", dest="with3d", action="store_false", help="skip the 3D solutes configuration")
-    ap.add_argument("--grid3d", type=int, default=128)
+    ap.add_argument("--grid3d", type=int, nargs="+", default=[128, 256])
+    ap.add_argument("--only3d", action="store_true",
+                    help="run only the 3D solutes configuration (first --grid3d size, --precision)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         line = run_reference(args, rank, world)
+    elif args.only3d:
+        line = run_3d_only(args) if rank == 0 else None
     else:
         line = run_ours(args, rank, world, local_rank)
     if rank == 0 and line is not None:

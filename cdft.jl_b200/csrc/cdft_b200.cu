@@ -638,24 +638,24 @@ int launch_iteration(Batch* b)
 }
 
 template <typename T, int NC>
-int launch_persistent_nc(Batch* b, int max_evals, size_t smem)
+int launch_persistent_nc(Batch* b, int max_evals, size_t smem, int vec_m)
 {
     auto kern = persistent_kernel<T, NC, 1>;
     CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<b->nsys, PERS_THREADS, smem, b->stream>>>(b->d_sys, b->d_st, b->d_done, max_evals);
+    kern<<<b->nsys, PERS_THREADS, smem, b->stream>>>(b->d_sys, b->d_st, b->d_done, max_evals, vec_m);
     CHECK_LAUNCH();
     g_launches += 1;
     return 0;
 }
 
 template <typename T>
-int launch_persistent(Batch* b, int max_evals, size_t smem)
+int launch_persistent(Batch* b, int max_evals, size_t smem, int vec_m)
 {
     switch (b->nc) {
-    case 1: return launch_persistent_nc<T, 1>(b, max_evals, smem);
-    case 2: return launch_persistent_nc<T, 2>(b, max_evals, smem);
-    case 3: return launch_persistent_nc<T, 3>(b, max_evals, smem);
-    case 4: return launch_persistent_nc<T, 4>(b, max_evals, smem);
+    case 1: return launch_persistent_nc<T, 1>(b, max_evals, smem, vec_m);
+    case 2: return launch_persistent_nc<T, 2>(b, max_evals, smem, vec_m);
+    case 3: return launch_persistent_nc<T, 3>(b, max_evals, smem, vec_m);
+    case 4: return launch_persistent_nc<T, 4>(b, max_evals, smem, vec_m);
     default: return set_error(CDFT_E_UNSUPPORTED, "nc=%d", b->nc);
     }
 }
@@ -805,10 +805,23 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
     }
     int rc = 0;
     if (use_persistent) {
-        // one launch: every block runs its system's aasol loop to the end (bounded by max_evals)
-        const size_t smem = persistent_smem_need(b);
+        // one launch: every block runs its system's aasol loop to the end (bounded by max_evals);
+        // the Anderson vectors join the block's shared memory when they fit
+        size_t smem = persistent_smem_need(b);
+        int vec_m = -1;
+        {
+            int nmax = 0;
+            for (auto* p : b->plans) nmax = std::max(nmax, p->N);
+            const SysDev& S0 = b->plans[0]->sys;
+            const size_t with_vec = pers_vec_offset(nmax, S0.nc, S0.nconv, S0.NF, b->cur32 ? sizeof(float) : sizeof(double))
+                                    + pers_vec_bytes(nmax * S0.nc, opts->m);
+            if (with_vec <= persistent_smem_limit(b)) {
+                smem = with_vec;
+                vec_m = opts->m;
+            }
+        }
         const int cap = (int)std::min<long long>(max_evals, 1 << 30);
-        rc = b->cur32 ? launch_persistent<float>(b, cap, smem) : launch_persistent<double>(b, cap, smem);
+        rc = b->cur32 ? launch_persistent<float>(b, cap, smem, vec_m) : launch_persistent<double>(b, cap, smem, vec_m);
         if (rc) return rc;
     } else {
         const int K = opts->iters_per_launch > 0 ? opts->iters_per_launch : 16;

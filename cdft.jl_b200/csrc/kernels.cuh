@@ -410,55 +410,51 @@ __device__ void aa_anderson_start(AAState& A)
 }
 
 // Householder QR of R[:, 2:m] (m x (m-1)) with LAPACK dlarfg conventions;
-// downdate_aaqr!, anderson.jl:552-583.
+// downdate_aaqr!, anderson.jl:552-583.  R[:, 2:m] of an upper triangular R is
+// upper Hessenberg, and every reflector keeps it so: the vector below the
+// diagonal of column j has the single entry at row j+1, each reflector touches
+// rows j and j+1 only.  The loops run over those rows (the dense loops add
+// exact zeros), in place on R with the column offset of the slice.
 __device__ void aa_downdate(AAState& A)
 {
     const int m = A.m, n = m - 1;
-    double Am[CDFT_MAX_M * CDFT_MAX_M];  // column-major m x n
-    for (int c = 0; c < n; ++c)
-        for (int r = 0; r < m; ++r) Am[r + c * m] = A.R[r + (c + 1) * m];
-    double tau[CDFT_MAX_M];
-    double V[CDFT_MAX_M * CDFT_MAX_M];
+    double* R = A.R;
+    double tau[CDFT_MAX_M], v1[CDFT_MAX_M];
     for (int j = 0; j < n; ++j) {
-        double alpha = Am[j + j * m];
-        double xn2 = 0.0;
-        for (int r = j + 1; r < m; ++r) xn2 += Am[r + j * m] * Am[r + j * m];
-        double xnorm = sqrt(xn2);
-        for (int r = 0; r < m; ++r) V[r + j * m] = 0.0;
-        V[j + j * m] = 1.0;
+        const double alpha = R[j + (j + 1) * m];
+        const double x = R[j + 1 + (j + 1) * m];
+        const double xnorm = sqrt(x * x);
         if (xnorm == 0.0) {
             tau[j] = 0.0;
-        } else {
-            const double beta = -copysign(hypot(alpha, xnorm), alpha);
-            tau[j] = (beta - alpha) / beta;
-            const double sc = 1.0 / (alpha - beta);
-            for (int r = j + 1; r < m; ++r) V[r + j * m] = Am[r + j * m] * sc;
-            Am[j + j * m] = beta;
-            for (int r = j + 1; r < m; ++r) Am[r + j * m] = 0.0;
-            for (int c = j + 1; c < n; ++c) {
-                double w = 0.0;
-                for (int r = j; r < m; ++r) w += V[r + j * m] * Am[r + c * m];
-                for (int r = j; r < m; ++r) Am[r + c * m] -= tau[j] * V[r + j * m] * w;
-            }
+            v1[j] = 0.0;
+            continue;
+        }
+        const double beta = -copysign(hypot(alpha, xnorm), alpha);
+        tau[j] = (beta - alpha) / beta;
+        v1[j] = x * (1.0 / (alpha - beta));
+        R[j + (j + 1) * m] = beta;
+        R[j + 1 + (j + 1) * m] = 0.0;
+        for (int c = j + 1; c < n; ++c) {
+            const double w = fma(v1[j], R[j + 1 + (c + 1) * m], R[j + (c + 1) * m]);
+            R[j + (c + 1) * m] = fma(-tau[j], w, R[j + (c + 1) * m]);
+            R[j + 1 + (c + 1) * m] = fma(-(tau[j] * v1[j]), w, R[j + 1 + (c + 1) * m]);
         }
     }
-    // thin Q (m x n)
-    double Qm[CDFT_MAX_M * CDFT_MAX_M];
+    // thin Q (m x n) = H_0 ... H_{n-1} [I; 0]
+    double* Qx = A.Qx;
     for (int c = 0; c < n; ++c)
-        for (int r = 0; r < m; ++r) Qm[r + c * m] = (r == c) ? 1.0 : 0.0;
+        for (int r = 0; r < m; ++r) Qx[r + c * m] = (r == c) ? 1.0 : 0.0;
     for (int j = n - 1; j >= 0; --j) {
         for (int c = 0; c < n; ++c) {
-            double w = 0.0;
-            for (int r = j; r < m; ++r) w += V[r + j * m] * Qm[r + c * m];
-            for (int r = j; r < m; ++r) Qm[r + c * m] -= tau[j] * V[r + j * m] * w;
+            const double w = fma(v1[j], Qx[j + 1 + c * m], Qx[j + c * m]);
+            Qx[j + c * m] = fma(-tau[j], w, Qx[j + c * m]);
+            Qx[j + 1 + c * m] = fma(-(tau[j] * v1[j]), w, Qx[j + 1 + c * m]);
         }
     }
+    // R[1:m-1, 1:m-1] = upper triangle of the slice; R[:, m] = 0
     for (int c = 0; c < n; ++c)
-        for (int r = 0; r < m; ++r) A.Qx[r + c * m] = Qm[r + c * m];
-    // R[1:m-1, 1:m-1] = Rd; R[:, m] = 0
-    for (int c = 0; c < n; ++c)
-        for (int r = 0; r < n; ++r) A.R[r + c * m] = (r <= c) ? Am[r + c * m] : 0.0;
-    for (int r = 0; r < m; ++r) A.R[r + (m - 1) * m] = 0.0;
+        for (int r = 0; r < m; ++r) R[r + c * m] = (r <= c) ? R[r + (c + 1) * m] : 0.0;
+    for (int r = 0; r < m; ++r) R[r + (m - 1) * m] = 0.0;
 }
 
 __device__ void aa_after_eval(AAState& A, double r, int* done_counter)

@@ -15,7 +15,7 @@
 
 #define PERS_THREADS 384
 #define PERS_WARPS (PERS_THREADS / 32)
-#define PERS_R 4
+#define PERS_R 8
 #define PERS_TILE (32 * PERS_R)
 
 // extended periodic window of one convolution input: ext[k] = in[(k - OFF) mod N]
@@ -28,6 +28,17 @@ __host__ __device__ __forceinline__ size_t pers_smem_bytes(int N, int nc, int nc
                   + (size_t)nc * nconv * pers_extn(N)  // extended inputs
                   + (size_t)nc * NF * N                // n, then dPhi/dn
                   + (size_t)nc * nconv * N);           // adjoint partials
+}
+
+// byte offset of the shared-memory Anderson vectors, and their size for n_elem
+// elements and m history columns (rho, sol, gx, res, df, V_ext, Q, DG)
+__host__ __device__ __forceinline__ size_t pers_vec_offset(int N, int nc, int nconv, int NF, size_t esz)
+{
+    return (pers_smem_bytes(N, nc, nconv, NF, esz) + 15) & ~(size_t)15;
+}
+__host__ __device__ __forceinline__ size_t pers_vec_bytes(int n_elem, int m)
+{
+    return sizeof(double) * (size_t)n_elem * (6 + 2 * (size_t)m);
 }
 
 template <int BLOCK>
@@ -52,6 +63,13 @@ __device__ __forceinline__ void block_reduce_to_smem(double* vals, int K, double
 }
 
 // all circulant convolutions of one stage: out[(i*nconv+f)*N + j] = scale * sum_q taps_if[q] in_if[j-q]
+//
+// A warp owns PERS_TILE = 32 * PERS_R outputs of one field; lane l accumulates
+// j = j0 + 32 r (r < PERS_R).  For each residue q0 = q mod 32 the inputs
+// in[j0 + 32 r - q] form a window that moves by one register per q += 32; the
+// window is a ring of PERS_R registers whose rotation is resolved at compile time
+// (the q loop is unrolled by PERS_R), so a step is one tap load, one window load
+// and PERS_R independent FMAs.
 template <typename T, int NC>
 __device__ __forceinline__ void pers_conv(const T* __restrict__ ext, bool shared_input, const T* __restrict__ taps,
                                           T* __restrict__ out, int out_comp_stride, int N, int nconv, T scale)
@@ -72,16 +90,21 @@ __device__ __forceinline__ void pers_conv(const T* __restrict__ ext, bool shared
         for (int r = 0; r < PERS_R; ++r) acc[r] = T(0);
         const int q0_end = min(32, N);
         for (int q0 = 0; q0 < q0_end; ++q0) {
-            T W[PERS_R];
+            T W[PERS_R];   // W[r] = in[j0 + 32 r - q] at the start of each unrolled block
 #pragma unroll
             for (int r = 0; r < PERS_R; ++r) W[r] = in[j0 + 32 * r - q0];
-            for (int q = q0; q < N; q += 32) {
-                const T t = tp[q];
+            for (int q = q0; q < N; q += 32 * PERS_R) {
 #pragma unroll
-                for (int r = 0; r < PERS_R; ++r) acc[r] = fma(t, W[r], acc[r]);
+                for (int s = 0; s < PERS_R; ++s) {
+                    const int qs = q + 32 * s;
+                    if (qs < N) {
+                        const T t = tp[qs];
 #pragma unroll
-                for (int r = PERS_R - 1; r > 0; --r) W[r] = W[r - 1];
-                W[0] = in[j0 - q - 32];
+                        for (int r = 0; r < PERS_R; ++r) acc[r] = fma(t, W[(r - s + PERS_R) % PERS_R], acc[r]);
+                        // the slot of output r = PERS_R-1 is free: it takes the input of step s+1, output 0
+                        W[PERS_R - 1 - s] = in[j0 - qs - 32];
+                    }
+                }
             }
         }
         T* o = out + (size_t)i * out_comp_stride + (size_t)f * N;
@@ -93,28 +116,121 @@ __device__ __forceinline__ void pers_conv(const T* __restrict__ ext, bool shared
     }
 }
 
+// FP64 tensor-core form of pers_conv (mma.sync m8n8k4 f64; the FP64 tensor path
+// of sm_100a).  With e[k] = in[k] the periodic extension and outputs grouped as
+// OUT[a][u] = out[8u + a] (a < 8):
+//   OUT[a][u] = sum_d sum_{c<8} t(8d + a - c) e[8(u - d) + c],  t(q) = 0 outside [0, N)
+// i.e. OUT = sum_d A_d B_d with A_d an 8x8 Toeplitz block of taps and
+// B_d[c][u] = e[8(u - d) + c] an 8-column slab of the extended input.  A warp owns
+// 8 columns (64 outputs) of one field and runs the k = (d, c) loop as 2 D mma of
+// k = 4 into two accumulators (c < 4, c >= 4).  Every q in [0, N) is visited once
+// per output, so the result is the circulant up to summation order.
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <int NC>
+__device__ __forceinline__ void pers_conv_dmma(const double* __restrict__ ext, bool shared_input,
+                                               const double* __restrict__ taps, double* __restrict__ out,
+                                               int out_comp_stride, int N, int nconv, double scale)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int EXTN = pers_extn(N), OFF = pers_off(N);
+    const int U = (N + 7) / 8;          // 8-output columns
+    const int nut = (U + 7) / 8;        // warp tiles of 8 columns
+    const int D = (N + 14) / 8;         // tap blocks: 8 (D - 1) + 7 >= N - 1
+    const int ntask = NC * nconv * nut;
+    const int r = lane >> 2, k = lane & 3;   // A row / C row, A column / B row
+    for (int task = warp; task < ntask; task += PERS_WARPS) {
+        const int ut = task % nut;
+        const int f = (task / nut) % nconv;
+        const int i = task / (nut * nconv);
+        const double* in = ext + (size_t)(shared_input ? i : i * nconv + f) * EXTN + OFF;
+        const double* tp = taps + (size_t)(i * nconv + f) * N;
+        const int u0 = ut * 8;
+        double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
+        // B: e[8 (u0 + r - d) + c], column n = r; A: t(8 d + r - c)
+        const double* bp = in + 8 * (u0 + r) + k;
+        for (int d = 0; d < D; ++d) {
+            const int q0 = 8 * d + r - k;        // c = k
+            const int q1 = q0 - 4;               // c = k + 4
+            const double a0 = (q0 >= 0 && q0 < N) ? tp[q0] : 0.0;
+            const double a1 = (q1 >= 0 && q1 < N) ? tp[q1] : 0.0;
+            const double b0 = bp[-8 * d];
+            const double b1 = bp[-8 * d + 4];
+            dmma_m8n8k4(c0, c1, a0, b0);
+            dmma_m8n8k4(e0, e1, a1, b1);
+        }
+        double* o = out + (size_t)i * out_comp_stride + (size_t)f * N;
+        const int j0 = 8 * (u0 + 2 * k) + r, j1 = j0 + 8;
+        if (j0 < N) o[j0] = (c0 + e0) * scale;
+        if (j1 < N) o[j1] = (c1 + e1) * scale;
+    }
+}
+
+template <typename T, int NC>
+__device__ __forceinline__ void pers_conv_any(const T* __restrict__ ext, bool shared_input, const T* __restrict__ taps,
+                                              T* __restrict__ out, int out_comp_stride, int N, int nconv, T scale)
+{
+    if constexpr (sizeof(T) == 8)
+        pers_conv_dmma<NC>(ext, shared_input, taps, out, out_comp_stride, N, nconv, scale);
+    else
+        pers_conv<T, NC>(ext, shared_input, taps, out, out_comp_stride, N, nconv, scale);
+}
+
 template <typename T, int NC, int ND>
 __global__ void __launch_bounds__(PERS_THREADS, 1)
-persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int* done_counter, int max_evals)
+persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int* done_counter, int max_evals,
+                  int vec_m)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ AAState sA;
+    __shared__ SysDev sS;
     __shared__ double sums[RED_SLOTS];
     constexpr int NF = 6 + ND, NCONV = 5 + ND;
-    const SysDev& S = sys[blockIdx.x];
-    const int N = S.N, n_elem = S.n_elem;
+    const SysDev& G = sys[blockIdx.x];
+    const int N = G.N, n_elem = G.n_elem;
     const int EXTN = pers_extn(N), OFF = pers_off(N);
     const int tid = threadIdx.x;
     T* taps = reinterpret_cast<T*>(smem_raw);
     T* ext = taps + (size_t)NC * NCONV * N;
     T* nf = ext + (size_t)NC * NCONV * EXTN;
     T* ip = nf + (size_t)NC * NF * N;
-    if (tid == 0) sA = st[blockIdx.x];
+    if (tid == 0) {
+        sA = st[blockIdx.x];
+        sS = G;
+    }
     {
-        const T* src = (sizeof(T) == 8) ? reinterpret_cast<const T*>(S.taps) : reinterpret_cast<const T*>(S.taps32);
+        const T* src = (sizeof(T) == 8) ? reinterpret_cast<const T*>(G.taps) : reinterpret_cast<const T*>(G.taps32);
         for (int k = tid; k < NC * NCONV * N; k += PERS_THREADS) taps[k] = src[k];
     }
+    // vec_m >= 0: the Anderson vectors (rho, sol, gx, res, df, V_ext, vec_m columns
+    // of Q and of DG) live in shared memory after the convolution buffers; rho and
+    // sol are read in here and written back at the end.
+    double* vs = reinterpret_cast<double*>(smem_raw + pers_vec_offset(N, NC, NCONV, NF, sizeof(T)));
+    if (vec_m >= 0) {
+        for (int e = tid; e < n_elem; e += PERS_THREADS) {
+            vs[e] = G.rho[e];
+            vs[n_elem + e] = G.sol[e];
+            if (G.vext) vs[5 * n_elem + e] = G.vext[e];
+        }
+    }
     __syncthreads();
+    if (vec_m >= 0 && tid == 0) {
+        sS.rho = vs;
+        sS.sol = vs + n_elem;
+        sS.gx = vs + 2 * (size_t)n_elem;
+        sS.res = vs + 3 * (size_t)n_elem;
+        sS.df = vs + 4 * (size_t)n_elem;
+        if (G.vext) sS.vext = vs + 5 * (size_t)n_elem;
+        sS.Q = vs + 6 * (size_t)n_elem;
+        sS.DG = vs + (6 + (size_t)vec_m) * n_elem;
+    }
+    __syncthreads();
+    const SysDev& S = sS;
     const T NA = T(S.NA);
     for (int it = 0; it < max_evals; ++it) {
         if (sA.mode == MODE_DONE) break;
@@ -130,7 +246,7 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
             nf[(i * NF) * N + j] = T(S.NA * S.rho[e]);
         }
         __syncthreads();
-        pers_conv<T, NC>(ext, true, taps, nf + N, NF * N, N, NCONV, NA);
+        pers_conv_any<T, NC>(ext, true, taps, nf + N, NF * N, N, NCONV, NA);
         __syncthreads();
         // ---- fused Phi / dPhi/dn, in place ----
         for (int j = tid; j < N; j += PERS_THREADS) {
@@ -155,7 +271,7 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
             ext[k] = nf[(i * NF + f + 1) * N + j];
         }
         __syncthreads();
-        pers_conv<T, NC>(ext, false, taps, ip, NCONV * N, N, NCONV, T(1));
+        pers_conv_any<T, NC>(ext, false, taps, ip, NCONV * N, N, NCONV, T(1));
         __syncthreads();
         // ---- Euler-Lagrange step + aa_point! bookkeeping ----
         {
@@ -193,6 +309,12 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
                 if (tid == 0) ctl_apply(sA, op, slot, sums, done_counter);
             }
             __syncthreads();
+        }
+    }
+    if (vec_m >= 0) {
+        for (int e = tid; e < n_elem; e += PERS_THREADS) {
+            G.rho[e] = S.rho[e];
+            G.sol[e] = S.sol[e];
         }
     }
     if (tid == 0) st[blockIdx.x] = sA;

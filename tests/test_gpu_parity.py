@@ -212,8 +212,11 @@ def test_batch_equals_individual_bitwise(engine):
 
 
 def test_engines_agree():
-    """Grid and persistent engines run the same aasol algorithm: same number of
-    evaluations and profiles equal to rounding (reduction orders differ)."""
+    """Grid and persistent engines run the same aasol algorithm with different
+    summation orders (the persistent engine's convolutions run on the FP64
+    tensor cores).  Their residual histories agree over the first evaluations,
+    until the Anderson steps amplify those rounding differences (within ~40
+    evaluations on the 8 nm pore at 1e7 Pa), and both reach the same fixed point."""
     import cdft_b200 as cd
     for H, p, N in [(2e-9, 1e3, 100), (8e-9, 1e7, 400), (5e-9, 7.2e5, 300)]:
         sp, _ = S.slit_pore(H, p, N)
@@ -222,8 +225,9 @@ def test_engines_agree():
         ra = cd.converge(sp, a, beta=0.1, tol=1e-10, anderson_m=5, engine="grid")
         rb = cd.converge(sp, b, beta=0.1, tol=1e-10, anderson_m=5, engine="persistent")
         assert ra.errcode == rb.errcode == 0
-        assert abs(ra.evaluations - rb.evaluations) <= 1
-        assert float(np.max(np.abs(a / b - 1))) < 1e-9
+        k = min(12, ra.evaluations, rb.evaluations)
+        np.testing.assert_allclose(ra.history[:k], rb.history[:k], rtol=1e-8, atol=1e-12 * ra.history[0])
+        assert float(np.max(np.abs(a / b - 1))) < 1e-8
 
 
 @pytest.mark.parametrize("engine", ["grid", "persistent"])
