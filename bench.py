@@ -34,7 +34,7 @@ PRESSURES = np.logspace(3, 7, 8)
 N_OF_WIDTH = [int(round(100 + 300 * k / 7)) for k in range(8)]
 SOLVER = dict(beta=0.1, tol=1e-10, anderson_m=5, maxit=10000)
 METHANE = dict(m=[1.0], sigma=[3.7039], epsilon=[150.03])
-FP64_PEAK_NOMINAL_TFLOPS = 37.0   # B200 FP64 vector (datasheet); no measured FP64 peak exists for this pool
+FP64_PEAK_NOMINAL_TFLOPS = 37.0   # HGX B200 FP64 / FP64 tensor (datasheet); no measured FP64 peak exists for this pool
 
 
 def isotherm_specs(rank=0):
@@ -247,12 +247,13 @@ def run_ours(args, rank, world, local_rank):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
             "gpu_launches": launches_timed,
             "roofline": {
-                "kernel": ("persistent_kernel (whole batched converge, 1 launch per step)" if args.engine != "grid"
+                "kernel": ("persistent_kernel (whole batched converge, 1 launch per step; circulant "
+                           "convolutions on the FP64 tensor cores, mma.sync m8n8k4 f64)" if args.engine != "grid"
                            else "grid engine (14 launches per evaluation)"),
-                "bound": "fp64" if args.precision == "fp64" else "fp32/fp64",
+                "bound": "tensor",
                 "achieved": round(achieved, 3),
                 "peak": FP64_PEAK_NOMINAL_TFLOPS,
-                "peak_source": "nominal B200 FP64 (MEASURED_PEAKS.json has no FP64 figure)",
+                "peak_source": "nominal HGX B200 FP64 tensor (of nominal: MEASURED_PEAKS.json has no FP64 figure)",
                 "unit": "TFLOP/s",
                 "frac": round(achieved / FP64_PEAK_NOMINAL_TFLOPS, 4),
                 "traffic": None,
@@ -293,18 +294,25 @@ def _solutes3d_system(N, precision):
     return cd.DFTSystem(model, st, cd.HardSphereSolutes(centres, 1.5 * s), cd.DFTOptions(precision))
 
 
-# HBM bytes per grid point of one functional-derivative evaluation of the 3D
-# pipeline, FP64 (8 B reals; the half spectrum holds 16 B per (N/2+1)/N point,
-# counted as 8 B per real point):
+# Algorithmic HBM bytes per grid point per Anderson iteration of the 3D path
+# (nc = 1, NF = 9, m = 10, one V_ext), each array read or written once per stage:
+#   (a) weighted densities  s (nc + (NF-1) nc)          FP64  72
+#   (b) Phi / dPhi          s (2 NF nc)                        144
+#   (c) adjoint + EL        s (NF nc + nc) + 8 (V_ext)          88
+#   (d) Anderson vectors    8 nc (2 m + 6)                     208
+# = 512 B in FP64 (s = 8), 364 B mixed (s = 4); FFT-internal passes are excluded.
+BYTES_3D_ITER = {"fp64": 512, "mixed": 364}
+# What the FFT pipeline of one functional derivative moves per point (x, y, z passes
+# of rho, the 8 convolved fields and the 8 dPhi/dn fields, Phi and the EL output;
+# the half spectrum holds 16 B per (N/2+1)/N point, counted as 8 B per real point):
 #   forward rho: x 8+8, y 16, z + multiply 8+64                    = 104
 #   inverse of the 8 convolved fields: y 128, x 64+64              = 256
 #   Phi: read 9 fields 72, write 8 gradients 64                    = 136
 #   forward of the 8 gradients: x 64+64, y 128                     = 256
 #   z adjoint 64+8, inverse y 16, x 8+8                            = 104
 #   Euler-Lagrange output: rho, V_ext, adjoint in, G(rho) out      =  32
-# total 888 B/point; mixed: the FFT and Phi arrays in FP32 (half), rho, V_ext,
-# adjoint and G in FP64.
-BYTES_3D = {"fp64": 888, "mixed": (104 + 256 + 136 + 256 + 104) // 2 + 32}
+# = 888 B/point in FP64; mixed: FFT and Phi arrays in FP32, the rest FP64.
+BYTES_3D_PIPE = {"fp64": 888, "mixed": (104 + 256 + 136 + 256 + 104) // 2 + 32}
 
 
 def solutes3d_run(N, precision, reps=2):
@@ -356,16 +364,20 @@ def solutes3d_run(N, precision, reps=2):
     sy.close()
     peaks = measured_peaks()
     peak = peaks["hbm_gbs"] if peaks else 6650.0
-    achieved = BYTES_3D[precision] * N ** 3 / (ms_eval.value * 1e-3) / 1e9
+    achieved = BYTES_3D_ITER[precision] * N ** 3 * ips / 1e9
+    pipe = BYTES_3D_PIPE[precision] * N ** 3 / (ms_eval.value * 1e-3) / 1e9
+    src = "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s (of fallback)"
     out = {
         "iterations_per_s": round(ips, 2), "ms_per_converge": round(ms, 3), "evaluations": evals,
         "errcode": res.errcode, "ms_per_iteration": round(ms / evals, 4), "gpu_launches_per_converge": launches,
         "functional_derivative_ms": round(ms_eval.value, 4),
-        "roofline_functional_derivative": {
-            "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
-            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s",
-            "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "algorithmic_bytes_per_point": BYTES_3D[precision]},
+        "roofline": {
+            "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "peak_source": src,
+            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+            "algorithmic_bytes_per_point_iteration": BYTES_3D_ITER[precision]},
+        "functional_derivative_pipeline": {
+            "bytes_per_point": BYTES_3D_PIPE[precision], "achieved_gbs": round(pipe, 1),
+            "frac": round(pipe / peak, 4)},
     }
     return out, rho, omega, fluid
 
