@@ -28,6 +28,7 @@ __all__ = [
     "DFTSystem", "AASol",
     "initialize_profiles", "converge", "batch_converge", "dFdrho_res", "F_res", "F_ideal",
     "free_energy", "surface_tension", "interfacial_tension", "adsorption", "integrate",
+    "F_res_grad", "grad_params", "dgamma_dtheta",
     "CDFTError", "launch_count",
 ]
 
@@ -486,6 +487,45 @@ def adsorption(system, rho):
     """adsorption(system, ρ) (adsorption.jl:182-188), mol/m^3 of the domain."""
     V = np.prod([ub - lb for (lb, ub) in system.structure.bounds])
     return np.array([integrate(rho[i], system.structure) / V for i in range(system.nc)])
+
+
+def F_res_grad(system, rho):
+    """dF_res/d(sigma_k [A], eps_k/k_B [K], m_k) at a fixed profile, shape (nc, 3);
+    units of F_res (1D).  No counterpart in the reference."""
+    _check_rho(system, rho)
+    out = np.zeros(3 * system.nc)
+    _lib.check(_LIB.cdft_free_energy_res_grad(system._plan, _lib.dptr(rho), _lib.dptr(out)))
+    return out.reshape(system.nc, 3)
+
+
+def grad_params(system, rho, dmu_dtheta=None, dp_dtheta=None):
+    """d Omega_ex / d(sigma_k [A], eps_k/k_B [K], m_k) at a converged profile, shape
+    (nc, 3), J/m^2 per parameter unit; Omega_ex is surface_tension's numerator.
+    dmu_dtheta (nc, 3nc) and dp_dtheta (3nc) describe how the bulk state moves with
+    the parameters (None: held fixed)."""
+    _check_rho(system, rho)
+    nt = 3 * system.nc
+    out = np.zeros(nt)
+    mu = None if dmu_dtheta is None else np.ascontiguousarray(dmu_dtheta, dtype=float).reshape(system.nc, nt)
+    dp = None if dp_dtheta is None else np.ascontiguousarray(dp_dtheta, dtype=float).reshape(nt)
+    _lib.check(_LIB.cdft_grad_params(system._plan, _lib.dptr(rho), None if mu is None else _lib.dptr(mu),
+                                     None if dp is None else _lib.dptr(dp), _lib.dptr(out)))
+    return out.reshape(system.nc, 3)
+
+
+def dgamma_dtheta(system, rho):
+    """d gamma / d(sigma_k [A], eps_k/k_B [K], m_k) of a converged TwoPhase1DCart
+    interface (periodic box, two interfaces: gamma = Omega_ex / 2), shape (nc, 3),
+    J/m^2 per parameter unit.  The bulk state follows phase coexistence (pure fluid:
+    saturation; binary: fixed p and T); its sensitivity comes from
+    thermo.coexistence_sensitivity."""
+    s = system.structure
+    if s.kind != "twophase":
+        raise ValueError("dgamma_dtheta needs a TwoPhase1DCart structure")
+    p, T = s.conditions
+    from .thermo import coexistence_sensitivity
+    dmu, dp = coexistence_sensitivity(system.model, T, s.rho_bulk, s.rho_bulk2, p=p)
+    return grad_params(system, rho, dmu, dp) / 2
 
 
 def launch_count(reset=False):

@@ -33,7 +33,7 @@ LIB_PATH = os.environ.get("CDFT_B200_LIB") or os.path.join(os.path.dirname(os.pa
 EXPORTED = [
     "cdft_plan_create", "cdft_plan_destroy",
     "cdft_functional_derivative", "cdft_functional_derivative_dev",
-    "cdft_free_energy_res", "cdft_phi_pointwise",
+    "cdft_free_energy_res", "cdft_phi_pointwise", "cdft_free_energy_res_grad", "cdft_grad_params",
     "cdft_converge", "cdft_converge_dev",
     "cdft_batch_converge", "cdft_batch_converge_dev",
     "cdft_plan_set_stream", "cdft_batch_time_stage", "cdft_functional_derivative_noalloc",
@@ -119,6 +119,8 @@ def load(path=LIB_PATH):
     lib.cdft_functional_derivative_dev.argtypes = [P, P, P]
     lib.cdft_free_energy_res.argtypes = [P, dp, dp]
     lib.cdft_phi_pointwise.argtypes = [P, dp, ctypes.c_int, dp, dp]
+    lib.cdft_free_energy_res_grad.argtypes = [P, dp, dp]
+    lib.cdft_grad_params.argtypes = [P, dp, dp, dp, dp]
     lib.cdft_converge.argtypes = [P, dp, ctypes.POINTER(SolverOpts), ctypes.POINTER(Result)]
     lib.cdft_converge_dev.argtypes = [P, P, ctypes.POINTER(SolverOpts), ctypes.POINTER(Result)]
     lib.cdft_batch_converge.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.POINTER(dp),

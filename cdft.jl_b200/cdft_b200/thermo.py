@@ -46,6 +46,7 @@ class PCSAFT:
         self.epsilon = np.asarray(epsilon, dtype=float)
         nc = len(self.m)
         k = np.zeros((nc, nc)) if kij is None else np.asarray(kij, dtype=float)
+        self.kij = k
         self.sigma_ij = (self.sigma[:, None] + self.sigma[None, :]) / 2
         self.eps_ij = np.sqrt(np.outer(self.epsilon, self.epsilon)) * (1 - k)
         self.assoc = dict(assoc or {})
@@ -56,6 +57,15 @@ class PCSAFT:
     def pure(self, i):
         a = {0: self.assoc[i]} if i in self.assoc else None
         return PCSAFT([self.components[i]], [self.m[i]], [self.sigma[i] * 1e10], [self.epsilon[i]], assoc=a)
+
+    def theta(self):
+        """Model parameters theta = (sigma_k [A], eps_k/k_B [K], m_k) for k < nc, flattened."""
+        return np.column_stack([self.sigma * 1e10, self.epsilon, self.m]).ravel()
+
+    def with_theta(self, theta):
+        """Copy of the model with parameters theta (layout of theta())."""
+        t = np.asarray(theta, dtype=float).reshape(-1, 3)
+        return PCSAFT(self.components, t[:, 2], t[:, 0], t[:, 1], kij=self.kij, assoc=self.assoc)
 
     def length_scale(self):
         return float(self.sigma_ij.max())
@@ -228,3 +238,67 @@ class PCSAFT:
             if done:
                 break
         return x1, x2
+
+
+def coexistence_sensitivity(model, T, rho1, rho2, p=None, rel=1e-6):
+    """Derivatives of a two-phase bulk state with respect to theta = model.theta().
+
+    Pure fluids (VLE): the unknowns (rho1, rho2) solve mu(rho1) = mu(rho2),
+    p(rho1) = p(rho2); binaries at fixed (p, T) (LLE): mu_i(rho1) = mu_i(rho2),
+    p(rho1) = p(rho2) = p.  The implicit-function theorem gives d rho / d theta;
+    partial derivatives by central differences (relative step ``rel``).  Returns
+    (dmu, dp): dmu[i, t] = d mu_i(rho1) / d theta_t in J/mol (total mu of
+    chemical_potential, the one surface_tension uses) and dp[t] in Pa (zero at fixed p).
+    """
+    rho1 = np.asarray(rho1, dtype=float)
+    rho2 = np.asarray(rho2, dtype=float)
+    nc = len(model)
+    if nc > 2:
+        raise NotImplementedError("coexistence sensitivity for pure fluids and binaries")
+    theta = model.theta()
+    nt = theta.size
+    x0 = np.concatenate([rho1, rho2])
+    pscale = R * T * x0.max()
+
+    def resid(x, mdl):
+        a, b = x[:nc], x[nc:]
+        mu = (mdl.chemical_potential(a, T) - mdl.chemical_potential(b, T)) / (R * T)
+        pa, pb = mdl.pressure(a, T), mdl.pressure(b, T)
+        if nc == 1:
+            return np.concatenate([mu, [(pa - pb) / pscale]])
+        return np.concatenate([mu, [(pa - p) / pscale, (pb - p) / pscale]])
+
+    def dtheta(fun):
+        cols = []
+        for t in range(nt):
+            h = rel * max(abs(theta[t]), 1.0)
+            tp, tm = theta.copy(), theta.copy()
+            tp[t] += h
+            tm[t] -= h
+            cols.append((np.asarray(fun(model.with_theta(tp))) - np.asarray(fun(model.with_theta(tm)))) / (2 * h))
+        return np.column_stack(cols)
+
+    J = np.empty((2 * nc, 2 * nc))
+    for j in range(2 * nc):
+        h = rel * x0[j]
+        xp, xm = x0.copy(), x0.copy()
+        xp[j] += h
+        xm[j] -= h
+        J[:, j] = (resid(xp, model) - resid(xm, model)) / (2 * h)
+    dx = -np.linalg.solve(J, dtheta(lambda mdl: resid(x0, mdl)))
+    d1 = dx[:nc]
+    # total derivative of mu(rho1(theta); theta) and p(rho1(theta); theta)
+    dmu = dtheta(lambda mdl: mdl.chemical_potential(rho1, T))
+    dp = dtheta(lambda mdl: [mdl.pressure(rho1, T)])[0]
+    Jmu = np.empty((nc, nc))
+    Jp = np.empty(nc)
+    for j in range(nc):
+        h = rel * rho1[j]
+        rp, rm = rho1.copy(), rho1.copy()
+        rp[j] += h
+        rm[j] -= h
+        Jmu[:, j] = (model.chemical_potential(rp, T) - model.chemical_potential(rm, T)) / (2 * h)
+        Jp[j] = (model.pressure(rp, T) - model.pressure(rm, T)) / (2 * h)
+    dmu = dmu + Jmu @ d1
+    dp = dp + Jp @ d1 if nc == 1 else np.zeros(nt)
+    return dmu, dp

@@ -1037,6 +1037,15 @@ struct KSum {
 // ===========================================================================
 // C ABI
 // ===========================================================================
+// per-point terms of the parameter gradient of F_res (cdft_free_energy_res_grad)
+template <int NC>
+int launch_grad_points(cdft_plan* p, Batch* b, const double* dn, double* gp, double* kt)
+{
+    grad_points_kernel<NC><<<(p->N + 127) / 128, 128, 0, p->stream>>>(b->d_sys, dn, gp, kt);
+    CHECK_LAUNCH();
+    return 0;
+}
+
 extern "C" {
 
 int cdft_plan_create(const cdft_system_desc* desc, cdft_plan** plan)
@@ -1268,6 +1277,184 @@ int cdft_last_error(char* buf, size_t len)
 }
 
 const char* cdft_version(void) { return "cdft_b200 0.1 (sm_100a)"; }
+
+// ---------------------------------------------------------------------------
+// Parameter gradient of F_res and of the excess grand potential (1D)
+// ---------------------------------------------------------------------------
+int cdft_free_energy_res_grad(cdft_plan* plan, const double* rho, double* dF)
+{
+    g_err_code = 0;
+    if (!plan || !rho || !dF) return set_error(CDFT_E_INVALID, "NULL argument");
+    const cdft_system_desc& d = plan->desc;
+    if (d.nd != 1) return set_error(CDFT_E_UNSUPPORTED, "the parameter gradient is implemented for 1D grids");
+    const int nc = d.nc, N = plan->N;
+    const double L = d.L, T = d.T;
+    // the chain below assumes PC-SAFT's diameter d_i = sigma_i (1 - 0.12 exp(-3 eps_i / T)) and the
+    // combining rule sigma_ij = (sigma_i + sigma_j) / 2 (eps_ij = sqrt(eps_i eps_j)(1 - k_ij), any k_ij)
+    for (int i = 0; i < nc; ++i) {
+        const double si = d.sigma[i * nc + i], ei = d.eps[i * nc + i];
+        const double dd = si * (1.0 - 0.12 * exp(-3.0 * ei / T));
+        if (fabs(dd / d.hsd[i] - 1.0) > 1e-9)
+            return set_error(CDFT_E_UNSUPPORTED, "hsd[%d] is not the PC-SAFT diameter of sigma and eps", i);
+        for (int j = 0; j < nc; ++j)
+            if (fabs(d.sigma[i * nc + j] / (0.5 * (si + d.sigma[j * nc + j])) - 1.0) > 1e-12)
+                return set_error(CDFT_E_UNSUPPORTED, "sigma[%d,%d] does not follow (sigma_i + sigma_j) / 2", i, j);
+    }
+    CU(cudaSetDevice(plan->device));
+    Batch* b = nullptr;
+    int rc = self_batch(plan, &b);
+    if (rc) return rc;
+    SysDev& S = plan->sys;
+    const int nconv = S.nconv;
+    const size_t ne = (size_t)S.n_elem;
+    CU(cudaMemcpyAsync(S.rho, rho, ne * sizeof(double), cudaMemcpyHostToDevice, plan->stream));
+    // weighted densities (FP64 in every precision mode)
+    {
+        const size_t smem = (size_t)(CONV_QC + CONV_TILE + CONV_QC + 31) * sizeof(double);
+        conv1d_kernel<double><<<b->ntasks, CONV_WARPS * 32, smem, plan->stream>>>(b->d_tasks, b->d_sys, nullptr, 0);
+        CHECK_LAUNCH();
+    }
+    const int NP = 2 * nc + 2 * nc * nc + 2;
+    const int types[6] = {1, 2, 3, 2, 1, 2};
+    const double wf[6] = {0.5, 0.5, 0.5, 1.0, 1.0, PSI_DISP};
+    double *d_dt = nullptr, *d_dn = nullptr, *d_gp = nullptr, *d_kt = nullptr, *d_scale = nullptr;
+    const size_t ntap = (size_t)nc * nconv * N;
+    CU(cudaMalloc(&d_dt, ntap * sizeof(double)));
+    CU(cudaMalloc(&d_dn, ntap * sizeof(double)));
+    CU(cudaMalloc(&d_gp, (size_t)NP * N * sizeof(double)));
+    CU(cudaMalloc(&d_kt, (size_t)nc * N * sizeof(double)));
+    CU(cudaMalloc(&d_scale, nconv * sizeof(double)));
+    double scale[6];
+    for (int f = 0; f < nconv; ++f) scale[f] = S.NA * 2.0 * 3.14159265358979323846 * wf[f];   // N_A L^3 dR/dd
+    CU(cudaMemcpyAsync(d_scale, scale, nconv * sizeof(double), cudaMemcpyHostToDevice, plan->stream));
+    const double span = d.bounds[0][1] - d.bounds[0][0];
+    for (int i = 0; i < nc; ++i)
+        for (int f = 0; f < nconv; ++f)
+            dtaps1d_kernel<<<(N + 127) / 128, 128, 0, plan->stream>>>(N, span, L, types[f], wf[f] * S.phi.d[i],
+                                                                     d_dt + ((size_t)i * nconv + f) * N);
+    CHECK_LAUNCH();
+    dconv1d_kernel<<<dim3((N + 127) / 128, nc * nconv), 128, 0, plan->stream>>>(N, nconv, d_dt, S.rho, d_scale, d_dn);
+    CHECK_LAUNCH();
+    switch (nc) {
+    case 1: rc = launch_grad_points<1>(plan, b, d_dn, d_gp, d_kt); break;
+    case 2: rc = launch_grad_points<2>(plan, b, d_dn, d_gp, d_kt); break;
+    case 3: rc = launch_grad_points<3>(plan, b, d_dn, d_gp, d_kt); break;
+    case 4: rc = launch_grad_points<4>(plan, b, d_dn, d_gp, d_kt); break;
+    default: rc = set_error(CDFT_E_UNSUPPORTED, "nc=%d", nc);
+    }
+    std::vector<double> gp((size_t)NP * N), kt((size_t)nc * N);
+    if (!rc) {
+        CU(cudaMemcpyAsync(gp.data(), d_gp, gp.size() * sizeof(double), cudaMemcpyDeviceToHost, plan->stream));
+        CU(cudaMemcpyAsync(kt.data(), d_kt, kt.size() * sizeof(double), cudaMemcpyDeviceToHost, plan->stream));
+        CU(cudaStreamSynchronize(plan->stream));
+    }
+    cudaFree(d_dt);
+    cudaFree(d_dn);
+    cudaFree(d_gp);
+    cudaFree(d_kt);
+    cudaFree(d_scale);
+    if (rc) return rc;
+    // Simpson integrals (as cdft_free_energy_res): G[q] = dF_res / dP_q, Gd[i] = dF_res / dd_i via the kernels
+    auto coef = [](int k, int n) { return (k == 1 || k == n) ? 1.0 : ((k % 2 == 0) ? 4.0 : 2.0); };
+    const double w = (plan->dz[0] / 3.0) / (L * L * L);
+    std::vector<double> G(NP), Gd(nc);
+    for (int q = 0; q < NP; ++q) {
+        KSum acc;
+        for (int k = 1; k <= N; ++k) acc.add(coef(k, N) * gp[(size_t)q * N + k - 1]);
+        G[q] = acc.value() * w;
+    }
+    for (int i = 0; i < nc; ++i) {
+        KSum acc;
+        for (int k = 1; k <= N; ++k) acc.add(coef(k, N) * kt[(size_t)i * N + k - 1]);
+        Gd[i] = acc.value() * w;
+    }
+    // chain to theta = (sigma_k [A], eps_k / k_B [K], m_k) with the length unit L held fixed
+    const int iM = 0, iD = nc, iC1 = 2 * nc, iC2 = 2 * nc + nc * nc, iAD = 2 * nc + 2 * nc * nc, iAK = iAD + 1;
+    const PhiParams& P = S.phi;
+    for (int k = 0; k < nc; ++k) {
+        const double sk = d.sigma[k * nc + k], ek = d.eps[k * nc + k];
+        const double ex = exp(-3.0 * ek / T);
+        // reduced diameter d_k / L: derivatives per m of sigma and per K of eps
+        const double dd_ds = (1.0 - 0.12 * ex) / L;
+        const double dd_de = sk * 0.36 / T * ex / L;
+        double g_s = 0.0, g_e = 0.0, g_m = 0.0;
+        // explicit dependence on d_k (FMT, chain, dispersion, association u_c) and through the kernels
+        g_s += (G[iD + k] + Gd[k]) * dd_ds;
+        g_e += (G[iD + k] + Gd[k]) * dd_de;
+        g_m += G[iM + k];
+        for (int i = 0; i < nc; ++i)
+            for (int j = 0; j < nc; ++j) {
+                const int dik = (i == k) + (j == k);
+                if (!dik) continue;
+                const double sg = d.sigma[i * nc + j] / L, e = d.eps[i * nc + j];
+                const double mm = d.m[i] * d.m[j];
+                const double c1 = mm * sg * sg * sg * e / T;
+                // c1 = m_i m_j sg^3 e / T, c2 = c1 e / T; d sg / d sigma_k = dik / (2 L); d e / d eps_k = e dik / (2 eps_k)
+                const double dc1_dm = ((i == k) * d.m[j] + (j == k) * d.m[i]) * sg * sg * sg * e / T;
+                const double dc1_ds = mm * 3.0 * sg * sg * (0.5 * dik / L) * e / T;
+                const double dc1_de = mm * sg * sg * sg / T * (e * 0.5 * dik / ek);
+                const double de = e * 0.5 * dik / ek;
+                g_m += G[iC1 + i * nc + j] * dc1_dm + G[iC2 + i * nc + j] * dc1_dm * e / T;
+                g_s += G[iC1 + i * nc + j] * dc1_ds + G[iC2 + i * nc + j] * dc1_ds * e / T;
+                g_e += G[iC1 + i * nc + j] * dc1_de + G[iC2 + i * nc + j] * (dc1_de * e / T + c1 * de / T);
+            }
+        if (P.has_assoc) {
+            const int ic = P.a_ic, jc = P.a_jc;
+            const double di = P.d[ic], dj = P.d[jc], den = (di + dj) * (di + dj);
+            // a_dij = d_i d_j / (d_i + d_j)
+            const double dA_dk = (ic == k ? dj * dj / den : 0.0) + (jc == k ? di * di / den : 0.0);
+            g_s += G[iAD] * dA_dk * dd_ds;
+            g_e += G[iAD] * dA_dk * dd_de;
+            // a_K = sg^3 (exp(eps_AB / T) - 1) kappa_AB with sg = sigma_{ic,jc} / L
+            const int dik = (ic == k) + (jc == k);
+            if (dik) {
+                const double sg = d.sigma[ic * nc + jc] / L;
+                g_s += G[iAK] * 3.0 * (P.a_K / sg) * (0.5 * dik / L);
+            }
+        }
+        dF[3 * k + 0] = g_s * 1e-10;   // per Angstrom
+        dF[3 * k + 1] = g_e;
+        dF[3 * k + 2] = g_m;
+    }
+    return 0;
+}
+
+int cdft_grad_params(cdft_plan* plan, const double* rho, const double* dmu_dtheta, const double* dp_dtheta,
+                     double* dOmega)
+{
+    g_err_code = 0;
+    if (!plan || !rho || !dOmega) return set_error(CDFT_E_INVALID, "NULL argument");
+    const cdft_system_desc& d = plan->desc;
+    if (plan->d_vext)
+        return set_error(CDFT_E_UNSUPPORTED, "external fields depend on the parameters and are not differentiated");
+    const int nc = d.nc, N = plan->N, np = 3 * nc;
+    std::vector<double> dF(np);
+    int rc = cdft_free_energy_res_grad(plan, rho, dF.data());
+    if (rc) return rc;
+    // Simpson integrals of rho_i (mol/m^2) and of 1 (m), as surface_tension's
+    auto coef = [](int k, int n) { return (k == 1 || k == n) ? 1.0 : ((k % 2 == 0) ? 4.0 : 2.0); };
+    std::vector<double> nint(nc);
+    double one = 0.0;
+    for (int i = 0; i < nc; ++i) {
+        KSum acc;
+        for (int k = 1; k <= N; ++k) acc.add(coef(k, N) * rho[(size_t)i * N + k - 1]);
+        nint[i] = acc.value() * plan->dz[0] / 3.0;
+    }
+    {
+        KSum acc;
+        for (int k = 1; k <= N; ++k) acc.add(coef(k, N));
+        one = acc.value() * plan->dz[0] / 3.0;
+    }
+    const double kB = 1.380649e-23;
+    for (int t = 0; t < np; ++t) {
+        double v = kB * d.T * dF[t];
+        if (dmu_dtheta)
+            for (int i = 0; i < nc; ++i) v -= dmu_dtheta[(size_t)i * np + t] * nint[i];
+        if (dp_dtheta) v += dp_dtheta[t] * one;
+        dOmega[t] = v;
+    }
+    return 0;
+}
 
 }  // extern "C"
 

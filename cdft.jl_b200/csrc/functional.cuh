@@ -54,9 +54,25 @@ __device__ __forceinline__ void wb_bracket(double n3, double D, double Lg, doubl
          - 1.0 / (c12 * n3 * n3 * D * D) + 2.0 / (c12 * n3 * D * D * D);
 }
 
-template <typename T, int NC, int ND>
-__device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + ND], T (&g)[NC][6 + ND])
+// Layout of the parameter gradient of Phi (phi_grad with PG = true): the entries of
+// PhiParams the functional depends on, m_i, d_i, c1_ij, c2_ij, the association d_ij and K.
+template <int NC> struct PhiParamIdx {
+    static constexpr int M = 0, D = NC, C1 = 2 * NC, C2 = 2 * NC + NC * NC, ADIJ = 2 * NC + 2 * NC * NC,
+                         AK = ADIJ + 1, NP = AK + 1;
+};
+
+// Phi and dPhi/dn at one point (reverse sweep).  PG = true also accumulates
+// dPhi/dP into gp[PhiParamIdx<NC>::NP] (same sweep, FP64): the explicit parameter
+// dependence used by the parameter gradient of F_res; PG = false compiles to the
+// plain evaluation.
+template <typename T, int NC, int ND, bool PG = false>
+__device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + ND], T (&g)[NC][6 + ND],
+                                      double* gp = nullptr)
 {
+    using PI_ = PhiParamIdx<NC>;
+    if constexpr (PG) {
+        for (int q = 0; q < PI_::NP; ++q) gp[q] = 0.0;
+    }
     constexpr int NF = 6 + ND;
     constexpr int F2 = 1, F3 = 2, FV = 3, IHC = 3 + ND, ILAM = 4 + ND, IDISP = 5 + ND;
     const T pi = T(3.14159265358979323846);
@@ -118,6 +134,25 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
 #pragma unroll
             for (int k = 0; k < ND; ++k) g[i][FV + k] += mi * (g_nv1[k] / di - two_pi * g_nv2[k]);
         }
+        if constexpr (PG) {
+            // n0, n1, n2, nv1, nv2, n3 are linear in m_i; n0, n2, nv1 carry d_i
+#pragma unroll
+            for (int i = 0; i < NC; ++i) {
+                const double mi = P.m[i], di = P.d[i];
+                const double f2 = double(n[i][F2]), f3 = double(n[i][F3]);
+                double gm = double(g_n0) * f2 / di + 0.5 * double(g_n1) * f2 + 3.14159265358979323846 * double(g_n2) * f2 * di
+                            + double(g_n3) * f3;
+                double gd = -double(g_n0) * f2 * mi / (di * di) + 3.14159265358979323846 * double(g_n2) * f2 * mi;
+#pragma unroll
+                for (int k = 0; k < ND; ++k) {
+                    const double nvi = double(n[i][FV + k]);
+                    gm += double(g_nv1[k]) * nvi / di - 2.0 * 3.14159265358979323846 * double(g_nv2[k]) * nvi;
+                    gd -= double(g_nv1[k]) * nvi * mi / (di * di);
+                }
+                gp[PI_::M + i] += gm;
+                gp[PI_::D + i] += gd;
+            }
+        }
     }
 
     // ---------------- hard chain (PCSAFT.jl:123-144) ----------------
@@ -136,7 +171,16 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
 #pragma unroll
         for (int i = 0; i < NC; ++i) {
             const T am1 = T(P.m[i]) - T(1);
-            if (am1 == T(0)) continue;   // exact zero contribution (m_i = 1)
+            if (am1 == T(0)) {   // exact zero contribution (m_i = 1); its m_i-derivative is not zero
+                if constexpr (PG) {
+                    const double di = P.d[i];
+                    const double lam = double(n[i][ILAM]) / (2.0 * di);
+                    const double y = double(I) + 1.5 * di * double(z2) * double(I2)
+                                     + 0.5 * di * di * double(z2) * double(z2) * double(I3);
+                    gp[PI_::M + i] += -double(n[i][0]) * log(fabs(y * lam / double(n[i][0])));
+                }
+                continue;
+            }
             const T di = T(P.d[i]);
             const T rho = n[i][0];
             const T lam = n[i][ILAM] / (T(2) * di);
@@ -148,9 +192,24 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
             const T gy = -rho * am1 / y;
             gz3 += gy * (I2 + T(3) * di * z2 * I3 + T(1.5) * di * di * z2 * z2 * I4);
             gz2 += gy * (T(1.5) * di * I2 + di * di * z2 * I3);
+            if constexpr (PG) {
+                // (m_i - 1) factor; explicit d_i in y and in lambda = n / (2 d_i)
+                gp[PI_::M + i] += -double(rho) * double(lg);
+                gp[PI_::D + i] += double(gy) * (1.5 * double(z2) * double(I2) + double(di) * double(z2) * double(z2) * double(I3))
+                                  + double(rho) * double(am1) / double(di);
+            }
         }
 #pragma unroll
         for (int i = 0; i < NC; ++i) g[i][IHC] += T(P.m[i]) / T(8) * (gz3 + gz2 / T(P.d[i]));
+        if constexpr (PG) {
+            // z3 = sum m_i n_i / 8, z2 = sum m_i n_i / (8 d_i)
+#pragma unroll
+            for (int i = 0; i < NC; ++i) {
+                const double nh = double(n[i][IHC]), di = P.d[i];
+                gp[PI_::M + i] += double(gz3) * nh / 8.0 + double(gz2) * nh / (8.0 * di);
+                gp[PI_::D + i] += -double(gz2) * P.m[i] * nh / (8.0 * di * di);
+            }
+        }
     }
 
     // ---------------- dispersion (PCSAFT.jl:150-211) ----------------
@@ -232,6 +291,18 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
             const T gr = g_m * (T(P.m[i]) - mbar) / S + g_e * pi / T(6) * T(P.m[i]) * d3
                          + g_s1 * T(2) * rc1[i] + g_s2 * T(2) * rc2[i];
             g[i][IDISP] += gr * factor / d3;
+            if constexpr (PG) {
+                // r_i = n_i factor / d_i^3; mbar = M / S; eta = pi/6 sum m_i r_i d_i^3 (explicit d_i^3)
+                const double ri = double(r[i]);
+                gp[PI_::M + i] += double(g_m) * ri / double(S) + double(g_e) * 3.14159265358979323846 / 6.0 * ri * double(d3);
+                gp[PI_::D + i] += double(gr) * (-3.0 * ri / double(di))
+                                  + double(g_e) * 3.14159265358979323846 / 2.0 * P.m[i] * ri * double(di) * double(di);
+#pragma unroll
+                for (int j = 0; j < NC; ++j) {
+                    gp[PI_::C1 + i * NC + j] += double(g_s1) * ri * double(r[j]);
+                    gp[PI_::C2 + i * NC + j] += double(g_s2) * ri * double(r[j]);
+                }
+            }
         }
     }
 
@@ -330,6 +401,29 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
 #pragma unroll
             for (int k = 0; k < ND; ++k)
                 g[i][FV + k] += T(gg * dg_dxi * (-2.0 * nv2m[k] / (n2m * n2m)) * (-TWO_PI * P.m[i]));
+        }
+        if constexpr (PG) {
+            gp[PI_::AK] += gDelta * ghs;
+            gp[PI_::ADIJ] += gg * (0.5 * xim * n2m * I * I + dij * n2m * n2m * xim * I * I * I / 9.0);
+#pragma unroll
+            for (int i = 0; i < NC; ++i) {
+                const double f2 = double(n[i][F2]);
+                double gm = g_n2m * PI * f2 * P.d[i] + g_n3m * double(n[i][F3]);
+#pragma unroll
+                for (int k = 0; k < ND; ++k)
+                    gm += gg * dg_dxi * (-2.0 * nv2m[k] / (n2m * n2m)) * (-TWO_PI * double(n[i][FV + k]));
+                gp[PI_::M + i] += gm;
+                gp[PI_::D + i] += g_n2m * PI * f2 * P.m[i];
+            }
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {   // u_c = n0_c xi_c with n0_c = n_F2 / d_c, n2_c = pi n_F2 d_c
+                const int c = s == 0 ? ic : jc;
+                const double dc = P.d[c];
+                const double du = xic[s] * (-n0c[s] / dc) + n0c[s] * (2.0 * sqc[s] / (n2c[s] * n2c[s] * n2c[s])) * (n2c[s] / dc);
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                    if (i == c) gp[PI_::D + i] += gu[s] * du;
+            }
         }
     }
     return phi;

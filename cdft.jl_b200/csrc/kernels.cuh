@@ -681,6 +681,84 @@ __global__ void taps1d_kernel(int N, double span, double L, int type, double wid
     taps[q] = acc / (double)N;
 }
 
+// ---------------------------------------------------------------------------
+// Parameter gradient of F_res (1D): derivative taps, rho * dtaps, per-point terms.
+// ---------------------------------------------------------------------------
+// d omega_hat / dR of kernel_hat_1d (same type codes; type 3 returns the imaginary part)
+__device__ __forceinline__ double kernel_hat_1d_dR(int type, double w, double R)
+{
+    const double PI = 3.14159265358979323846, TWO_PI = 2.0 * PI;
+    const double wb = fabs(w);
+    if (type == 1) return 2.0 * cos(wb * R) / TWO_PI;
+    if (type == 2) {
+        if (wb == 0.0) return 4.0 * PI * R * R / (TWO_PI * TWO_PI * TWO_PI);
+        return 4.0 * PI * R * sin(wb * R) / wb / (TWO_PI * TWO_PI * TWO_PI);
+    }
+    if (wb == 0.0) return 4.0 * PI / (TWO_PI * TWO_PI * TWO_PI);
+    return 4.0 * PI * w * R * sin(wb * R) / wb / (TWO_PI * TWO_PI * TWO_PI);
+}
+
+// d taps / dR: Re(IDFT(d omega_hat / dR)), the derivative of taps1d_kernel's output
+__global__ void dtaps1d_kernel(int N, double span, double L, int type, double width_red, double* __restrict__ dtaps)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= N) return;
+    const double R = 2.0 * 3.14159265358979323846 * width_red;
+    double acc = 0.0;
+    const int half = (N + 1) / 2;
+    for (int k = 0; k < N; ++k) {
+        const int kk = (k < half) ? k : k - N;
+        const double w = (double)kk / span * L;
+        const long long ph = ((long long)k * (long long)q) % N;
+        double sn, cs;
+        sincospi(2.0 * (double)ph / (double)N, &sn, &cs);
+        const double K = kernel_hat_1d_dR(type, w, R);
+        acc += (type == 3) ? -K * sn : K * cs;
+    }
+    dtaps[q] = acc / (double)N;
+}
+
+// dn[(i*nconv + f)*N + j] = scale[f] * sum_q dtaps[(i*nconv + f)*N + q] rho[i*N + (j - q) mod N]
+__global__ void dconv1d_kernel(int N, int nconv, const double* __restrict__ dtaps, const double* __restrict__ rho,
+                               const double* __restrict__ scale, double* __restrict__ dn)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int slot = blockIdx.y;   // i * nconv + f
+    if (j >= N) return;
+    const int i = slot / nconv, f = slot - i * nconv;
+    const double* t = dtaps + (size_t)slot * N;
+    const double* r = rho + (size_t)i * N;
+    double acc = 0.0;
+    int src = j;
+    for (int q = 0; q < N; ++q) {
+        acc = fma(t[q], r[src], acc);
+        src = (src == 0) ? N - 1 : src - 1;
+    }
+    dn[(size_t)slot * N + j] = acc * scale[f];
+}
+
+// per point j: gp[q*N + j] = dPhi/dP_q (explicit parameters) and
+// kt[i*N + j] = sum_f dPhi/dn_{i,f} * dn_{i,f}/dd_i (kernels)
+template <int NC>
+__global__ void grad_points_kernel(const SysDev* __restrict__ sys, const double* __restrict__ dn,
+                                   double* __restrict__ gp_out, double* __restrict__ kt_out)
+{
+    const SysDev& S = sys[0];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= S.N) return;
+    double n[NC][7], g[NC][7];
+    double gp[PhiParamIdx<NC>::NP];
+    load_n<double, NC, 1>(S, j, n);
+    phi_grad<double, NC, 1, true>(S.phi, n, g, gp);
+    for (int q = 0; q < PhiParamIdx<NC>::NP; ++q) gp_out[(size_t)q * S.N + j] = gp[q];
+#pragma unroll
+    for (int i = 0; i < NC; ++i) {
+        double acc = 0.0;
+        for (int f = 0; f < S.nconv; ++f) acc += g[i][f + 1] * dn[((size_t)i * S.nconv + f) * S.N + j];
+        kt_out[(size_t)i * S.N + j] = acc;
+    }
+}
+
 __global__ void to_float_kernel(const double* __restrict__ a, float* __restrict__ b, size_t n)
 {
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;

@@ -146,6 +146,29 @@ int cdft_free_energy_res(cdft_plan* plan, const double* rho, double* F);
  * differentiate f_res (PCSAFT.jl:110-117). */
 int cdft_phi_pointwise(cdft_plan* plan, const double* n, int npts, double* fval, double* dphi);
 
+/* Parameter gradient of F_res at a fixed profile (1D): dF[3k + 0..2] =
+ * dF_res/d(sigma_k [A], eps_k/k_B [K], m_k) in the units of cdft_free_energy_res,
+ * with the PC-SAFT diameter d = sigma (1 - 0.12 exp(-3 eps/T)) and
+ * sigma_ij = (sigma_i + sigma_j)/2 (CDFT_E_UNSUPPORTED otherwise).  Explicit
+ * parameter dependence of Phi (f_res, PCSAFT.jl:110-117) from the same reverse sweep
+ * as dPhi/dn; dependence through the kernels (weighted_densities.jl:48-69, widths
+ * PCSAFT.jl:55-61) as sum_alpha <dPhi/dn_alpha, rho * d omega_alpha / d theta>.  The
+ * reference has no counterpart (it differentiates f_res in n only, models.jl:355-411). */
+int cdft_free_energy_res_grad(cdft_plan* plan, const double* rho, double* dF);
+
+/* d Omega_ex / d theta at a converged profile (1D), theta = (sigma_k [A], eps_k/k_B [K],
+ * m_k) for k < nc, Omega_ex = F k_B T - sum_i mu_i int rho_i + p int 1 (J/m^2): the
+ * numerator of surface_tension(system, ρ), src/methods/surface_tension.jl:31-53
+ * (interfacial tension = Omega_ex, or Omega_ex / 2 for the periodic two-interface
+ * box, :28).  At a converged profile delta Omega / delta rho = 0, so
+ *   dOmega_ex/dtheta = k_B T dF_res/dtheta|_rho - sum_i dmu_i/dtheta int rho_i + dp/dtheta int 1.
+ * dmu_dtheta (nc x 3nc, row i = d mu_i / d theta in J/mol) and dp_dtheta (3nc, Pa) are
+ * the caller's derivatives of the bulk state the structure was built on (e.g. along
+ * phase coexistence); NULL means held fixed.  Plans with an external field are refused
+ * (CDFT_E_UNSUPPORTED): V_ext depends on the parameters and is not differentiated. */
+int cdft_grad_params(cdft_plan* plan, const double* rho, const double* dmu_dtheta, const double* dp_dtheta,
+                     double* dOmega);
+
 /* Converge rho in place.  Replaces converge!(prob::DFTProblem, method::AASol, ρ),
  * src/methods/converge.jl:220-254, running aasol (src/utils/anderson.jl:301-443)
  * on the device; rho_inout holds the initial profile on entry and

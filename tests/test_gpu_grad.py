@@ -1,0 +1,124 @@
+"""Parameter gradients through the C ABI, against central finite differences.
+
+theta = (sigma_k [A], eps_k/k_B [K], m_k) for every component k.  The reference has
+no parameter gradient (it differentiates f_res in the weighted densities only,
+models.jl:355-411), so the checks are central differences:
+
+- dF_res/dtheta at a fixed profile against the oracle's F_res with perturbed
+  parameters (FMT, chain, dispersion, association, and the kernels through the
+  hard-sphere diameter);
+- d gamma/dtheta of the water/n-octane liquid-liquid interface (the differentiation
+  configuration, on a shorter grid) against gamma recomputed through the whole
+  pipeline at theta +- h: bulk coexistence, converge from the converged profile,
+  surface tension.
+"""
+import numpy as np
+import pytest
+
+import _systems as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_model(names, theta):
+    from oracle import pcsaft_bulk as pb
+    t = np.asarray(theta, dtype=float).reshape(-1, 3)
+    P = [S.PARAMS[n] for n in names]
+    assoc = [(i, i, p["assoc"][0], p["assoc"][1]) for i, p in enumerate(P) if "assoc" in p]
+    return pb.PCSAFTModel(names, t[:, 2], t[:, 0], t[:, 1], assoc=assoc)
+
+
+CASES = {
+    "methane_wall": (["methane"], lambda: S.methane_wall(N=201)),
+    "octane_vle": (["octane"], lambda: S.octane_vle(N=256)),
+    "water_octane_lle": (["water", "octane"], lambda: S.water_octane_lle(N=256)),
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_F_res_grad_matches_oracle_fd(case):
+    """Hand-written parameter gradient of F_res vs the oracle's central differences
+    (relative step 1e-5: truncation ~1e-10, rounding ~1e-11 relative)."""
+    import cdft_b200 as cd
+    from oracle import functional as fn
+    names, build = CASES[case]
+    sp, so = build()
+    rng = np.random.default_rng(5)
+    rho = S.random_smooth_profile(sp, rng, amp=0.2)
+    g = cd.F_res_grad(sp, rho).ravel()
+    theta0 = sp.model.theta()
+    fd = np.empty_like(theta0)
+    for t in range(theta0.size):
+        h = 1e-5 * abs(theta0[t])
+        vals = []
+        for sgn in (1.0, -1.0):
+            th = theta0.copy()
+            th[t] += sgn * h
+            st = fn.DFTSystem(_oracle_model(names, th), so.structure, so.walls)
+            vals.append(st.F_res(rho))
+        fd[t] = (vals[0] - vals[1]) / (2 * h)
+    # each entry against its own size, floored at 1e-4 of the largest: the differences
+    # carry rounding noise eps |F_res| / h, which for the smallest entries (a component's
+    # sigma in a mixture dominated by the other) is ~1e-6 of the entry itself
+    scale = np.maximum(np.abs(fd), 1e-4 * np.max(np.abs(fd)))
+    err = np.abs(g - fd) / scale
+    assert float(np.max(err)) < 1e-6, (g, fd)
+
+
+def test_grad_params_refuses_external_fields_and_3d():
+    """V_ext (Steele walls, solutes) depends on the parameters and is not differentiated:
+    cdft_grad_params refuses such plans; the 3D engine has no parameter gradient."""
+    import cdft_b200 as cd
+    from cdft_b200._lib import CDFTError
+    sp, _ = S.methane_wall(N=101)
+    rho = cd.initialize_profiles(sp)
+    cd.F_res_grad(sp, rho)   # F_res itself carries no external field
+    with pytest.raises(CDFTError):
+        cd.grad_params(sp, rho)
+    pm, _ = S.models(["argon"])
+    s3 = cd.DFTSystem(pm, cd.Uniform3DCart((1e5, 100.0), [0.021e30 / cd.N_A], [0.0, 8 * 3.4e-10], 32))
+    with pytest.raises(CDFTError):
+        cd.F_res_grad(s3, cd.initialize_profiles(s3))
+
+
+def _lle_system(model, N, box_sigmas=60.0, T=298.15, p=1e5):
+    import cdft_b200 as cd
+    x1, x2 = model.lle(p, T)
+    r1 = model.molar_density(p, T, x1, "liquid") * x1
+    r2 = model.molar_density(p, T, x2, "liquid") * x2
+    s = model.sigma[0]
+    half = box_sigmas * s / 2
+    st = cd.TwoPhase1DCart((p, T), list(r1), list(r2), [-half, half], N)
+    return cd.DFTSystem(model, st)
+
+
+def test_dgamma_dtheta_water_octane_matches_fd():
+    """d gamma/dtheta (adjoint at the converged profile + coexistence sensitivity) vs
+    central differences of gamma through bulk LLE, converge and surface tension."""
+    import cdft_b200 as cd
+    pm, _ = S.models(["water", "octane"])
+    N = 256
+    kw = dict(beta=0.01, tol=1e-12, anderson_m=5, maxit=20000)
+    sys0 = _lle_system(pm, N)
+    rho0 = cd.initialize_profiles(sys0)
+    res = cd.converge(sys0, rho0, **kw)
+    assert res.errcode == 0
+    grad = cd.dgamma_dtheta(sys0, rho0).ravel()
+    theta0 = pm.theta()
+    fd = np.empty_like(theta0)
+    for t in range(theta0.size):
+        h = 1e-5 * abs(theta0[t])
+        vals = []
+        for sgn in (1.0, -1.0):
+            th = theta0.copy()
+            th[t] += sgn * h
+            mdl = pm.with_theta(th)
+            st = _lle_system(mdl, N)
+            r = rho0.copy()
+            rr = cd.converge(st, r, **kw)
+            assert rr.errcode in (0, -1)
+            vals.append(cd.surface_tension(st, r) / 2)
+            st.close()
+        fd[t] = (vals[0] - vals[1]) / (2 * h)
+    err = np.abs(grad - fd) / np.max(np.abs(fd))
+    assert float(np.max(err)) < 1e-5, (grad, fd)
