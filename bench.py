@@ -46,6 +46,20 @@ def isotherm_specs(rank=0):
     return out
 
 
+def max_over_ranks(value, dist, device):
+    """Max of a per-rank time over all ranks (all_reduce MAX), then a barrier."""
+    import torch
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, ms_max):
+    """Units per second of the whole job: every rank's units over the slowest rank's time."""
+    return units_per_rank * world / (ms_max * 1e-3)
+
+
 def build_systems(specs, precision):
     import cdft_b200 as cd
     model = cd.PCSAFT(["methane"], **METHANE)
@@ -184,10 +198,7 @@ def run_ours(args, rank, world, local_rank):
             total += e0.elapsed_time(e1)
         torch.cuda.synchronize()
         if dist:
-            t = torch.tensor([total], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total = float(t.item())
-            dist.barrier()
+            total = max_over_ranks(total, dist, "cuda")
         return total / steps
 
     cd.launch_count(reset=True)
@@ -218,7 +229,7 @@ def run_ours(args, rank, world, local_rank):
     achieved = step_flops / (ms_dev * 1e-3) / 1e12
     plain = plain_fp64_gpu(specs) if (rank == 0 and args.plain) else None
     total_units = n * world
-    value = total_units / (ms_dev * 1e-3)
+    value = whole_job_rate(n, world, ms_dev)
     h2d = sum(r.nbytes for r in rho0)
     line = None
     if rank == 0:
