@@ -625,12 +625,12 @@ int launch_iteration(Batch* b)
     int rc = launch_eval_stages<T>(b, b->d_st, true);
     if (rc) return rc;
     el_kernel<T><<<b->nechunks, ELEM_THREADS, 0, b->stream>>>(b->d_echunks, b->d_sys, b->d_st, b->d_partials);
-    const int ctl_blocks = (b->nsys * 32 + 127) / 128;
-    ctl_kernel<<<ctl_blocks, 128, 0, b->stream>>>(b->d_sys, b->d_st, b->d_partials, b->nsys, 0, b->d_done);
+    const int ctl_blocks = b->nsys;
+    ctl_kernel<<<ctl_blocks, CTL_THREADS, 0, b->stream>>>(b->d_sys, b->d_st, b->d_partials, b->nsys, 0, b->d_done);
     for (int slot = 1; slot <= N_VEC_SLOTS; ++slot) {
         vec_kernel<<<b->nechunks, ELEM_THREADS, 0, b->stream>>>(b->d_echunks, b->d_sys, b->d_st, b->d_partials, slot);
         if (slot < N_VEC_SLOTS)
-            ctl_kernel<<<ctl_blocks, 128, 0, b->stream>>>(b->d_sys, b->d_st, b->d_partials, b->nsys, slot, b->d_done);
+            ctl_kernel<<<ctl_blocks, CTL_THREADS, 0, b->stream>>>(b->d_sys, b->d_st, b->d_partials, b->nsys, slot, b->d_done);
     }
     g_launches += 2 * N_VEC_SLOTS;   // el, ctl0, 5 vec, 4 ctl (eval stages counted above)
     CHECK_LAUNCH();

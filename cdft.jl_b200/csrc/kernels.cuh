@@ -167,7 +167,9 @@ __device__ __forceinline__ void block_reduce_store(double* vals, int K, double* 
 {
     __shared__ double red[BLOCK / 32][RED_SLOTS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int c = 0; c < K; ++c) {
+#pragma unroll
+    for (int c = 0; c < RED_SLOTS; ++c) {
+        if (c >= K) break;
         double v = vals[c];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -245,11 +247,15 @@ el_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
 // Applies slot operation `op` to the elements e = e0, e0 + stride, ... < e1 of
 // one system and accumulates this thread's partial sums into acc[0..K).
 // Returns K (0 for the solution updates, which reduce nothing).
+// Column loops are unrolled to the compile-time bound CDFT_MAX_M and left early, so
+// the per-element history row and the partial sums stay in registers; dot products
+// use the values just computed instead of reading them back.
 __device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AAState& A, int e0, int e1, int stride,
                                             double* acc)
 {
     const int n = S.n_elem;
     const int m = A.m;
+    double* __restrict__ Q = S.Q;
     switch (op) {
     case OP_NORM_DF:
         for (int e = e0; e < e1; e += stride) {
@@ -259,19 +265,36 @@ __device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AASta
         return 1;
     case OP_DOT_H1: {
         const int K = A.kq;
+        const bool down = A.downdate;
         for (int e = e0; e < e1; e += stride) {
-            if (A.downdate) {   // Q[:, 1:m-1] = Q * Qx; Q[:, m] = 0  (downdate_aaqr!)
-                double row[CDFT_MAX_M];
-                for (int r = 0; r < m; ++r) row[r] = S.Q[(size_t)r * n + e];
-                for (int cc = 0; cc < m - 1; ++cc) {
-                    double v = 0.0;
-                    for (int r = 0; r < m; ++r) v += row[r] * A.Qx[r + cc * m];
-                    S.Q[(size_t)cc * n + e] = v;
-                }
-                S.Q[(size_t)(m - 1) * n + e] = 0.0;
-            }
             const double dv = S.df[e];
-            for (int cc = 0; cc < K; ++cc) acc[cc] += S.Q[(size_t)cc * n + e] * dv;
+            if (down) {   // Q[:, 1:m-1] = Q * Qx; Q[:, m] = 0  (downdate_aaqr!)
+                double row[CDFT_MAX_M];
+#pragma unroll
+                for (int r = 0; r < CDFT_MAX_M; ++r) {
+                    if (r >= m) break;
+                    row[r] = Q[(size_t)r * n + e];
+                }
+#pragma unroll
+                for (int cc = 0; cc < CDFT_MAX_M - 1; ++cc) {
+                    if (cc >= m - 1) break;
+                    double v = 0.0;
+#pragma unroll
+                    for (int r = 0; r < CDFT_MAX_M; ++r) {
+                        if (r >= m) break;
+                        v += row[r] * A.Qx[r + cc * m];
+                    }
+                    Q[(size_t)cc * n + e] = v;
+                    if (cc < K) acc[cc] += v * dv;
+                }
+                Q[(size_t)(m - 1) * n + e] = 0.0;
+            } else {
+#pragma unroll
+                for (int cc = 0; cc < CDFT_MAX_M; ++cc) {
+                    if (cc >= K) break;
+                    acc[cc] += Q[(size_t)cc * n + e] * dv;
+                }
+            }
         }
         return K;
     }
@@ -279,11 +302,21 @@ __device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AASta
     case OP_SUB_NORM: {
         const int kq = A.kq;
         for (int e = e0; e < e1; e += stride) {
+            double q[CDFT_MAX_M];
             double v = S.df[e];
-            for (int cc = 0; cc < kq; ++cc) v += (-A.coef[cc]) * S.Q[(size_t)cc * n + e];  // gemv, alpha=-1
+#pragma unroll
+            for (int cc = 0; cc < CDFT_MAX_M; ++cc) {
+                if (cc >= kq) break;
+                q[cc] = Q[(size_t)cc * n + e];
+                v += (-A.coef[cc]) * q[cc];   // gemv, alpha = -1
+            }
             S.df[e] = v;
             if (op == OP_SUB_DOT) {
-                for (int cc = 0; cc < kq; ++cc) acc[cc] += S.Q[(size_t)cc * n + e] * v;
+#pragma unroll
+                for (int cc = 0; cc < CDFT_MAX_M; ++cc) {
+                    if (cc >= kq) break;
+                    acc[cc] += q[cc] * v;
+                }
             } else {
                 acc[0] += v * v;
             }
@@ -295,10 +328,14 @@ __device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AASta
         const int K = A.mk;
         const double r = A.rnorm;
         for (int e = e0; e < e1; e += stride) {
-            const double q = S.df[e] / r;
-            S.Q[(size_t)kq * n + e] = q;
+            const double qn = S.df[e] / r;
+            Q[(size_t)kq * n + e] = qn;
             const double rv = S.res[e];
-            for (int cc = 0; cc < K; ++cc) acc[cc] += S.Q[(size_t)cc * n + e] * rv;
+#pragma unroll
+            for (int cc = 0; cc < CDFT_MAX_M; ++cc) {
+                if (cc >= K) break;
+                acc[cc] += (cc == kq ? qn : Q[(size_t)cc * n + e]) * rv;
+            }
         }
         return K;
     }
@@ -306,8 +343,11 @@ __device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AASta
         const int mk = A.mk;
         for (int e = e0; e < e1; e += stride) {
             double v = S.gx[e];
-            for (int cc = 0; cc < mk; ++cc) {
-                const int slotc = (A.head + cc) % m;
+#pragma unroll
+            for (int cc = 0; cc < CDFT_MAX_M; ++cc) {
+                if (cc >= mk) break;
+                int slotc = A.head + cc;
+                slotc -= (slotc >= m) ? m : 0;
                 v += (-A.coef[cc]) * S.DG[(size_t)slotc * n + e];
             }
             S.sol[e] = v;
@@ -595,37 +635,48 @@ __device__ void ctl_apply(AAState& A, int op, int slot_done, const double* sums,
     }
 }
 
-__global__ void ctl_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, const double* __restrict__ partials,
-                           int nsys, int slot_done, int* done_counter)
+// One block of CTL_THREADS per system: threads stride over the system's chunk
+// partials in a fixed order, a fixed-shape tree reduces them (deterministic, and
+// independent of the other systems of the batch), thread 0 applies the step.
+#define CTL_THREADS 128
+__global__ void __launch_bounds__(CTL_THREADS)
+ctl_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, const double* __restrict__ partials,
+           int nsys, int slot_done, int* done_counter)
 {
-    const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp_global >= nsys) return;
-    const int s = warp_global;
+    const int s = blockIdx.x;
+    if (s >= nsys) return;
     AAState& A = st[s];
     const SysDev& S = sys[s];
     if (A.mode == MODE_DONE) {
-        if (slot_done == 0 && lane == 0)
+        if (slot_done == 0 && threadIdx.x == 0)
             for (int k = 1; k <= N_VEC_SLOTS; ++k) A.op[k] = OP_NONE;
         return;
     }
     const int op = (slot_done == 0) ? -1 : A.op[slot_done];
     if (op == OP_NONE || op == OP_SOL_AA || op == OP_SOL_COPY) return;
     const int K = ctl_nsums(A, op);
-    double sums[RED_SLOTS];
-    for (int k = 0; k < RED_SLOTS; ++k) sums[k] = 0.0;
-    for (int ch = lane; ch < S.chunk_count; ch += 32) {
-        const double* p = partials + (size_t)(S.chunk_begin + ch) * RED_SLOTS;
-        for (int k = 0; k < K; ++k) sums[k] += p[k];
-    }
-    for (int k = 0; k < K; ++k) {
-        double v = sums[k];
+    __shared__ double red[CTL_THREADS / 32][RED_SLOTS];
+    __shared__ double sums[RED_SLOTS];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < RED_SLOTS; ++k) {
+        if (k >= K) break;
+        double v = 0.0;
+        for (int ch = threadIdx.x; ch < S.chunk_count; ch += CTL_THREADS)
+            v += partials[(size_t)(S.chunk_begin + ch) * RED_SLOTS + k];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        sums[k] = v;
+        if (lane == 0) red[warp][k] = v;
     }
-    if (lane != 0) return;
-    ctl_apply(A, op, slot_done, sums, done_counter);
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double v = 0.0;
+#pragma unroll
+        for (int w = 0; w < CTL_THREADS / 32; ++w) v += red[w][threadIdx.x];
+        sums[threadIdx.x] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) ctl_apply(A, op, slot_done, sums, done_counter);
 }
 
 // initial iterate: sol = log(rho0); rho = exp(sol)   (converge.jl:244, GFix! :236)

@@ -46,7 +46,9 @@ __device__ __forceinline__ void block_reduce_to_smem(double* vals, int K, double
 {
     __shared__ double red[BLOCK / 32][RED_SLOTS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int c = 0; c < K; ++c) {
+#pragma unroll
+    for (int c = 0; c < RED_SLOTS; ++c) {
+        if (c >= K) break;
         double v = vals[c];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -132,10 +134,13 @@ __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, do
                  : "d"(a), "d"(b));
 }
 
-template <int NC>
+// PERIODIC = true: the inputs are read in place, input (i, f) = ext + i * in_comp_stride
+// + f * N, with the index taken mod N (no extended copy); false: the extended inputs.
+template <int NC, bool PERIODIC = false>
 __device__ __forceinline__ void pers_conv_dmma(const double* __restrict__ ext, bool shared_input,
                                                const double* __restrict__ taps, double* __restrict__ out,
-                                               int out_comp_stride, int N, int nconv, double scale)
+                                               int out_comp_stride, int N, int nconv, double scale,
+                                               int in_comp_stride = 0)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int EXTN = pers_extn(N), OFF = pers_off(N);
@@ -148,21 +153,41 @@ __device__ __forceinline__ void pers_conv_dmma(const double* __restrict__ ext, b
         const int ut = task % nut;
         const int f = (task / nut) % nconv;
         const int i = task / (nut * nconv);
-        const double* in = ext + (size_t)(shared_input ? i : i * nconv + f) * EXTN + OFF;
         const double* tp = taps + (size_t)(i * nconv + f) * N;
         const int u0 = ut * 8;
         double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
         // B: e[8 (u0 + r - d) + c], column n = r; A: t(8 d + r - c)
-        const double* bp = in + 8 * (u0 + r) + k;
-        for (int d = 0; d < D; ++d) {
-            const int q0 = 8 * d + r - k;        // c = k
-            const int q1 = q0 - 4;               // c = k + 4
-            const double a0 = (q0 >= 0 && q0 < N) ? tp[q0] : 0.0;
-            const double a1 = (q1 >= 0 && q1 < N) ? tp[q1] : 0.0;
-            const double b0 = bp[-8 * d];
-            const double b1 = bp[-8 * d + 4];
-            dmma_m8n8k4(c0, c1, a0, b0);
-            dmma_m8n8k4(e0, e1, a1, b1);
+        if constexpr (PERIODIC) {
+            const double* in = ext + (size_t)i * in_comp_stride + (size_t)f * N;
+            // N >= 8 (checked by the caller): one conditional add/subtract keeps the
+            // index in [0, N) and the loop free of branches
+            int i0 = (8 * (u0 + r) + k) % N;   // index of d = 0, c = k; c = k + 4 is 4 further
+            for (int d = 0; d < D; ++d) {
+                const int q0 = 8 * d + r - k;
+                const int q1 = q0 - 4;
+                const double a0 = (q0 >= 0 && q0 < N) ? tp[q0] : 0.0;
+                const double a1 = (q1 >= 0 && q1 < N) ? tp[q1] : 0.0;
+                const int i1 = i0 + 4 - ((i0 + 4 >= N) ? N : 0);
+                const double b0 = in[i0];
+                const double b1 = in[i1];
+                dmma_m8n8k4(c0, c1, a0, b0);
+                dmma_m8n8k4(e0, e1, a1, b1);
+                i0 -= 8;
+                i0 += (i0 < 0) ? N : 0;
+            }
+        } else {
+            const double* in = ext + (size_t)(shared_input ? i : i * nconv + f) * EXTN + OFF;
+            const double* bp = in + 8 * (u0 + r) + k;
+            for (int d = 0; d < D; ++d) {
+                const int q0 = 8 * d + r - k;        // c = k
+                const int q1 = q0 - 4;               // c = k + 4
+                const double a0 = (q0 >= 0 && q0 < N) ? tp[q0] : 0.0;
+                const double a1 = (q1 >= 0 && q1 < N) ? tp[q1] : 0.0;
+                const double b0 = bp[-8 * d];
+                const double b1 = bp[-8 * d + 4];
+                dmma_m8n8k4(c0, c1, a0, b0);
+                dmma_m8n8k4(e0, e1, a1, b1);
+            }
         }
         double* o = out + (size_t)i * out_comp_stride + (size_t)f * N;
         const int j0 = 8 * (u0 + 2 * k) + r, j1 = j0 + 8;
@@ -263,15 +288,22 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
         }
         __syncthreads();
         // ---- adjoint convolutions (integrate_field!) ----
-        for (int k = tid; k < NC * NCONV * EXTN; k += PERS_THREADS) {
-            const int slot = k / EXTN, u = k - slot * EXTN;
-            const int i = slot / NCONV, f = slot - i * NCONV;
-            int j = (u - OFF) % N;
-            j += (j < 0) ? N : 0;
-            ext[k] = nf[(i * NF + f + 1) * N + j];
+        if (sizeof(T) == 8 && N >= 8) {
+            // FP64: the tensor-core convolution reads dPhi/dn in place, periodically indexed
+            pers_conv_dmma<NC, true>(reinterpret_cast<const double*>(nf + N), false,
+                                     reinterpret_cast<const double*>(taps), reinterpret_cast<double*>(ip),
+                                     NCONV * N, N, NCONV, 1.0, NF * N);
+        } else {
+            for (int k = tid; k < NC * NCONV * EXTN; k += PERS_THREADS) {
+                const int slot = k / EXTN, u = k - slot * EXTN;
+                const int i = slot / NCONV, f = slot - i * NCONV;
+                int j = (u - OFF) % N;
+                j += (j < 0) ? N : 0;
+                ext[k] = nf[(i * NF + f + 1) * N + j];
+            }
+            __syncthreads();
+            pers_conv_any<T, NC>(ext, false, taps, ip, NCONV * N, N, NCONV, T(1));
         }
-        __syncthreads();
-        pers_conv_any<T, NC>(ext, false, taps, ip, NCONV * N, N, NCONV, T(1));
         __syncthreads();
         // ---- Euler-Lagrange step + aa_point! bookkeeping ----
         {
