@@ -24,7 +24,8 @@ from .thermo import PCSAFT, N_A, K_B, R
 _LIB = _lib.load()
 
 __all__ = [
-    "PCSAFT", "Steele", "HardSphereSolutes", "Uniform1DCart", "Uniform3DCart", "TwoPhase1DCart", "DFTOptions",
+    "PCSAFT", "Steele", "HardSphereSolutes", "HardCore", "Uniform1DCart", "Uniform3DCart", "Uniform1DSphr",
+    "Uniform1DCyl", "TwoPhase1DCart", "DFTOptions",
     "DFTSystem", "AASol",
     "initialize_profiles", "converge", "batch_converge", "dFdrho_res", "F_res", "F_ideal",
     "free_energy", "surface_tension", "interfacial_tension", "adsorption", "integrate",
@@ -118,6 +119,8 @@ class HardSphereSolutes:
 
 
 class Structure:
+    coord = "cart"
+
     def __init__(self, conditions, rho_bulk, bounds, ngrid, kind, rho_bulk2=None):
         self.conditions = (float(conditions[0]), float(conditions[1]))
         self.rho_bulk = np.asarray(rho_bulk, dtype=float)
@@ -158,6 +161,62 @@ def Uniform3DCart(conditions, rho_bulk, bounds, ngrid):
         b = np.tile(b.reshape(1, 2), (3, 1))
     ng = ngrid if isinstance(ngrid, (tuple, list)) else (ngrid,) * 3
     return Structure(conditions, rho_bulk, b, ng, "uniform")
+
+
+class RadialStructure(Structure):
+    """Uniform1DSphr / Uniform1DCyl (src/base/structure.jl:355-433): the grid is the
+    sampling grid of the quasi-discrete Hankel transform on [0, ub] (the reference's
+    Hankel.QDHT(0, n, ub, N), n = 2 sphere, 1 cylinder): r_m = j_m ub / j_{N+1} with j_m the
+    zeros of J_nu, nu = 1/2 (sphere) or 0 (cylinder).  lb is kept for external fields."""
+
+    def __init__(self, conditions, rho_bulk, bounds, ngrid, coord):
+        b = np.asarray(bounds, dtype=float).ravel()
+        if b.size == 1:
+            b = np.array([0.0, b[0]])
+        super().__init__(conditions, rho_bulk, b, ngrid, "uniform")
+        self.coord = coord
+        N = self.ngrid[0]
+        ub = self.bounds[0][1]
+        nu = 0.5 if coord == "sphr" else 0.0
+        from scipy import special
+        j = np.pi * np.arange(1, N + 2) if nu == 0.5 else special.jn_zeros(0, N + 1)
+        S = j[-1]
+        self._r = j[:-1] * ub / S
+        jn1 = np.abs(special.jv(nu + 1, j[:-1]))
+        ang = 4 * np.pi if coord == "sphr" else 2 * np.pi
+        # 4 pi / 2 pi integrateR: Fourier-Bessel quadrature of int f r^(2 nu + 1) dr
+        self.weights = ang * 2 * ub ** 2 / (S ** 2 * jn1 ** 2) * self._r ** (2 * nu)
+
+    def coords(self, d=0):
+        return self._r
+
+    def volume(self):
+        ub = self.bounds[0][1]
+        return 4 / 3 * np.pi * ub ** 3 if self.coord == "sphr" else np.pi * ub ** 2
+
+
+def Uniform1DSphr(conditions, rho_bulk, bounds, ngrid):
+    """src/base/structure.jl:383 (spherical symmetry, radial grid on [0, ub])."""
+    return RadialStructure(conditions, rho_bulk, bounds, ngrid, "sphr")
+
+
+def Uniform1DCyl(conditions, rho_bulk, bounds, ngrid):
+    """src/base/structure.jl:406 (cylindrical symmetry, radial grid on [0, ub])."""
+    return RadialStructure(conditions, rho_bulk, bounds, ngrid, "cyl")
+
+
+class HardCore:
+    """A hard core of radius `radius` at the origin of a spherical or cylindrical grid
+    (a solute or a rod): V_ext = `height` k_B T for r < radius.  An external field the
+    reference does not define; it gives the radial systems structure to converge."""
+
+    def __init__(self, radius, height=100.0):
+        self.radius = float(radius)
+        self.height = float(height)
+
+    def potential(self, model, r, T):
+        V = np.where(np.asarray(r) < self.radius, self.height, 0.0)
+        return np.repeat(V[None], len(model), axis=0)
 
 
 def TwoPhase1DCart(conditions, rho_bulk, rho_bulk2, bounds, ngrid):
@@ -212,7 +271,7 @@ class DFTSystem:
         for k in range(nd):
             d.ngrid[k] = structure.ngrid[k]
             d.bounds[k][0], d.bounds[k][1] = structure.bounds[k]
-        d.coord = _lib.COORD_CART
+        d.coord = {"cart": _lib.COORD_CART, "sphr": _lib.COORD_SPH, "cyl": _lib.COORD_CYL}[structure.coord]
         d.nc = nc
         for i in range(nc):
             d.m[i] = model.m[i]
@@ -429,6 +488,11 @@ def integrate(f, structure):
     """``∫(f, structure)`` (integrals.jl:17,28-41): Simpson weights 1,4,2,...,1 per
     dimension (outer product), dz = (ub-lb)/N, compensated FP64 summation."""
     f = np.asarray(f, dtype=float)
+    if getattr(structure, "coord", "cart") != "cart":   # 4 pi / 2 pi integrateR (integrals.jl:18-19)
+        acc = _KSum()
+        for v in (structure.weights * f).ravel():
+            acc.add(float(v))
+        return acc.value()
     w = np.ones(())
     for ax, n in enumerate(f.shape):
         k = np.arange(1, n + 1)
@@ -485,8 +549,9 @@ def interfacial_tension(system, rho):
 
 def adsorption(system, rho):
     """adsorption(system, ρ) (adsorption.jl:182-188), mol/m^3 of the domain."""
-    V = np.prod([ub - lb for (lb, ub) in system.structure.bounds])
-    return np.array([integrate(rho[i], system.structure) / V for i in range(system.nc)])
+    st = system.structure
+    V = st.volume() if hasattr(st, "volume") else np.prod([ub - lb for (lb, ub) in st.bounds])
+    return np.array([integrate(rho[i], st) / V for i in range(system.nc)])
 
 
 def F_res_grad(system, rho):

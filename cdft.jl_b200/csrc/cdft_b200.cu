@@ -87,6 +87,8 @@ struct cdft_plan {
     void* d_part = nullptr;
     void* d_dfield = nullptr;
     double* d_fval = nullptr;
+    double* d_mats = nullptr;     // radial: dense weighted-density operators (both stages)
+    std::vector<double> rw;       // radial: quadrature weights of the integral (angular factor included)
     void* d_spec = nullptr;       // 3D: convolved-field spectra [comp][field][z][y][kx]
     void* d_R = nullptr;          // 3D: spectrum of rho / accumulated adjoint spectrum
     void* d_adj = nullptr;        // 3D: adjoint sum in real space
@@ -98,7 +100,7 @@ struct cdft_plan {
 
 struct Batch {
     std::vector<cdft_plan*> plans;
-    int nsys = 0, nc = 0, nd = 0, mixed = 0;
+    int nsys = 0, nc = 0, nd = 0, mixed = 0, coord = 0;
     cudaStream_t stream = nullptr;
     SysDev* d_sys = nullptr;
     AAState* d_st = nullptr;
@@ -172,7 +174,10 @@ int validate_desc(const cdft_system_desc* d)
                 return set_error(CDFT_E_UNSUPPORTED, "3D boxes must be cubic (equal periods)");
         if (d->nc > 2) return set_error(CDFT_E_UNSUPPORTED, "3D systems support nc <= 2");
     }
-    if (d->coord != CDFT_COORD_CART) return set_error(CDFT_E_UNSUPPORTED, "only Cartesian coordinates are implemented");
+    if (d->coord != CDFT_COORD_CART && d->coord != CDFT_COORD_SPH && d->coord != CDFT_COORD_CYL)
+        return set_error(CDFT_E_INVALID, "coord=%d", d->coord);
+    if (d->coord != CDFT_COORD_CART && (d->nd != 1 || d->ngrid[0] < 4))
+        return set_error(CDFT_E_UNSUPPORTED, "spherical and cylindrical grids are 1D (radial) with at least 4 points");
     if (d->nc < 1 || d->nc > CDFT_MAX_NC) return set_error(CDFT_E_INVALID, "nc=%d out of [1,%d]", d->nc, CDFT_MAX_NC);
     if (d->ngrid[0] < 2) return set_error(CDFT_E_INVALID, "ngrid[0]=%d < 2", d->ngrid[0]);
     if (!(d->bounds[0][1] > d->bounds[0][0])) return set_error(CDFT_E_INVALID, "bounds must satisfy ub > lb");
@@ -210,6 +215,143 @@ int plan_alloc_m(cdft_plan* p, int m)
 
 int plan_build3d(cdft_plan* p);
 
+// ---------------------------------------------------------------------------
+// Radial grids (Uniform1DSphr / Uniform1DCyl, src/base/structure.jl:355-433).
+// The reference transforms with Hankel.jl's QDHT(0, n, ub, N) (n = 2 sphere, 1
+// cylinder).  Restated from the published quasi-discrete Hankel transform
+// (Guizar-Sicairos & Gutierrez-Vega, JOSA A 21 (2004) 53) for radially symmetric
+// functions in n + 1 dimensions: Bessel order nu = (n - 1) / 2, zeros j_1..j_{N+1},
+// S = j_{N+1}, r_m = j_m R / S, k_m = j_m / R, the symmetric matrix
+// T_mq = 2 J_nu(j_m j_q / S) / (|J_{nu+1}(j_m)| |J_{nu+1}(j_q)| S) for both directions,
+// and point weights a_m = r_m^nu / |J_{nu+1}(j_m)|.  A convolution with multiplier
+// w(k) is then the dense operator diag(1/a) T diag(w) T diag(a).
+// ---------------------------------------------------------------------------
+std::vector<double> bessel_zeros(double nu, int count)
+{
+    std::vector<double> z(count);
+    const double PI = 3.14159265358979323846;
+    for (int m = 1; m <= count; ++m) {
+        if (nu == 0.5) {   // J_{1/2}(x) = sqrt(2 / (pi x)) sin x
+            z[m - 1] = m * PI;
+            continue;
+        }
+        double x = (m - 0.25) * PI;   // McMahon's first term for J_0, then Newton (J_0' = -J_1)
+        x += 1.0 / (8.0 * x);
+        for (int it = 0; it < 60; ++it) {
+            const double dx = std::cyl_bessel_j(0.0, x) / std::cyl_bessel_j(1.0, x);
+            x += dx;
+            if (std::fabs(dx) < 1e-16 * x) break;
+        }
+        z[m - 1] = x;
+    }
+    return z;
+}
+
+int radial_build(cdft_plan* p)
+{
+    const cdft_system_desc& d = p->desc;
+    SysDev& S = p->sys;
+    const int N = d.ngrid[0], nc = d.nc, nconv = S.nconv;
+    const double PI = 3.14159265358979323846, TWO_PI = 2.0 * PI;
+    const double nu = (d.coord == CDFT_COORD_SPH) ? 0.5 : 0.0;
+    const double R = d.bounds[0][1], L = d.L;
+    const std::vector<double> j = bessel_zeros(nu, N + 1);
+    const double Sz = j[N];
+    std::vector<double> r(N), k(N), a(N), jn1(N), T((size_t)N * N);
+    p->rw.assign(N, 0.0);
+    const double ang = (d.coord == CDFT_COORD_SPH) ? 4.0 * PI : TWO_PI;   // integrals.jl:18-19
+    for (int m = 0; m < N; ++m) {
+        r[m] = j[m] * R / Sz;
+        k[m] = j[m] / R;
+        jn1[m] = std::fabs(std::cyl_bessel_j(nu + 1.0, j[m]));
+        a[m] = std::pow(r[m], nu) / jn1[m];
+        // int_0^R f r^(2 nu + 1) dr: Fourier-Bessel quadrature of the k -> 0 limit
+        p->rw[m] = ang * 2.0 * R * R / (Sz * Sz * jn1[m] * jn1[m]) * std::pow(r[m], 2.0 * nu);
+    }
+    for (int m = 0; m < N; ++m)
+        for (int q = 0; q < N; ++q)
+            T[(size_t)m * N + q] = 2.0 * std::cyl_bessel_j(nu, j[m] * j[q] / Sz) / (jn1[m] * jn1[q] * Sz);
+    // radial_derivative_matrix (src/structure/transforms.jl:43-64) on the physical grid
+    std::vector<double> D((size_t)N * N, 0.0);
+    for (int i = 1; i < N - 1; ++i) {
+        const double h1 = r[i] - r[i - 1], h2 = r[i + 1] - r[i];
+        D[(size_t)i * N + i - 1] = -h2 / (h1 * (h1 + h2));
+        D[(size_t)i * N + i] = (h2 - h1) / (h1 * h2);
+        D[(size_t)i * N + i + 1] = h1 / (h2 * (h1 + h2));
+    }
+    {
+        double h1 = r[1] - r[0], h2 = r[2] - r[1];
+        D[0] = -(2 * h1 + h2) / (h1 * (h1 + h2));
+        D[1] = (h1 + h2) / (h1 * h2);
+        D[2] = -h1 / (h2 * (h1 + h2));
+        h1 = r[N - 2] - r[N - 3];
+        h2 = r[N - 1] - r[N - 2];
+        D[(size_t)(N - 1) * N + N - 3] = h2 / (h1 * (h1 + h2));
+        D[(size_t)(N - 1) * N + N - 2] = -(h1 + h2) / (h1 * h2);
+        D[(size_t)(N - 1) * N + N - 1] = (2 * h2 + h1) / (h2 * (h1 + h2));
+    }
+    auto conv = [&](const std::vector<double>& w, std::vector<double>& M) {   // diag(1/a) T diag(w) T diag(a)
+        std::vector<double> TW((size_t)N * N);
+        for (int m = 0; m < N; ++m)
+            for (int q = 0; q < N; ++q) TW[(size_t)m * N + q] = T[(size_t)m * N + q] * w[q];
+        M.assign((size_t)N * N, 0.0);
+        for (int m = 0; m < N; ++m)
+            for (int t = 0; t < N; ++t) {
+                const double v = TW[(size_t)m * N + t];
+                for (int q = 0; q < N; ++q) M[(size_t)m * N + q] += v * T[(size_t)t * N + q];
+            }
+        for (int m = 0; m < N; ++m)
+            for (int q = 0; q < N; ++q) M[(size_t)m * N + q] *= a[q] / a[m];
+    };
+    // fields of get_fields(::PCSAFTModel) (PCSAFT.jl:55-61): types and widths as in 1D Cartesian
+    const int types[6] = {1, 2, 3, 2, 1, 2};
+    const double wf[6] = {0.5, 0.5, 0.5, 1.0, 1.0, PSI_DISP};
+    const size_t NN = (size_t)N * N;
+    std::vector<double> mats(2 * (size_t)nc * nconv * NN);
+    std::vector<double> w(N), M;
+    for (int i = 0; i < nc; ++i)
+        for (int f = 0; f < nconv; ++f) {
+            const double width = wf[f] * S.phi.d[i];
+            double* A0 = mats.data() + ((size_t)(0 * nc + i) * nconv + f) * NN;
+            double* A1 = mats.data() + ((size_t)(1 * nc + i) * nconv + f) * NN;
+            if (types[f] != 3) {   // SWeightedDensity(::RadialFrequency): omega_bar scaled by L, R = 2 pi width
+                const double Rr = TWO_PI * width;
+                for (int m = 0; m < N; ++m) {
+                    const double wb = k[m] / TWO_PI * L;
+                    w[m] = (types[f] == 1) ? 2.0 * std::sin(wb * Rr) / wb / TWO_PI
+                                           : 4.0 * PI / (wb * wb * wb) * (std::sin(wb * Rr) - Rr * wb * std::cos(wb * Rr))
+                                                 / (TWO_PI * TWO_PI * TWO_PI);
+                }
+                conv(w, M);
+                std::copy(M.begin(), M.end(), A0);
+                std::copy(M.begin(), M.end(), A1);   // integrate_field! applies the same convolution
+            } else {   // VWeightedDensity(::RadialFrequency): D QDHT^-1 diag(H) QDHT, raw omega, physical width
+                const double Rk = TWO_PI * width * L;
+                for (int m = 0; m < N; ++m) {
+                    const double wr = k[m] / TWO_PI;
+                    w[m] = 4.0 * PI / (wr * wr * wr) * (std::sin(wr * Rk) - Rk * wr * std::cos(wr * Rk))
+                           / (TWO_PI * TWO_PI * TWO_PI);
+                }
+                conv(w, M);
+                for (int m = 0; m < N; ++m)
+                    for (int q = 0; q < N; ++q) {
+                        double v = 0.0;
+                        for (int t = 0; t < N; ++t) v += D[(size_t)m * N + t] * M[(size_t)t * N + q];
+                        A0[(size_t)m * N + q] = v;
+                    }
+                // adjoint: the transpose, added (weighted_densities.jl:368-385); stored negated because
+                // the EL assembly subtracts the vector field's adjoint term (the Cartesian sign)
+                for (int m = 0; m < N; ++m)
+                    for (int q = 0; q < N; ++q) A1[(size_t)m * N + q] = -A0[(size_t)q * N + m];
+            }
+        }
+    CU(cudaMalloc(&p->d_mats, mats.size() * sizeof(double)));
+    CU(cudaMemcpyAsync(p->d_mats, mats.data(), mats.size() * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    CU(cudaStreamSynchronize(p->stream));
+    S.mats = p->d_mats;
+    return 0;
+}
+
 int plan_build(cdft_plan* p)
 {
     if (p->desc.nd == 3) return plan_build3d(p);
@@ -225,7 +367,7 @@ int plan_build(cdft_plan* p)
     S.NF = 6 + d.nd;
     S.nconv = S.NF - 1;
     S.ngrid[0] = N; S.ngrid[1] = 1; S.ngrid[2] = 1;
-    S.ksplit = (N + CONV_QC - 1) / CONV_QC;
+    S.ksplit = (d.coord == CDFT_COORD_CART) ? (N + CONV_QC - 1) / CONV_QC : 1;
     S.n_elem = N * nc;
     S.mixed = d.precision == CDFT_PREC_MIXED;
     const double L = d.L, T = d.T;
@@ -286,6 +428,11 @@ int plan_build(cdft_plan* p)
     S.vext = p->d_vext;
     S.taps = p->d_taps;
 
+    if (d.coord != CDFT_COORD_CART) {
+        const int rc = radial_build(p);
+        CU(cudaStreamSynchronize(p->stream));
+        return rc;
+    }
     // kernels of get_fields(::PCSAFTModel) (PCSAFT.jl:55-61), fields 2..7 in 1D
     const double psi = PSI_DISP;
     const int types[6] = {1, 2, 3, 2, 1, 2};
@@ -422,6 +569,7 @@ int plan_build3d(cdft_plan* p)
 
 void plan_free(cdft_plan* p)
 {
+    cudaFree(p->d_mats);
     cudaFree(p->d_taps);
     cudaFree(p->d_taps32);
     cudaFree(p->d_vext);
@@ -448,13 +596,14 @@ int batch_build(const std::vector<cdft_plan*>& plans, Batch** out)
     b->nsys = (int)plans.size();
     b->nc = plans[0]->desc.nc;
     b->nd = plans[0]->desc.nd;
+    b->coord = plans[0]->desc.coord;
     b->mixed = plans[0]->sys.mixed;
     b->cur32 = b->mixed;
     b->stream = plans[0]->stream;
     for (auto* p : plans) {
-        if (p->desc.nc != b->nc || p->desc.nd != b->nd || p->sys.mixed != b->mixed) {
+        if (p->desc.nc != b->nc || p->desc.nd != b->nd || p->sys.mixed != b->mixed || p->desc.coord != b->coord) {
             free_batch(b);
-            return set_error(CDFT_E_UNSUPPORTED, "systems of one batch must share nc, nd and precision");
+            return set_error(CDFT_E_UNSUPPORTED, "systems of one batch must share nc, nd, coordinates and precision");
         }
         if (p->device != plans[0]->device) {
             free_batch(b);
@@ -470,7 +619,7 @@ int batch_build(const std::vector<cdft_plan*>& plans, Batch** out)
     for (int s = 0; s < b->nsys; ++s) {
         SysDev& S = plans[s]->sys;
         const int tiles = (S.N + CONV_TILE - 1) / CONV_TILE;
-        if (b->nd == 1)
+        if (b->nd == 1 && b->coord == CDFT_COORD_CART)
             for (int i = 0; i < S.nc; ++i)
                 for (int f = 0; f < S.nconv; ++f)
                     for (int t = 0; t < tiles; ++t)
@@ -604,9 +753,36 @@ int launch_eval3d(Batch* b, const AAState* st, bool with_int)
 }
 
 template <typename T>
+int launch_dense_stage(Batch* b, const AAState* st, int stage)
+{
+    for (int s = 0; s < b->nsys; ++s) {
+        const SysDev& S = b->plans[s]->sys;
+        const long long rows = (long long)S.nc * S.nconv * S.N;
+        const int blocks = (int)((rows * 32 + DENSE_THREADS - 1) / DENSE_THREADS);
+        dense1d_kernel<T><<<blocks, DENSE_THREADS, 0, b->stream>>>(b->d_sys, s, stage, st);
+        g_launches += 1;
+    }
+    CHECK_LAUNCH();
+    return 0;
+}
+
+template <typename T>
+int launch_eval_radial(Batch* b, const AAState* st, bool with_int)
+{
+    int rc = launch_dense_stage<T>(b, st, 0);
+    if (rc) return rc;
+    rc = launch_phi<T>(b, st);
+    if (rc) return rc;
+    g_launches += 1;
+    if (with_int) rc = launch_dense_stage<T>(b, st, 1);
+    return rc;
+}
+
+template <typename T>
 int launch_eval_stages(Batch* b, const AAState* st, bool with_int)
 {
     if (b->nd == 3) return launch_eval3d<T>(b, st, with_int);
+    if (b->coord != CDFT_COORD_CART) return launch_eval_radial<T>(b, st, with_int);
     const size_t smem = (size_t)(CONV_QC + CONV_TILE + CONV_QC + 31) * sizeof(T);
     conv1d_kernel<T><<<b->ntasks, CONV_WARPS * 32, smem, b->stream>>>(b->d_tasks, b->d_sys, st, 0);
     int rc = launch_phi<T>(b, st);
@@ -796,7 +972,10 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
         return set_error(CDFT_E_UNSUPPORTED, "3D systems run on the grid engine");
     if (opts->engine != CDFT_ENGINE_AUTO && opts->engine != CDFT_ENGINE_GRID && opts->engine != CDFT_ENGINE_PERSISTENT)
         return set_error(CDFT_E_INVALID, "engine=%d", opts->engine);
-    if (b->nd == 1 && (opts->engine == CDFT_ENGINE_AUTO || opts->engine == CDFT_ENGINE_PERSISTENT)) {
+    if (b->coord != CDFT_COORD_CART && opts->engine == CDFT_ENGINE_PERSISTENT)
+        return set_error(CDFT_E_UNSUPPORTED, "spherical and cylindrical systems run on the grid engine");
+    if (b->nd == 1 && b->coord == CDFT_COORD_CART &&
+        (opts->engine == CDFT_ENGINE_AUTO || opts->engine == CDFT_ENGINE_PERSISTENT)) {
         const size_t need = persistent_smem_need(b), limit = persistent_smem_limit(b);
         use_persistent = need <= limit;
         if (!use_persistent && opts->engine == CDFT_ENGINE_PERSISTENT)
@@ -965,6 +1144,8 @@ int launch_stage(Batch* b, int stage)
     const bool mixed = b->cur32;
     if (b->nd == 3 && stage != 3) return set_error(CDFT_E_UNSUPPORTED, "3D systems time stage 3 only");
     const size_t smem = (size_t)(CONV_QC + CONV_TILE + CONV_QC + 31) * (mixed ? sizeof(float) : sizeof(double));
+    if (b->coord != CDFT_COORD_CART && (stage == 0 || stage == 2))
+        return mixed ? launch_dense_stage<float>(b, nullptr, stage / 2) : launch_dense_stage<double>(b, nullptr, stage / 2);
     switch (stage) {
     case 0:
     case 2:
@@ -1125,7 +1306,10 @@ int cdft_free_energy_res(cdft_plan* plan, const double* rho, double* F)
     auto coef = [](int k, int n) { return (k == 1 || k == n) ? 1.0 : ((k % 2 == 0) ? 4.0 : 2.0); };
     KSum acc;
     const double L = plan->desc.L;
-    if (plan->desc.nd == 1) {
+    if (plan->desc.coord != CDFT_COORD_CART) {   // 4 pi / 2 pi integrateR (integrals.jl:18-19)
+        for (int k = 0; k < plan->N; ++k) acc.add(plan->rw[k] * f[k]);
+        *F = acc.value() / (L * L * L);
+    } else if (plan->desc.nd == 1) {
         const int N = plan->N;
         for (int k = 1; k <= N; ++k) acc.add(coef(k, N) * f[k - 1]);
         *F = acc.value() * (plan->dz[0] / 3.0) / (L * L * L);
@@ -1286,7 +1470,8 @@ int cdft_free_energy_res_grad(cdft_plan* plan, const double* rho, double* dF)
     g_err_code = 0;
     if (!plan || !rho || !dF) return set_error(CDFT_E_INVALID, "NULL argument");
     const cdft_system_desc& d = plan->desc;
-    if (d.nd != 1) return set_error(CDFT_E_UNSUPPORTED, "the parameter gradient is implemented for 1D grids");
+    if (d.nd != 1 || d.coord != CDFT_COORD_CART)
+        return set_error(CDFT_E_UNSUPPORTED, "the parameter gradient is implemented for 1D Cartesian grids");
     const int nc = d.nc, N = plan->N;
     const double L = d.L, T = d.T;
     // the chain below assumes PC-SAFT's diameter d_i = sigma_i (1 - 0.12 exp(-3 eps_i / T)) and the
@@ -1501,6 +1686,8 @@ extern "C" int cdft_functional_derivative_noalloc(const cdft_system_desc* desc, 
     int rc = validate_desc(desc);
     if (rc) return rc;
     const cdft_system_desc& d = *desc;
+    if (d.nd != 1 || d.coord != CDFT_COORD_CART)
+        return set_error(CDFT_E_UNSUPPORTED, "the allocation-free entry point handles 1D Cartesian grids only");
     if (d.precision != CDFT_PREC_FP64)
         return set_error(CDFT_E_UNSUPPORTED, "the allocation-free entry point computes in FP64 only");
     const int N = d.ngrid[0], nc = d.nc;
@@ -1524,7 +1711,7 @@ extern "C" int cdft_functional_derivative_noalloc(const cdft_system_desc* desc, 
     S.NF = 7;
     S.nconv = 6;
     S.ngrid[0] = N; S.ngrid[1] = 1; S.ngrid[2] = 1;
-    S.ksplit = (N + CONV_QC - 1) / CONV_QC;
+    S.ksplit = (d.coord == CDFT_COORD_CART) ? (N + CONV_QC - 1) / CONV_QC : 1;
     S.n_elem = N * nc;
     const double L = d.L, T = d.T;
     S.NA = kNA * L * L * L;

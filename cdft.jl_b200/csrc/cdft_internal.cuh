@@ -78,6 +78,7 @@ struct SysDev {
     double* fval;                // Phi per point
     double* out;                 // scratch output (functional derivative)
     void* adj;                   // 3D: adjoint sum sum_f ±omega_f * dPhi/dn_f per element (T), else nullptr
+    const double* mats;          // radial grids: dense operators [(stage*nc + i)*nconv + f][j][q], else nullptr
 };
 
 struct AAState {

@@ -733,6 +733,39 @@ __global__ void taps1d_kernel(int N, double span, double L, int type, double wid
 }
 
 // ---------------------------------------------------------------------------
+// Radial (spherical / cylindrical) grids: the weighted densities and their adjoint
+// are dense operators (the reference's QDHT convolution and its materialised vector
+// operator, weighted_densities.jl:92-116,248-343).  One warp per output:
+// out[(i*nconv + f)*N + j] = scale * sum_q A[j][q] x[q], x = rho_i (stage 0, scale N_A L^3)
+// or dPhi/dn_{i,f} (stage 1); written where the Cartesian convolutions write.
+// ---------------------------------------------------------------------------
+#define DENSE_THREADS 256
+template <typename T>
+__global__ void __launch_bounds__(DENSE_THREADS)
+dense1d_kernel(const SysDev* __restrict__ sys, int s, int stage, const AAState* __restrict__ st)
+{
+    if (!sys_active(st, s)) return;
+    const SysDev& S = sys[s];
+    const int N = S.N, nconv = S.nconv;
+    const int row = (blockIdx.x * DENSE_THREADS + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= S.nc * nconv * N) return;
+    const int slot = row / N, j = row - slot * N;
+    const int i = slot / nconv, f = slot - i * nconv;
+    const double* A = S.mats + (((size_t)stage * S.nc * nconv + slot) * N + j) * N;
+    double acc = 0.0;
+    if (stage == 0) {
+        const double* x = S.rho + (size_t)i * N;
+        for (int q = lane; q < N; q += 32) acc = fma(A[q], x[q], acc);
+    } else {
+        const T* x = reinterpret_cast<const T*>(S.dfield) + (size_t)(i * S.NF + f + 1) * N;
+        for (int q = lane; q < N; q += 32) acc = fma(A[q], double(x[q]), acc);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) reinterpret_cast<T*>(S.part)[(size_t)slot * N + j] = T(stage == 0 ? acc * S.NA : acc);
+}
+
+// ---------------------------------------------------------------------------
 // Parameter gradient of F_res (1D): derivative taps, rho * dtaps, per-point terms.
 // ---------------------------------------------------------------------------
 // d omega_hat / dR of kernel_hat_1d (same type codes; type 3 returns the imaginary part)

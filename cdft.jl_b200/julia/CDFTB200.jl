@@ -116,7 +116,9 @@ function system_desc(system::DFTSystem{<:PCSAFTModel}, vext::Union{Nothing,Array
     else
         (CDFTAssocPair(0, 0, 0, 0, 0.0, 0.0),)
     end
-    coord = st isa cDFT.DFTStructByCoord{cDFT.Cartesian} ? 0 : error("Cartesian structures only")
+    coord = st isa cDFT.DFTStructByCoord{cDFT.Cartesian} ? 0 :
+            st isa cDFT.DFTStructByCoord{cDFT.Spherical} ? 1 :
+            st isa cDFT.DFTStructByCoord{cDFT.Cylindrical} ? 2 : error("unsupported coordinates")
     prec = cDFT.fptype(system.options) == Float64 ? Cint(0) : Cint(1)
     CDFTSystemDesc(nd, ng, Tuple(b), coord, nc, pad(model.params.segment.values, MAX_NC),
                    pad(sp.size, MAX_NC), sigma, epsv, cDFT.length_scale(model), T, nassoc, pairs,

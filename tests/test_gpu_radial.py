@@ -1,0 +1,86 @@
+"""Spherical and cylindrical (QDHT) grids through the C ABI against the oracle's
+restatement (oracle/radial.py).  The reference's radial path is CPU-only; its QDHT
+comes from Hankel.jl, which is not vendored, so the oracle restates the published
+transform and is pinned only by bulk consistency (test_oracle_radial.py)."""
+import numpy as np
+import pytest
+
+import _systems as S
+
+pytestmark = pytest.mark.gpu
+
+T_M, P_M = 150.0, 1e7
+
+
+def _pair(names, coord, ub_L, N, core=None, precision="fp64"):
+    import cdft_b200 as cd
+    from oracle import pcsaft_bulk as pb
+    from oracle import radial as rd
+    pm, om = S.models(names)
+    if names == ["methane"]:
+        rb = [pb.density(om, P_M, T_M, [1.0])]
+        cond = (P_M, T_M)
+    else:   # water-rich liquid of the water/octane LLE
+        r1, _ = S._lle(tuple(names), 1e5, 298.15)
+        rb = list(r1)
+        cond = (1e5, 298.15)
+    L = om.length_scale()
+    make = cd.Uniform1DSphr if coord == "sphr" else cd.Uniform1DCyl
+    st = make(cond, rb, [0.0, ub_L * L], N)
+    fields = None if core is None else [cd.HardCore(core * om.sigma[0])]
+    sp = cd.DFTSystem(pm, st, fields, cd.DFTOptions(precision))
+    ost = rd.RadialStructure(cond, rb, ub_L * L, N, coord)
+    so = rd.RadialDFTSystem(om, ost, vext=sp.vext)
+    return sp, so
+
+
+@pytest.mark.parametrize("coord,ub_L,N", [("sphr", 10.0, 151), ("cyl", 20.0, 101)])
+def test_bulk_consistency_radial_gpu(coord, ub_L, N):
+    import cdft_b200 as cd
+    from oracle import pcsaft_bulk as pb
+    sp, so = _pair(["methane"], coord, ub_L, N)
+    d = cd.dFdrho_res(sp, cd.initialize_profiles(sp))
+    mu = pb.mu_res(so.model, sp.structure.rho_bulk, T_M)[0]
+    assert abs(d[0, 0] - mu) < 1e-5          # the reference's tolerance
+    do = so.dFdrho(so.initialize_profiles())
+    assert float(np.max(np.abs(d - do)) / np.max(np.abs(do))) < 1e-10
+
+
+@pytest.mark.parametrize("names", [["methane"], ["water", "octane"]])
+@pytest.mark.parametrize("coord", ["sphr", "cyl"])
+def test_functional_derivative_radial(coord, names):
+    import cdft_b200 as cd
+    sp, so = _pair(names, coord, 10.0, 121)
+    rng = np.random.default_rng(3)
+    rho = S.random_smooth_profile(sp, rng, amp=0.2)
+    d = cd.dFdrho_res(sp, rho)
+    do = so.dFdrho(rho)
+    assert float(np.max(np.abs(d - do)) / np.max(np.abs(do))) < 1e-10
+    assert cd.F_res(sp, rho) == pytest.approx(so.F_res(rho), rel=1e-11)
+
+
+@pytest.mark.parametrize("coord,N", [("sphr", 151), ("cyl", 101)])
+def test_converge_radial_hard_core(coord, N):
+    """Methane around a hard core of radius 1.5 sigma at the origin, converged to 1e-11:
+    fluid profiles agree with the oracle's to 1e-9."""
+    import cdft_b200 as cd
+    sp, so = _pair(["methane"], coord, 10.0, N, core=1.5)
+    r0 = cd.initialize_profiles(sp)
+    rho = r0.copy()
+    kw = dict(beta=0.05, tol=1e-11, anderson_m=5, maxit=5000)
+    res = cd.converge(sp, rho, **kw)
+    ro, out = so.converge(r0.copy(), **kw)
+    assert res.errcode == 0 and out.errcode == 0
+    fluid = sp.vext[0] == 0
+    assert float(np.max(np.abs(rho[0, fluid] / ro[0, fluid] - 1))) < 1e-9
+    assert cd.free_energy(sp, rho) == pytest.approx(so.free_energy(ro), rel=1e-10)
+
+
+def test_radial_runs_on_the_grid_engine():
+    import cdft_b200 as cd
+    from cdft_b200._lib import CDFTError
+    sp, _ = _pair(["methane"], "sphr", 10.0, 101, core=1.5)
+    rho = cd.initialize_profiles(sp)
+    with pytest.raises(CDFTError):
+        cd.converge(sp, rho, beta=0.05, tol=1e-8, engine="persistent")
+    assert cd.converge(sp, rho, beta=0.05, tol=1e-8, engine="auto").errcode == 0

@@ -1,0 +1,53 @@
+"""The oracle's radial (QDHT) restatement: transform checks and the reference's own
+radial pin, bulk consistency (test/test_coordinate_systems.jl:60-81: at a uniform
+profile dF/drho at the first grid point equals mu_res to 1e-5)."""
+import numpy as np
+import pytest
+
+import _systems as S
+from oracle import pcsaft_bulk as pb
+from oracle import radial as rd
+
+
+@pytest.mark.parametrize("n", [1, 2])
+def test_qdht_convolution_of_gaussians_is_exact(n):
+    """A Gaussian convolved with a Gaussian kernel (multiplier exp(-k^2 s2^2 / 2)) in D = n + 1
+    dimensions is the Gaussian of variance s1^2 + s2^2 scaled by (s1^2/(s1^2+s2^2))^(D/2)."""
+    Q = rd.QDHT(n, 2.0, 151)
+    s1, s2 = 0.2, 0.15
+    f = np.exp(-Q.r ** 2 / (2 * s1 ** 2))
+    g = Q.conv_matrix(np.exp(-Q.k ** 2 * s2 ** 2 / 2)) @ f
+    D = n + 1
+    ref = (s1 ** 2 / (s1 ** 2 + s2 ** 2)) ** (D / 2) * np.exp(-Q.r ** 2 / (2 * (s1 ** 2 + s2 ** 2)))
+    assert np.max(np.abs(g - ref)) < 1e-13
+
+
+def test_qdht_spherical_grid_is_the_sine_grid():
+    """Order 1/2: zeros j_m = m pi, so r_m = m R / (N + 1) and T is the orthogonal DST-I."""
+    Q = rd.QDHT(2, 3.0, 50)
+    np.testing.assert_allclose(Q.r, 3.0 * np.arange(1, 51) / 51, rtol=1e-15)
+    np.testing.assert_allclose(Q.T @ Q.T, np.eye(50), atol=1e-13)
+
+
+@pytest.mark.parametrize("coord,ub_L,N", [("sphr", 10.0, 151), ("cyl", 20.0, 101)])
+def test_bulk_consistency_radial(coord, ub_L, N):
+    """The reference's configuration: PC-SAFT methane, 150 K, 10 MPa liquid."""
+    _, om = S.models(["methane"])
+    T, p = 150.0, 1e7
+    rb = pb.density(om, p, T, [1.0])
+    L = om.length_scale()
+    so = rd.RadialDFTSystem(om, rd.RadialStructure((p, T), [rb], ub_L * L, N, coord))
+    d = so.dFdrho(so.initialize_profiles())
+    mu = pb.mu_res(om, [rb], T)[0]
+    assert abs(d[0, 0] - mu) < 1e-5
+
+
+def test_product_radial_grid_matches_oracle():
+    import cdft_b200 as cd
+    L = 3.7039e-10
+    for coord, make in [("sphr", cd.Uniform1DSphr), ("cyl", cd.Uniform1DCyl)]:
+        st = make((1e7, 150.0), [3e4], [0.0, 10 * L], 101)
+        ost = rd.RadialStructure((1e7, 150.0), [3e4], 10 * L, 101, coord)
+        np.testing.assert_allclose(st.coords(0), ost.coords(0), rtol=1e-14)
+        ang = 4 * np.pi if coord == "sphr" else 2 * np.pi
+        np.testing.assert_allclose(st.weights, ang * ost.qdht.w, rtol=1e-13)
