@@ -15,8 +15,8 @@
 // their own axis and k = 0 set to zero: that is the Hermitian part of the
 // reference's kernel, i.e. exactly what real(ifft(...)) keeps.
 //
-// FFTs: radix-2 Stockham autosort in shared memory (Govindaraju et al., SC'08),
-// twiddles exp(-2 pi i q / N) from sincospi.
+// FFTs: two register passes per transform (L = R1 R2 Cooley-Tukey, radix-2 DFTs in
+// registers, one shared-memory exchange), twiddles exp(-2 pi i q / N) from sincospi.
 #pragma once
 #include "cdft_internal.cuh"
 
@@ -51,28 +51,91 @@ __device__ __forceinline__ void fft_twiddles(typename V2<T>::t* tw)
     }
 }
 
-// log2(L) radix-2 Stockham stages over LINES lines stored as buf[n * LS + line];
-// ping-pongs between x and y and returns the buffer that holds the result.
+// Split of an L-point transform into two register passes, L = R1 * R2.
+template <int L> struct FftSplit;
+template <> struct FftSplit<32> { static constexpr int R1 = 4, R2 = 8; };
+template <> struct FftSplit<64> { static constexpr int R1 = 8, R2 = 8; };
+template <> struct FftSplit<128> { static constexpr int R1 = 8, R2 = 16; };
+template <> struct FftSplit<256> { static constexpr int R1 = 16, R2 = 16; };
+
+__host__ __device__ constexpr int fft_bitrev(int i, int R)
+{
+    int r = 0;
+    for (int b = 1; b < R; b <<= 1) {
+        r = (r << 1) | (i & 1);
+        i >>= 1;
+    }
+    return r;
+}
+
+// w_L^m = exp(-+2 pi i m / L), m in [0, L), from the half table tw[q], q < L/2
+template <typename C, int L>
+__device__ __forceinline__ C fft_tw(const C* tw, int m, bool inverse)
+{
+    C w = tw[m & (L / 2 - 1)];
+    if (m >= L / 2) { w.x = -w.x; w.y = -w.y; }
+    if (inverse) w.y = -w.y;
+    return w;
+}
+
+// R-point DFT of v in registers (radix-2, decimation in time, all indices compile-time);
+// twiddles w_R^q = w_L^(q L / R) from the block's table
+template <typename C, int R, int L>
+__device__ __forceinline__ void fft_reg(C (&v)[R], const C* tw, bool inverse)
+{
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        const int jr = fft_bitrev(i, R);
+        if (jr > i) { const C t = v[i]; v[i] = v[jr]; v[jr] = t; }
+    }
+#pragma unroll
+    for (int half = 1; half < R; half <<= 1) {
+#pragma unroll
+        for (int q = 0; q < half; ++q) {
+            const C w = fft_tw<C, L>(tw, q * (L / (2 * half)), inverse);
+#pragma unroll
+            for (int b = 0; b < R; b += 2 * half) {
+                const C a = v[b + q], c = cmul(v[b + q + half], w);
+                v[b + q] = cadd(a, c);
+                v[b + q + half] = csub(a, c);
+            }
+        }
+    }
+}
+
+// L-point transforms of LINES lines stored as x[n * LS + line] (LS = LINES + 1 avoids bank
+// conflicts).  Two register passes, L = R1 R2 (decimation in time):
+//   pass 1, for each (t < R2, line): DFT over s of x[t + R2 s] -> u[k1], times w_L^(t k1),
+//           stored at y[k1 R2 + t]
+//   pass 2, for each (k1 < R1, line): DFT over t of y[k1 R2 + t] -> X[k1 + R1 k2] into x
+// since w_L^((t + R2 s)(k1 + R1 k2)) = w_L^(t k1) w_R2^(t k2) w_R1^(s k1).  The caller has
+// synchronised after filling x; the result is in x (returned) after a barrier.
 template <typename T, int L, int LINES, int LS>
 __device__ __forceinline__ typename V2<T>::t* fft_lines(typename V2<T>::t* x, typename V2<T>::t* y,
                                                         const typename V2<T>::t* tw, bool inverse)
 {
     typedef typename V2<T>::t C;
-    for (int Ns = 1; Ns < L; Ns <<= 1) {
-        for (int idx = threadIdx.x; idx < (L / 2) * LINES; idx += blockDim.x) {
-            const int line = idx % LINES, j = idx / LINES;
-            const int k = j & (Ns - 1);
-            C w = tw[k * (L / (2 * Ns))];
-            if (inverse) w.y = -w.y;
-            const C a = x[j * LS + line];
-            const C b = cmul(x[(j + L / 2) * LS + line], w);
-            const int out = (j / Ns) * 2 * Ns + k;
-            y[out * LS + line] = cadd(a, b);
-            y[(out + Ns) * LS + line] = csub(a, b);
-        }
-        __syncthreads();
-        C* t = x; x = y; y = t;
+    constexpr int R1 = FftSplit<L>::R1, R2 = FftSplit<L>::R2;
+    for (int it = threadIdx.x; it < R2 * LINES; it += blockDim.x) {
+        const int line = it % LINES, t = it / LINES;
+        C v[R1];
+#pragma unroll
+        for (int s = 0; s < R1; ++s) v[s] = x[(t + R2 * s) * LS + line];
+        fft_reg<C, R1, L>(v, tw, inverse);
+#pragma unroll
+        for (int k1 = 0; k1 < R1; ++k1) y[(k1 * R2 + t) * LS + line] = cmul(v[k1], fft_tw<C, L>(tw, t * k1, inverse));
     }
+    __syncthreads();
+    for (int it = threadIdx.x; it < R1 * LINES; it += blockDim.x) {
+        const int line = it % LINES, k1 = it / LINES;
+        C v[R2];
+#pragma unroll
+        for (int t = 0; t < R2; ++t) v[t] = y[(k1 * R2 + t) * LS + line];
+        fft_reg<C, R2, L>(v, tw, inverse);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) x[(k1 + R1 * k2) * LS + line] = v[k2];
+    }
+    __syncthreads();
     return x;
 }
 

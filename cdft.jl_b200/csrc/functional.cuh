@@ -65,7 +65,10 @@ template <int NC> struct PhiParamIdx {
 // dPhi/dP into gp[PhiParamIdx<NC>::NP] (same sweep, FP64): the explicit parameter
 // dependence used by the parameter gradient of F_res; PG = false compiles to the
 // plain evaluation.
-template <typename T, int NC, int ND, bool PG = false>
+// PART selects the terms: 0 all; 1 hard sphere + association (they read and write the
+// n2, n3 and vector fields only); 2 chain + dispersion (rho, chain, lambda, dispersion
+// fields only).  The two parts of one point can run on two threads, in place.
+template <typename T, int NC, int ND, bool PG = false, int PART = 0>
 __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + ND], T (&g)[NC][6 + ND],
                                       double* gp = nullptr)
 {
@@ -82,6 +85,8 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
 #pragma unroll
         for (int a = 0; a < NF; ++a) g[i][a] = T(0);
 
+    T phi = T(0);
+    if constexpr (PART != 2) {
     // ---------------- hard sphere (FMT.jl:17-46) ----------------
     T n0 = 0, n1 = 0, n2 = 0, n3 = 0;
     T nv1[ND], nv2[ND];
@@ -114,7 +119,7 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
     wb_bracket(n3d, Dd, Lg, invD, Bd, dBd);
     const T A3 = n2 * n2 * n2 / T(3) - n2 * nv2sq;
     const T A2 = n1 * n2 - nv1v2;
-    T phi = T(-double(n0) * Lg) + A2 * T(invD) + A3 * T(Bd);
+    phi = T(-double(n0) * Lg) + A2 * T(invD) + A3 * T(Bd);
     {
         const T g_n0 = T(-Lg);
         const T g_n1 = n2 * T(invD);
@@ -155,6 +160,9 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
         }
     }
 
+    }   // hard sphere
+
+    if constexpr (PART != 1) {
     // ---------------- hard chain (PCSAFT.jl:123-144) ----------------
     {
         T z3 = 0, z2 = 0;
@@ -306,8 +314,10 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
         }
     }
 
+    }   // chain and dispersion
+
     // ---------------- association, one pair (assoc.jl:702-769), FP64 ----------------
-    if (P.has_assoc) {
+    if (PART != 2 && P.has_assoc) {
         const double PI = 3.14159265358979323846, TWO_PI = 2.0 * PI;
         double n2m = 0, n3m = 0, nv2m[ND];
 #pragma unroll

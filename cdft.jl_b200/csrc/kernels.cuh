@@ -497,7 +497,73 @@ __device__ void aa_downdate(AAState& A)
     for (int r = 0; r < m; ++r) R[r + (m - 1) * m] = 0.0;
 }
 
-__device__ void aa_after_eval(AAState& A, double r, int* done_counter)
+// defer_downdate: leave the QR downdate to the caller (flagged in A.pad0), which runs it
+// warp-parallel (aa_downdate_warp)
+// aa_downdate by one warp: lane 0 forms each 2-row reflector, the lanes update the
+// trailing columns and build Qx column by column; per element the arithmetic of
+// aa_downdate (a reflector with tau = v1 = 0 leaves the columns unchanged).  A lives in
+// shared memory; the reflectors go to A.h1 / A.coef, which the next slots overwrite.
+__device__ void aa_downdate_warp(AAState& A, int lane)
+{
+    const int m = A.m, n = m - 1;
+    double* R = A.R;
+    double* tau = A.h1;
+    double* v1 = A.coef;
+    for (int j = 0; j < n; ++j) {
+        if (lane == 0) {
+            const double alpha = R[j + (j + 1) * m];
+            const double x = R[j + 1 + (j + 1) * m];
+            const double xnorm = sqrt(x * x);
+            if (xnorm == 0.0) {
+                tau[j] = 0.0;
+                v1[j] = 0.0;
+            } else {
+                const double beta = -copysign(hypot(alpha, xnorm), alpha);
+                tau[j] = (beta - alpha) / beta;
+                v1[j] = x * (1.0 / (alpha - beta));
+                R[j + (j + 1) * m] = beta;
+                R[j + 1 + (j + 1) * m] = 0.0;
+            }
+        }
+        __syncwarp();
+        const double tj = tau[j], vj = v1[j];
+        for (int c = j + 1 + lane; c < n; c += 32) {
+            const double w = fma(vj, R[j + 1 + (c + 1) * m], R[j + (c + 1) * m]);
+            R[j + (c + 1) * m] = fma(-tj, w, R[j + (c + 1) * m]);
+            R[j + 1 + (c + 1) * m] = fma(-(tj * vj), w, R[j + 1 + (c + 1) * m]);
+        }
+        __syncwarp();
+    }
+    double* Qx = A.Qx;
+    for (int c = lane; c < n; c += 32) {   // thin Q = H_0 ... H_{n-1} [I; 0], one column per lane
+        for (int r = 0; r < m; ++r) Qx[r + c * m] = (r == c) ? 1.0 : 0.0;
+        for (int j = n - 1; j >= 0; --j) {
+            const double w = fma(v1[j], Qx[j + 1 + c * m], Qx[j + c * m]);
+            Qx[j + c * m] = fma(-tau[j], w, Qx[j + c * m]);
+            Qx[j + 1 + c * m] = fma(-(tau[j] * v1[j]), w, Qx[j + 1 + c * m]);
+        }
+    }
+    // R[1:m-1, 1:m-1] = upper triangle of the slice; R[:, m] = 0 (read all, then write)
+    double v[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const int idx = lane + 32 * t;
+        if (idx < n * m) {
+            const int c = idx / m, r = idx - c * m;
+            v[t] = (r <= c) ? R[r + (c + 1) * m] : 0.0;
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const int idx = lane + 32 * t;
+        if (idx < n * m) R[idx] = v[t];
+    }
+    if (lane < m) R[lane + (m - 1) * m] = 0.0;
+    __syncwarp();
+}
+
+__device__ void aa_after_eval(AAState& A, double r, int* done_counter, bool defer_downdate = false)
 {
     A.resnorm = r;
     if (A.history && A.nevals < A.history_cap) A.history[A.nevals] = r;
@@ -558,7 +624,10 @@ __device__ void aa_after_eval(AAState& A, double r, int* done_counter)
             return;
         }
         A.downdate = (kqr > A.m - 1) ? 1 : 0;
-        if (A.downdate) aa_downdate(A);
+        if (A.downdate) {
+            if (defer_downdate) A.pad0 = 1;
+            else aa_downdate(A);
+        }
         A.kq = min(kqr, A.m - 1);
         A.op[1] = OP_DOT_H1;
         return;
@@ -581,12 +650,13 @@ __device__ __forceinline__ int ctl_nsums(const AAState& A, int op)
 
 // Finish slot `slot_done` (0 = EL) of a system given its reduced sums; sets the
 // operation of the next slot.  One thread.
-__device__ void ctl_apply(AAState& A, int op, int slot_done, const double* sums, int* done_counter)
+__device__ void ctl_apply(AAState& A, int op, int slot_done, const double* sums, int* done_counter,
+                          bool defer_downdate = false)
 {
     const int next = slot_done + 1;
     switch (op) {
     case -1:
-        aa_after_eval(A, sqrt(sums[0]), done_counter);
+        aa_after_eval(A, sqrt(sums[0]), done_counter, defer_downdate);
         break;
     case OP_NORM_DF: {   // k == 0 branch of aa_qr_update!: R[1,1] = norm(df)
         const double r = sqrt(sums[0]);

@@ -273,18 +273,28 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
         __syncthreads();
         pers_conv_any<T, NC>(ext, true, taps, nf + N, NF * N, N, NCONV, NA);
         __syncthreads();
-        // ---- fused Phi / dPhi/dn, in place ----
-        for (int j = tid; j < N; j += PERS_THREADS) {
+        // ---- fused Phi / dPhi/dn, in place: two threads per point ----
+        // items j < N: hard sphere + association (fields 1 .. 2 + ND); items N + j: chain +
+        // dispersion (fields 0, 3 + ND .. 5 + ND).  The two halves read and write disjoint
+        // fields, and they fall in different warps except around item N.
+        for (int w = tid; w < 2 * N; w += PERS_THREADS) {
+            const bool first = w < N;
+            const int j = first ? w : w - N;
             T n[NC][NF], g[NC][NF];
 #pragma unroll
             for (int i = 0; i < NC; ++i)
 #pragma unroll
-                for (int a = 0; a < NF; ++a) n[i][a] = nf[(i * NF + a) * N + j];
-            phi_grad<T, NC, ND>(S.phi, n, g);
+                for (int a = 0; a < NF; ++a) {
+                    const bool mine = (a >= 1 && a <= 2 + ND) == first;
+                    n[i][a] = mine ? nf[(i * NF + a) * N + j] : T(1);
+                }
+            if (first) phi_grad<T, NC, ND, false, 1>(S.phi, n, g);
+            else phi_grad<T, NC, ND, false, 2>(S.phi, n, g);
 #pragma unroll
             for (int i = 0; i < NC; ++i)
 #pragma unroll
-                for (int a = 0; a < NF; ++a) nf[(i * NF + a) * N + j] = g[i][a];
+                for (int a = 0; a < NF; ++a)
+                    if ((a >= 1 && a <= 2 + ND) == first) nf[(i * NF + a) * N + j] = g[i][a];
         }
         __syncthreads();
         // ---- adjoint convolutions (integrate_field!) ----
@@ -325,8 +335,13 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
                 ss[0] += el_elem(S, e, i, dF, beta, aa, DGs);
             }
             block_reduce_to_smem<PERS_THREADS>(ss, 1, sums);
-            if (tid == 0) ctl_apply(sA, -1, 0, sums, done_counter);
+            if (tid == 0) ctl_apply(sA, -1, 0, sums, done_counter, true);
             __syncthreads();
+            if (sA.pad0) {   // the QR downdate of this Anderson step, on warp 0
+                if (tid < 32) aa_downdate_warp(sA, tid);
+                __syncthreads();
+                if (tid == 0) sA.pad0 = 0;
+            }
         }
         // ---- Anderson vector slots ----
         for (int slot = 1; slot <= N_VEC_SLOTS; ++slot) {
