@@ -118,6 +118,7 @@ struct Batch {
     int cur32 = 0;                          // arithmetic of the running phase: 1 FP32, 0 FP64
     cudaGraphExec_t graph[2] = {nullptr, nullptr};   // indexed by cur32
     int graph_iters[2] = {0, 0};
+    long long graph_launches[2] = {0, 0};             // kernel launches captured in each graph
 };
 
 namespace {
@@ -808,7 +809,7 @@ int launch_iteration(Batch* b)
         if (slot < N_VEC_SLOTS)
             ctl_kernel<<<ctl_blocks, CTL_THREADS, 0, b->stream>>>(b->d_sys, b->d_st, b->d_partials, b->nsys, slot, b->d_done);
     }
-    g_launches += 2 * N_VEC_SLOTS;   // el, ctl0, 5 vec, 4 ctl (eval stages counted above)
+    g_launches += 2 * N_VEC_SLOTS + 1;   // el, ctl0, N_VEC_SLOTS vec, N_VEC_SLOTS - 1 ctl (eval stages counted above)
     CHECK_LAUNCH();
     return 0;
 }
@@ -885,6 +886,7 @@ int batch_capture(Batch* b, int iters)
     const long long before = g_launches;
     int rc = 0;
     for (int it = 0; it < iters && !rc; ++it) rc = g32 ? launch_iteration<float>(b) : launch_iteration<double>(b);
+    b->graph_launches[g32] = g_launches - before;   // kernel nodes of the graph, counted when it runs
     g_launches = before;
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (rc) return rc;
@@ -1006,11 +1008,10 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
         const int K = opts->iters_per_launch > 0 ? opts->iters_per_launch : 16;
         rc = batch_capture(b, K);
         if (rc) return rc;
-        const int per_iter = 3 + 2 * N_VEC_SLOTS;   // conv, phi, conv, el, ctl0, 5 vec, 4 ctl
         long long launched_evals = 0;
         while (true) {
             CU(cudaGraphLaunch(b->graph[b->cur32], b->stream));
-            g_launches += (long long)K * per_iter;
+            g_launches += b->graph_launches[b->cur32];
             launched_evals += K;
             CU(cudaMemcpyAsync(b->h_done, b->d_done, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
             CU(cudaStreamSynchronize(b->stream));
