@@ -941,7 +941,8 @@ int validate_opts(const cdft_solver_opts* o)
 // One aasol run over the batch from the profiles currently in the plans' rho
 // buffers, with the arithmetic of b->cur32.  hist_off[s]: history entries already
 // written for system s by an earlier phase.
-// atol_sys (optional): one absolute tolerance per system, replacing rtol/atol.
+// atol_sys (optional): one absolute tolerance per system, replacing rtol/atol
+// (a negative entry keeps rtol/atol for that system).
 int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, const std::vector<int>& hist_off,
               std::vector<AAState>& st, std::chrono::steady_clock::time_point t0, bool* budget_hit,
               const std::vector<double>* atol_sys = nullptr)
@@ -956,8 +957,9 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
         A.picard_maxit = opts->picard_maxit;
         A.beta = opts->beta;
         A.picard_beta = opts->picard_beta;
-        A.rtol = atol_sys ? 0.0 : rtol;
-        A.atol = atol_sys ? (*atol_sys)[s] : atol;
+        const bool abs_tol = atol_sys && (*atol_sys)[s] >= 0.0;
+        A.rtol = abs_tol ? 0.0 : rtol;
+        A.atol = abs_tol ? (*atol_sys)[s] : atol;
         A.picard_rtol = opts->picard_rtol;
         A.picard_atol = opts->picard_atol;
         const int off = std::min(hist_off[s], b->hist_cap);
@@ -1036,7 +1038,9 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
 // until ||r|| <= max(rtol, s) ||r0|| + atol (s = mixed_switch_rtol), then a
 // second aasol in FP64 from that profile until the FP64 residual meets the
 // stopping test of a plain FP64 run, rtol ||r0|| + atol with r0 the residual
-// of the initial profile (taken from the first phase).
+// of the initial profile (taken from the first phase).  A system whose FP32 phase
+// diverges (errcode -2, which includes a non-finite evaluation) is converged again
+// in FP64 from its initial profile; its evaluation count includes both phases.
 int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, bool is_dev,
                    const cdft_solver_opts* opts, cdft_result* results)
 {
@@ -1074,7 +1078,7 @@ int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, boo
     }
     std::vector<AAState> st(b->nsys), st1;
     std::vector<int> hist_off(b->nsys, 0);
-    bool budget_hit = false;
+    bool budget_hit = false, phase2 = false;
     if (b->mixed) {
         const double sw = opts->mixed_switch_rtol > 0 ? opts->mixed_switch_rtol : 1e-5;
         b->cur32 = 1;
@@ -1082,15 +1086,26 @@ int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, boo
         if (rc) return rc;
         st1 = st;
         for (int s = 0; s < b->nsys; ++s) hist_off[s] = st1[s].nevals;
-        bool diverged = false;
-        for (int s = 0; s < b->nsys; ++s) diverged |= (st1[s].errcode == -2);
-        if (!budget_hit && !diverged) {
+        if (!budget_hit) {
             // phase-1 tol = max(rtol, sw) ||r0|| + atol gives back ||r0||
             const double r1 = std::max(opts->rtol, sw);
             std::vector<double> target(b->nsys);
-            for (int s = 0; s < b->nsys; ++s)
+            for (int s = 0; s < b->nsys; ++s) {
                 target[s] = opts->rtol * ((st1[s].tol - opts->atol) / r1) + opts->atol;
+                if (st1[s].errcode == -2) {
+                    // the FP32 phase diverged (residual blow-up or a non-finite evaluation):
+                    // this system restarts in FP64 from its initial profile, which the
+                    // caller's buffer still holds, under the stopping test of a plain FP64
+                    // run (target < 0: rtol ||r0|| + atol with its own r0)
+                    target[s] = -1.0;
+                    cdft_plan* p = plans[s];
+                    const size_t bytes = (size_t)p->sys.n_elem * sizeof(double);
+                    CU(cudaMemcpyAsync(p->sys.rho, rho[s], bytes,
+                                       is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->stream));
+                }
+            }
             b->cur32 = 0;
+            phase2 = true;
             rc = run_phase(b, opts, opts->rtol, opts->atol, hist_off, st, t0, &budget_hit, &target);
             b->cur32 = 1;
             if (rc) return rc;
@@ -1109,10 +1124,11 @@ int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, boo
     if (results) {
         for (int s = 0; s < b->nsys; ++s) {
             cdft_result& r = results[s];
-            const AAState& A = (st1.empty() || st1[s].errcode != -2) ? st[s] : st1[s];
-            const int prev_evals = st1.empty() ? 0 : st1[s].nevals;
-            const int prev_k = st1.empty() ? 0 : st1[s].k;
-            const bool two = !st1.empty() && st1[s].errcode != -2;
+            // st holds the last phase that ran; a mixed run counts the evaluations of both
+            const AAState& A = st[s];
+            const int prev_evals = phase2 ? st1[s].nevals : 0;
+            const int prev_k = phase2 ? st1[s].k : 0;
+            const bool two = phase2;
             r.idid = A.idid;
             r.errcode = A.errcode;
             r.iterations = two ? prev_k + A.k : A.k;

@@ -189,8 +189,11 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
                 }
                 continue;
             }
-            const T di = T(P.d[i]);
             const T rho = n[i][0];
+            // exact zeros (rho inside a hard wall, lambda as rounded FP32 FFT noise) make
+            // rho ln(y lambda / rho) 0/0 or 0 * inf: the point contributes nothing
+            if (rho == T(0) || n[i][ILAM] == T(0)) continue;
+            const T di = T(P.d[i]);
             const T lam = n[i][ILAM] / (T(2) * di);
             const T y = I + T(1.5) * di * z2 * I2 + T(0.5) * di * di * z2 * z2 * I3;
             const T lg = T(log(fabs(double(y * lam / rho))));
@@ -235,7 +238,15 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
             M += r[i] * T(P.m[i]);
             eta += T(P.m[i]) * r[i] * d3;
         }
-        const T mbar = M / S;
+        // mbar = sum r_i m_i / sum r_i (PCSAFT.jl:165-170).  One component: mbar = m
+        // exactly, with no division.  Where a mixture's dispersion density is exactly zero
+        // (FP32 FFT noise inside a hard solute rounds to 0.0 at some points) the ratio is
+        // 0/0 while the term and its gradient vanish with r: any finite mbar serves there
+        // and the composition derivatives are dropped.
+        const bool S0 = (NC > 1) && (S == T(0));
+        T mbar;
+        if constexpr (NC == 1) mbar = T(P.m[0]);
+        else mbar = S0 ? T(P.m[0]) : M / S;
         eta = eta * pi / T(6);
         T s1 = 0, s2 = 0;
         T rc1[NC], rc2[NC];
@@ -296,13 +307,15 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
         for (int i = 0; i < NC; ++i) {
             const T di = T(P.d[i]);
             const T d3 = di * di * di;
-            const T gr = g_m * (T(P.m[i]) - mbar) / S + g_e * pi / T(6) * T(P.m[i]) * d3
+            const T gm_i = (NC == 1 || S0) ? T(0) : g_m * (T(P.m[i]) - mbar) / S;
+            const T gr = gm_i + g_e * pi / T(6) * T(P.m[i]) * d3
                          + g_s1 * T(2) * rc1[i] + g_s2 * T(2) * rc2[i];
             g[i][IDISP] += gr * factor / d3;
             if constexpr (PG) {
                 // r_i = n_i factor / d_i^3; mbar = M / S; eta = pi/6 sum m_i r_i d_i^3 (explicit d_i^3)
                 const double ri = double(r[i]);
-                gp[PI_::M + i] += double(g_m) * ri / double(S) + double(g_e) * 3.14159265358979323846 / 6.0 * ri * double(d3);
+                const double dmbar = (NC == 1) ? 1.0 : (S0 ? 0.0 : ri / double(S));   // d mbar / d m_i
+                gp[PI_::M + i] += double(g_m) * dmbar + double(g_e) * 3.14159265358979323846 / 6.0 * ri * double(d3);
                 gp[PI_::D + i] += double(gr) * (-3.0 * ri / double(di))
                                   + double(g_e) * 3.14159265358979323846 / 2.0 * P.m[i] * ri * double(di) * double(di);
 #pragma unroll
@@ -329,16 +342,26 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
 #pragma unroll
             for (int k = 0; k < ND; ++k) nv2m[k] -= TWO_PI * double(n[i][FV + k]) * P.m[i];
         }
+        // xi = 1 - |nv2|^2 / n2^2 (assoc.jl:734) is 0/0 where n2 is exactly zero (in the
+        // mixed mode the weighted densities are FP32 FFT output, which rounds to 0.0 inside
+        // hard walls at some points); there u = n0 xi and every xi term vanish with n2, so
+        // xi = 1 and the vector fields drop out.
+        if (n2m == 0.0) {
+#pragma unroll
+            for (int k = 0; k < ND; ++k) nv2m[k] = 0.0;
+        }
+        const double d2m = (n2m == 0.0) ? 1.0 : n2m;
         double nv2sqm = 0;
 #pragma unroll
         for (int k = 0; k < ND; ++k) nv2sqm += nv2m[k] * nv2m[k];
-        const double xim = 1.0 - nv2sqm / (n2m * n2m);
+        const double xim = 1.0 - nv2sqm / (d2m * d2m);
         const double dij = P.a_dij;
         const double I = 1.0 / (1.0 - n3m);
         const double ghs = I + 0.5 * dij * xim * n2m * I * I + dij * dij * n2m * n2m * xim * (I * I * I) / 18.0;
         const double Delta = ghs * P.a_K;
         const int ic = P.a_ic, jc = P.a_jc;
         double n0c[2], n2c[2], sqc[2], xic[2], uc[2];
+        bool zc[2];
 #pragma unroll
         for (int s = 0; s < 2; ++s) {
             const int c = s == 0 ? ic : jc;
@@ -352,11 +375,13 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
                 }
             n0c[s] = nc_f2 / P.d[c];
             n2c[s] = PI * nc_f2 * P.d[c];
+            zc[s] = (n2c[s] == 0.0);   // as above: xi_c = 1 where n2_c is exactly zero
             double sq = 0;
 #pragma unroll
             for (int k = 0; k < ND; ++k) { const double t = -TWO_PI * vv[k]; sq += t * t; }
-            sqc[s] = sq;
-            xic[s] = 1.0 - sq / (n2c[s] * n2c[s]);
+            sqc[s] = zc[s] ? 0.0 : sq;
+            if (zc[s]) n2c[s] = 1.0;   // denominator only: n0_c = 0 carries the zero
+            xic[s] = 1.0 - sqc[s] / (n2c[s] * n2c[s]);
             uc[s] = n0c[s] * xic[s];
         }
         const double nia = P.a_nia, njb = P.a_njb;
@@ -395,14 +420,14 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
                     g[i][F2] += T(g_n0 / P.d[c] + g_n2 * PI * P.d[c]);
 #pragma unroll
                     for (int k = 0; k < ND; ++k)
-                        g[i][FV + k] += T(g_xi * (-2.0 * TWO_PI * TWO_PI * double(n[i][FV + k]) / (n2c[s] * n2c[s])));
+                        if (!zc[s]) g[i][FV + k] += T(g_xi * (-2.0 * TWO_PI * TWO_PI * double(n[i][FV + k]) / (n2c[s] * n2c[s])));
                 }
         }
         const double gg = gDelta * P.a_K;
         const double dg_dI = 1.0 + dij * xim * n2m * I + dij * dij * n2m * n2m * xim * I * I / 6.0;
         const double dg_dn2 = 0.5 * dij * xim * I * I + dij * dij * n2m * xim * I * I * I / 9.0;
         const double dg_dxi = 0.5 * dij * n2m * I * I + dij * dij * n2m * n2m * I * I * I / 18.0;
-        const double g_n2m = gg * (dg_dn2 + dg_dxi * 2.0 * nv2sqm / (n2m * n2m * n2m));
+        const double g_n2m = gg * (dg_dn2 + dg_dxi * 2.0 * nv2sqm / (d2m * d2m * d2m));
         const double g_n3m = gg * dg_dI * I * I;
 #pragma unroll
         for (int i = 0; i < NC; ++i) {
@@ -410,7 +435,7 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
             g[i][F3] += T(g_n3m * P.m[i]);
 #pragma unroll
             for (int k = 0; k < ND; ++k)
-                g[i][FV + k] += T(gg * dg_dxi * (-2.0 * nv2m[k] / (n2m * n2m)) * (-TWO_PI * P.m[i]));
+                g[i][FV + k] += T(gg * dg_dxi * (-2.0 * nv2m[k] / (d2m * d2m)) * (-TWO_PI * P.m[i]));
         }
         if constexpr (PG) {
             gp[PI_::AK] += gDelta * ghs;
@@ -421,7 +446,7 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
                 double gm = g_n2m * PI * f2 * P.d[i] + g_n3m * double(n[i][F3]);
 #pragma unroll
                 for (int k = 0; k < ND; ++k)
-                    gm += gg * dg_dxi * (-2.0 * nv2m[k] / (n2m * n2m)) * (-TWO_PI * double(n[i][FV + k]));
+                    gm += gg * dg_dxi * (-2.0 * nv2m[k] / (d2m * d2m)) * (-TWO_PI * double(n[i][FV + k]));
                 gp[PI_::M + i] += gm;
                 gp[PI_::D + i] += g_n2m * PI * f2 * P.m[i];
             }

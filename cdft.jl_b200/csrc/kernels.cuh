@@ -391,7 +391,9 @@ vec_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
 __device__ __forceinline__ double el_elem(const SysDev& S, int e, int i, double dF, double beta, bool aa, double* DGs)
 {
     double lnG = S.cprd[i] - dF;
-    lnG = fmin(fmax(lnG, -100.0), 100.0);             // clamp!(ln_Gx, -100, 100)
+    // clamp!(ln_Gx, -100, 100) with Julia's clamp semantics: a NaN stays NaN (fmin/fmax
+    // would turn it into a bound and hide a failed evaluation inside a finite residual)
+    lnG = (lnG > 100.0) ? 100.0 : ((lnG < -100.0) ? -100.0 : lnG);
     const double s = S.sol[e];
     const double gxn = (beta == 1.0) ? lnG : (1.0 - beta) * s + beta * lnG;  // betafix!
     const double rn = gxn - s;
@@ -569,6 +571,13 @@ __device__ void aa_after_eval(AAState& A, double r, int* done_counter, bool defe
     if (A.history && A.nevals < A.history_cap) A.history[A.nevals] = r;
     A.nevals++;
     for (int s = 1; s <= N_VEC_SLOTS; ++s) A.op[s] = OP_NONE;
+    if (!isfinite(r)) {   // a non-finite evaluation ends the run as a divergence
+        A.idid = 0;
+        A.errcode = -2;
+        A.mode = MODE_DONE;
+        atomicAdd(done_counter, 1);
+        return;
+    }
     switch (A.mode) {
     case MODE_EVAL_INIT: {
         A.up_bd = 1.0e4 * r;

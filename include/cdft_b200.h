@@ -96,8 +96,9 @@ typedef struct {
     int iters_per_launch;  /* fixed-point evaluations per CUDA-graph launch (grid engine), <= 0: default */
     int engine;            /* CDFT_ENGINE_* */
     double mixed_switch_rtol; /* mixed plans: FP32 phase until ||r|| <= max(rtol, this) ||r0|| + atol,
-                                 then FP64 until ||r|| <= rtol ||r0|| + atol, the stopping test of an
-                                 FP64 run (r0 of the initial profile); <= 0: 1e-5 */
+                                 then FP64 until ||r|| <= rtol ||r0|| + atol, the stopping test of an FP64 run (r0 of
+                                 the initial profile); a system whose FP32 phase diverges is converged
+                                 again in FP64 from its initial profile; <= 0: 1e-5 */
 } cdft_solver_opts;
 
 /* execution engines of cdft_converge / cdft_batch_converge */
@@ -108,7 +109,8 @@ typedef struct {
 /* The (idid, errcode, history) part of aasol's output (anderson.jl:81-103,727-757). */
 typedef struct {
     int idid;              /* 1 converged, 0 not */
-    int errcode;           /* -1 initial iterate within tol, -2 divergence, 0 converged, 10 maxit */
+    int errcode;           /* -1 initial iterate within tol, -2 divergence (residual above 1e4 ||r0||
+                              or not finite), 0 converged, 10 maxit */
     int iterations;        /* Anderson counter k of aasol */
     int evaluations;       /* fixed-point map evaluations */
     double resnorm;        /* final ||beta (G(x) - x)||_2 */

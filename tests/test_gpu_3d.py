@@ -176,3 +176,31 @@ def test_functional_derivative_256_planar_matches_1d(axis):
     d1 = cd.dFdrho_res(s1, (rb * p1)[None].copy())
     ref = np.broadcast_to(d1[0].reshape(shape), (N, N, N))
     assert float(np.max(np.abs(d3[0] - ref)) / np.max(np.abs(d1))) < 1e-11
+
+
+def test_converge_256_mixed_matches_fp64():
+    """The 3D benchmark box at 256^3 (27 solutes, m = 10, tol 1e-10): the mixed run
+    reaches the FP64 fixed point.  At this size FP32 FFT noise inside the solutes rounds
+    to exactly 0.0 at some points in some evaluations; the functional has to stay finite
+    there, or one evaluation's NaN sends the liquid to another fixed point."""
+    import cdft_b200 as cd
+    from oracle import pcsaft_bulk as pb
+    N = 256
+    pm, om = S.models(["argon"])
+    s = om.sigma[0]
+    box = 16.0 * s
+    rb = 0.021e30 / pb.N_A
+    hs = cd.HardSphereSolutes(cd.HardSphereSolutes.seeded(27, 1.5 * s, box, 2 * box / N, seed=0), 1.5 * s)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        sp = cd.DFTSystem(pm, cd.Uniform3DCart((1e5, T_AR), [rb], [0.0, box], N), [hs], cd.DFTOptions(prec))
+        rho = cd.initialize_profiles(sp)
+        res = cd.converge(sp, rho, beta=0.1, tol=1e-10, anderson_m=10, maxit=2000, engine="grid")
+        assert res.errcode == 0, (prec, res)
+        out[prec] = (sp, rho, cd.free_energy(sp, rho))
+    (s64, a, fa), (s32, b, fb) = out["fp64"], out["mixed"]
+    rel, ab = _fluid_solute_diff(s64, a, b)
+    assert rel < 1e-6 and ab < 1e-10, (rel, ab)
+    assert fb == pytest.approx(fa, rel=1e-9)
+    s64.close()
+    s32.close()
