@@ -960,6 +960,10 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
         const bool abs_tol = atol_sys && (*atol_sys)[s] >= 0.0;
         A.rtol = abs_tol ? 0.0 : rtol;
         A.atol = abs_tol ? (*atol_sys)[s] : atol;
+        // an FP64 polish of an FP32 result starts with Anderson: the Picard warm-up of
+        // aasol targets picard_rtol times the residual of its first iterate, which is
+        // already small here, and damped Picard does not reach it
+        if (abs_tol) A.picard_maxit = 0;
         A.picard_rtol = opts->picard_rtol;
         A.picard_atol = opts->picard_atol;
         const int off = std::min(hist_off[s], b->hist_cap);

@@ -96,7 +96,8 @@ typedef struct {
     int iters_per_launch;  /* fixed-point evaluations per CUDA-graph launch (grid engine), <= 0: default */
     int engine;            /* CDFT_ENGINE_* */
     double mixed_switch_rtol; /* mixed plans: FP32 phase until ||r|| <= max(rtol, this) ||r0|| + atol,
-                                 then FP64 until ||r|| <= rtol ||r0|| + atol, the stopping test of an FP64 run (r0 of
+                                 then FP64 (Anderson from the first step, no Picard warm-up) until
+                                 ||r|| <= rtol ||r0|| + atol, the stopping test of an FP64 run (r0 of
                                  the initial profile); a system whose FP32 phase diverges is converged
                                  again in FP64 from its initial profile; <= 0: 1e-5 */
 } cdft_solver_opts;
