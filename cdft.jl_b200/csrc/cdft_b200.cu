@@ -118,6 +118,8 @@ struct Batch {
     int cur32 = 0;                          // arithmetic of the running phase: 1 FP32, 0 FP64
     cudaGraphExec_t graph[2] = {nullptr, nullptr};   // indexed by cur32
     int graph_iters[2] = {0, 0};
+    int vec_mb = CDFT_MAX_M;                          // compile-time depth bound of vec_kernel
+    int graph_mb[2] = {0, 0};                         // ... captured in each graph
     long long graph_launches[2] = {0, 0};             // kernel launches captured in each graph
 };
 
@@ -804,8 +806,9 @@ int launch_iteration(Batch* b)
     el_kernel<T><<<b->nechunks, ELEM_THREADS, 0, b->stream>>>(b->d_echunks, b->d_sys, b->d_st, b->d_partials);
     const int ctl_blocks = b->nsys;
     ctl_kernel<<<ctl_blocks, CTL_THREADS, 0, b->stream>>>(b->d_sys, b->d_st, b->d_partials, b->nsys, 0, b->d_done);
+    auto vec = (b->vec_mb <= 8) ? vec_kernel<8> : (b->vec_mb <= 12) ? vec_kernel<12> : vec_kernel<CDFT_MAX_M>;
     for (int slot = 1; slot <= N_VEC_SLOTS; ++slot) {
-        vec_kernel<<<b->nechunks, ELEM_THREADS, 0, b->stream>>>(b->d_echunks, b->d_sys, b->d_st, b->d_partials, slot);
+        vec<<<b->nechunks, ELEM_THREADS, 0, b->stream>>>(b->d_echunks, b->d_sys, b->d_st, b->d_partials, slot);
         if (slot < N_VEC_SLOTS)
             ctl_kernel<<<ctl_blocks, CTL_THREADS, 0, b->stream>>>(b->d_sys, b->d_st, b->d_partials, b->nsys, slot, b->d_done);
     }
@@ -876,7 +879,7 @@ size_t persistent_smem_limit(const Batch* b)
 int batch_capture(Batch* b, int iters)
 {
     const int g32 = b->cur32;
-    if (b->graph[g32] && b->graph_iters[g32] == iters) return 0;
+    if (b->graph[g32] && b->graph_iters[g32] == iters && b->graph_mb[g32] == b->vec_mb) return 0;
     if (b->graph[g32]) {
         cudaGraphExecDestroy(b->graph[g32]);
         b->graph[g32] = nullptr;
@@ -895,6 +898,7 @@ int batch_capture(Batch* b, int iters)
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return set_error(CDFT_E_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
     b->graph_iters[g32] = iters;
+    b->graph_mb[g32] = b->vec_mb;
     return 0;
 }
 
@@ -1012,6 +1016,8 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
         if (rc) return rc;
     } else {
         const int K = opts->iters_per_launch > 0 ? opts->iters_per_launch : 16;
+        // the vector kernel instance whose history bound covers m (8, 12 or CDFT_MAX_M)
+        b->vec_mb = (opts->m <= 8) ? 8 : (opts->m <= 12) ? 12 : CDFT_MAX_M;
         rc = batch_capture(b, K);
         if (rc) return rc;
         long long launched_evals = 0;

@@ -162,13 +162,13 @@ __global__ void phi_points_kernel(PhiParams P, const double* __restrict__ n_in, 
 // ---------------------------------------------------------------------------
 // Block reduction of K partial sums (deterministic order).
 // ---------------------------------------------------------------------------
-template <int BLOCK>
+template <int BLOCK, int NS = RED_SLOTS>
 __device__ __forceinline__ void block_reduce_store(double* vals, int K, double* out)
 {
     __shared__ double red[BLOCK / 32][RED_SLOTS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int c = 0; c < RED_SLOTS; ++c) {
+    for (int c = 0; c < NS; ++c) {
         if (c >= K) break;
         double v = vals[c];
 #pragma unroll
@@ -247,9 +247,10 @@ el_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
 // Applies slot operation `op` to the elements e = e0, e0 + stride, ... < e1 of
 // one system and accumulates this thread's partial sums into acc[0..K).
 // Returns K (0 for the solution updates, which reduce nothing).
-// Column loops are unrolled to the compile-time bound CDFT_MAX_M and left early, so
+// Column loops are unrolled to the compile-time bound MB (>= m) and left early, so
 // the per-element history row and the partial sums stay in registers; dot products
 // use the values just computed instead of reading them back.
+template <int MB = CDFT_MAX_M>
 __device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AAState& A, int e0, int e1, int stride,
                                             double* acc)
 {
@@ -269,18 +270,18 @@ __device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AASta
         for (int e = e0; e < e1; e += stride) {
             const double dv = S.df[e];
             if (down) {   // Q[:, 1:m-1] = Q * Qx; Q[:, m] = 0  (downdate_aaqr!)
-                double row[CDFT_MAX_M];
+                double row[MB];
 #pragma unroll
-                for (int r = 0; r < CDFT_MAX_M; ++r) {
+                for (int r = 0; r < MB; ++r) {
                     if (r >= m) break;
                     row[r] = Q[(size_t)r * n + e];
                 }
 #pragma unroll
-                for (int cc = 0; cc < CDFT_MAX_M - 1; ++cc) {
+                for (int cc = 0; cc < MB - 1; ++cc) {
                     if (cc >= m - 1) break;
                     double v = 0.0;
 #pragma unroll
-                    for (int r = 0; r < CDFT_MAX_M; ++r) {
+                    for (int r = 0; r < MB; ++r) {
                         if (r >= m) break;
                         v += row[r] * A.Qx[r + cc * m];
                     }
@@ -290,7 +291,7 @@ __device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AASta
                 Q[(size_t)(m - 1) * n + e] = 0.0;
             } else {
 #pragma unroll
-                for (int cc = 0; cc < CDFT_MAX_M; ++cc) {
+                for (int cc = 0; cc < MB; ++cc) {
                     if (cc >= K) break;
                     acc[cc] += Q[(size_t)cc * n + e] * dv;
                 }
@@ -302,10 +303,10 @@ __device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AASta
     case OP_SUB_NORM: {
         const int kq = A.kq;
         for (int e = e0; e < e1; e += stride) {
-            double q[CDFT_MAX_M];
+            double q[MB];
             double v = S.df[e];
 #pragma unroll
-            for (int cc = 0; cc < CDFT_MAX_M; ++cc) {
+            for (int cc = 0; cc < MB; ++cc) {
                 if (cc >= kq) break;
                 q[cc] = Q[(size_t)cc * n + e];
                 v += (-A.coef[cc]) * q[cc];   // gemv, alpha = -1
@@ -313,7 +314,7 @@ __device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AASta
             S.df[e] = v;
             if (op == OP_SUB_DOT) {
 #pragma unroll
-                for (int cc = 0; cc < CDFT_MAX_M; ++cc) {
+                for (int cc = 0; cc < MB; ++cc) {
                     if (cc >= kq) break;
                     acc[cc] += q[cc] * v;
                 }
@@ -332,7 +333,7 @@ __device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AASta
             Q[(size_t)kq * n + e] = qn;
             const double rv = S.res[e];
 #pragma unroll
-            for (int cc = 0; cc < CDFT_MAX_M; ++cc) {
+            for (int cc = 0; cc < MB; ++cc) {
                 if (cc >= K) break;
                 acc[cc] += (cc == kq ? qn : Q[(size_t)cc * n + e]) * rv;
             }
@@ -344,7 +345,7 @@ __device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AASta
         for (int e = e0; e < e1; e += stride) {
             double v = S.gx[e];
 #pragma unroll
-            for (int cc = 0; cc < CDFT_MAX_M; ++cc) {
+            for (int cc = 0; cc < MB; ++cc) {
                 if (cc >= mk) break;
                 int slotc = A.head + cc;
                 slotc -= (slotc >= m) ? m : 0;
@@ -367,7 +368,12 @@ __device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AASta
     }
 }
 
-__global__ void __launch_bounds__(ELEM_THREADS)
+// MB: compile-time bound of the Anderson depth m (MB >= m), chosen by the host; the
+// per-thread history rows and partial sums scale with it.  Three resident blocks per SM
+// (80 registers; no spills up to MB = 12) keep enough loads in flight: with the
+// unbounded 128 registers two blocks left this memory-bound kernel latency-bound.
+template <int MB>
+__global__ void __launch_bounds__(ELEM_THREADS, 3)
 vec_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
            const AAState* __restrict__ st, double* __restrict__ partials, int slot)
 {
@@ -376,13 +382,13 @@ vec_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
     const int op = A.op[slot];
     if (op == OP_NONE) return;
     const SysDev& S = sys[c.sys];
-    double acc[RED_SLOTS];
+    double acc[MB];
 #pragma unroll
-    for (int k = 0; k < RED_SLOTS; ++k) acc[k] = 0.0;
+    for (int k = 0; k < MB; ++k) acc[k] = 0.0;
     const int e1 = min(c.begin + ELEM_CHUNK, S.n_elem);
-    const int K = vec_op_range(op, S, A, c.begin + threadIdx.x, e1, ELEM_THREADS, acc);
+    const int K = vec_op_range<MB>(op, S, A, c.begin + threadIdx.x, e1, ELEM_THREADS, acc);
     if (K == 0) return;   // block-uniform
-    block_reduce_store<ELEM_THREADS>(acc, K, partials + (size_t)blockIdx.x * RED_SLOTS);
+    block_reduce_store<ELEM_THREADS, MB>(acc, K, partials + (size_t)blockIdx.x * RED_SLOTS);
 }
 
 // Euler-Lagrange step on a range of elements: ln G = mu - dF/drho, clamp, betafix!,
@@ -737,15 +743,26 @@ ctl_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, const doubl
     __shared__ double red[CTL_THREADS / 32][RED_SLOTS];
     __shared__ double sums[RED_SLOTS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // one pass over this thread's chunk rows with the K sums side by side: the loads of
+    // a row are independent, and each sum still adds its chunks in the same order
+    double v[RED_SLOTS];
+#pragma unroll
+    for (int k = 0; k < RED_SLOTS; ++k) v[k] = 0.0;
+    for (int ch = threadIdx.x; ch < S.chunk_count; ch += CTL_THREADS) {
+        const double* p = partials + (size_t)(S.chunk_begin + ch) * RED_SLOTS;
+#pragma unroll
+        for (int k = 0; k < RED_SLOTS; ++k) {
+            if (k >= K) break;
+            v[k] += p[k];
+        }
+    }
 #pragma unroll
     for (int k = 0; k < RED_SLOTS; ++k) {
         if (k >= K) break;
-        double v = 0.0;
-        for (int ch = threadIdx.x; ch < S.chunk_count; ch += CTL_THREADS)
-            v += partials[(size_t)(S.chunk_begin + ch) * RED_SLOTS + k];
+        double w = v[k];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) red[warp][k] = v;
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        if (lane == 0) red[warp][k] = w;
     }
     __syncthreads();
     if (threadIdx.x < K) {

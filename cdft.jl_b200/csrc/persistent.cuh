@@ -41,27 +41,35 @@ __host__ __device__ __forceinline__ size_t pers_vec_bytes(int n_elem, int m)
     return sizeof(double) * (size_t)n_elem * (6 + 2 * (size_t)m);
 }
 
+// Sums of K per-thread values over the block into sums[0..K), for thread 0 only: the
+// caller lets thread 0 consume them and then synchronises the block.  Threads with
+// index >= active hold exact zeros (they had no element); their warps skip the shuffles
+// and store +0.0, which is what the shuffles would give, so the sums do not change.
 template <int BLOCK>
-__device__ __forceinline__ void block_reduce_to_smem(double* vals, int K, double* sums)
+__device__ __forceinline__ void block_reduce_to_smem(double* vals, int K, double* sums, int active)
 {
     __shared__ double red[BLOCK / 32][RED_SLOTS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp * 32 < active) {
 #pragma unroll
-    for (int c = 0; c < RED_SLOTS; ++c) {
-        if (c >= K) break;
-        double v = vals[c];
+        for (int c = 0; c < RED_SLOTS; ++c) {
+            if (c >= K) break;
+            double v = vals[c];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) red[warp][c] = v;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) red[warp][c] = v;
+        }
+    } else if (lane < K) {
+        red[warp][lane] = 0.0;
     }
     __syncthreads();
-    if (threadIdx.x < K) {
+    if (threadIdx.x < K) {   // warp 0
         double s = 0.0;
 #pragma unroll
         for (int w = 0; w < BLOCK / 32; ++w) s += red[w][threadIdx.x];
         sums[threadIdx.x] = s;
     }
-    __syncthreads();
+    __syncwarp();
 }
 
 // all circulant convolutions of one stage: out[(i*nconv+f)*N + j] = scale * sum_q taps_if[q] in_if[j-q]
@@ -334,7 +342,7 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
                 if (S.vext) dF += S.vext[e];
                 ss[0] += el_elem(S, e, i, dF, beta, aa, DGs);
             }
-            block_reduce_to_smem<PERS_THREADS>(ss, 1, sums);
+            block_reduce_to_smem<PERS_THREADS>(ss, 1, sums, n_elem);
             if (tid == 0) ctl_apply(sA, -1, 0, sums, done_counter, true);
             __syncthreads();
             if (sA.pad0) {   // the QR downdate of this Anderson step, on warp 0
@@ -352,7 +360,7 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
             for (int k = 0; k < RED_SLOTS; ++k) acc[k] = 0.0;
             const int K = vec_op_range(op, S, sA, tid, n_elem, PERS_THREADS, acc);
             if (K > 0) {
-                block_reduce_to_smem<PERS_THREADS>(acc, K, sums);
+                block_reduce_to_smem<PERS_THREADS>(acc, K, sums, n_elem);
                 if (tid == 0) ctl_apply(sA, op, slot, sums, done_counter);
             }
             __syncthreads();
