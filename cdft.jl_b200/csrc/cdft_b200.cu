@@ -676,8 +676,16 @@ int launch_phi(Batch* b, const AAState* st)
         phi_kernel<T, NC_, ND_><<<b->npchunks, POINT_THREADS, 0, b->stream>>>(b->d_pchunks, b->d_sys, st); \
         return 0;                                                                                       \
     }
-    PHI_CASE(1, 1) PHI_CASE(2, 1) PHI_CASE(3, 1) PHI_CASE(4, 1) PHI_CASE(1, 3) PHI_CASE(2, 3)
+    PHI_CASE(1, 1) PHI_CASE(2, 1) PHI_CASE(3, 1) PHI_CASE(4, 1)
 #undef PHI_CASE
+    if (b->nd == 3 && b->nc == 1) {
+        phi_kernel3d<T, 1><<<b->npchunks, POINT_THREADS, 0, b->stream>>>(b->d_pchunks, b->d_sys, st);
+        return 0;
+    }
+    if (b->nd == 3 && b->nc == 2) {
+        phi_kernel3d<T, 2><<<b->npchunks, POINT_THREADS, 0, b->stream>>>(b->d_pchunks, b->d_sys, st);
+        return 0;
+    }
     return set_error(CDFT_E_UNSUPPORTED, "no Phi kernel for nc=%d nd=%d", b->nc, b->nd);
 }
 

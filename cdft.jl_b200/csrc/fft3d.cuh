@@ -26,6 +26,12 @@
 // beat more lines per block once a line exceeds 512 B (measured at 128^3 and 256^3)
 template <typename T, int L> struct FftLines { static constexpr int value = (L * (int)sizeof(T) <= 512) ? 16 : 8; };
 
+// resident blocks per SM the register allocation must allow: unbounded, the FP64 transforms
+// of 128 and 256 points took 96-132 registers (two blocks of 256 threads; shared memory
+// allows five); at 80 registers three fit (+5-8% per 3D iteration, measured).  The other
+// instances used at most 64-72 registers unbounded and get that cap.
+template <typename T, int L> struct FftMinBlocks { static constexpr int value = (sizeof(T) == 8 && L >= 128) ? 3 : 4; };
+
 template <typename T> struct V2;
 template <> struct V2<double> { typedef double2 t; };
 template <> struct V2<float> { typedef float2 t; };
@@ -153,7 +159,7 @@ struct Grid3 {
 __device__ __forceinline__ bool fft_skip(const AAState* st) { return st != nullptr && st[0].mode == MODE_DONE; }
 
 template <typename T, typename Tin, int L, int LINES>
-__global__ void __launch_bounds__(FFT_THREADS)
+__global__ void __launch_bounds__(FFT_THREADS, (FftMinBlocks<T, L>::value))
 fft_x_r2c(const Tin* __restrict__ in, size_t in_stride, typename V2<T>::t* __restrict__ out, size_t out_stride,
           const AAState* __restrict__ st)
 {
@@ -196,7 +202,7 @@ fft_x_r2c(const Tin* __restrict__ in, size_t in_stride, typename V2<T>::t* __res
 // x pass, half spectrum -> real, times `scale`.
 // ---------------------------------------------------------------------------
 template <typename T, int L, int LINES>
-__global__ void __launch_bounds__(FFT_THREADS)
+__global__ void __launch_bounds__(FFT_THREADS, (FftMinBlocks<T, L>::value))
 fft_x_c2r(const typename V2<T>::t* __restrict__ in, size_t in_stride, T* __restrict__ out, size_t out_stride, T scale,
           const AAState* __restrict__ st)
 {
@@ -245,7 +251,7 @@ __device__ __forceinline__ size_t yz_base(int axis, int outer, int kx0)
 }
 
 template <typename T, int L, int LINES>
-__global__ void __launch_bounds__(FFT_THREADS)
+__global__ void __launch_bounds__(FFT_THREADS, (FftMinBlocks<T, L>::value))
 fft_yz(typename V2<T>::t* __restrict__ data, size_t stride, int axis, int inverse, const AAState* __restrict__ st)
 {
     typedef typename V2<T>::t C;
@@ -316,7 +322,7 @@ __device__ __forceinline__ typename V2<T>::t k3_apply(const KTab3& K, int comp, 
 // z pass of the weighted densities: forward z-FFT of the rho spectrum, then for
 // every convolved field: multiply by the kernel and inverse z-FFT into its spectrum.
 template <typename T, int L, int LINES>
-__global__ void __launch_bounds__(FFT_THREADS)
+__global__ void __launch_bounds__(FFT_THREADS, (FftMinBlocks<T, L>::value))
 fft_z_eval(const typename V2<T>::t* __restrict__ R, size_t r_stride, typename V2<T>::t* __restrict__ out,
            size_t out_stride, KTab3 K, const AAState* __restrict__ st)
 {
@@ -370,7 +376,7 @@ fft_z_eval(const typename V2<T>::t* __restrict__ R, size_t r_stride, typename V2
 // z pass of the adjoint: forward z-FFT of every field's dPhi/dn spectrum,
 // accumulate sign_f * kernel_f * spectrum_f, inverse z-FFT of the sum.
 template <typename T, int L, int LINES>
-__global__ void __launch_bounds__(FFT_THREADS)
+__global__ void __launch_bounds__(FFT_THREADS, (FftMinBlocks<T, L>::value))
 fft_z_adjoint(const typename V2<T>::t* __restrict__ in, size_t in_stride, typename V2<T>::t* __restrict__ out,
               size_t out_stride, KTab3 K, const AAState* __restrict__ st)
 {

@@ -121,8 +121,8 @@ __device__ __forceinline__ void load_n(const SysDev& S, int j, T (&n)[NC][6 + ND
 }
 
 template <typename T, int NC, int ND>
-__global__ void __launch_bounds__(POINT_THREADS)
-phi_kernel(const Chunk* __restrict__ pchunks, const SysDev* __restrict__ sys, const AAState* __restrict__ st)
+__device__ __forceinline__ void phi_point(const Chunk* __restrict__ pchunks, const SysDev* __restrict__ sys,
+                                          const AAState* __restrict__ st)
 {
     const Chunk c = pchunks[blockIdx.x];
     if (!sys_active(st, c.sys)) return;
@@ -138,6 +138,22 @@ phi_kernel(const Chunk* __restrict__ pchunks, const SysDev* __restrict__ sys, co
 #pragma unroll
         for (int a = 0; a < 6 + ND; ++a) df[(i * (6 + ND) + a) * S.N + j] = g[i][a];
     S.fval[j] = double(f);
+}
+
+template <typename T, int NC, int ND>
+__global__ void __launch_bounds__(POINT_THREADS)
+phi_kernel(const Chunk* __restrict__ pchunks, const SysDev* __restrict__ sys, const AAState* __restrict__ st)
+{
+    phi_point<T, NC, ND>(pchunks, sys, st);
+}
+
+// The 3D grids' Phi pass streams millions of points: four resident blocks per SM (at
+// most 128 registers; 146 unbounded gave three) keep more loads in flight.
+template <typename T, int NC>
+__global__ void __launch_bounds__(POINT_THREADS, 4)
+phi_kernel3d(const Chunk* __restrict__ pchunks, const SysDev* __restrict__ sys, const AAState* __restrict__ st)
+{
+    phi_point<T, NC, 3>(pchunks, sys, st);
 }
 
 // standalone pointwise evaluation (cdft_phi_pointwise): n, dphi are (npts, NF, nc) column-major
