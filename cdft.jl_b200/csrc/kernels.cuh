@@ -759,26 +759,18 @@ ctl_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, const doubl
     __shared__ double red[CTL_THREADS / 32][RED_SLOTS];
     __shared__ double sums[RED_SLOTS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // one pass over this thread's chunk rows with the K sums side by side: the loads of
-    // a row are independent, and each sum still adds its chunks in the same order
-    double v[RED_SLOTS];
-#pragma unroll
-    for (int k = 0; k < RED_SLOTS; ++k) v[k] = 0.0;
-    for (int ch = threadIdx.x; ch < S.chunk_count; ch += CTL_THREADS) {
-        const double* p = partials + (size_t)(S.chunk_begin + ch) * RED_SLOTS;
-#pragma unroll
-        for (int k = 0; k < RED_SLOTS; ++k) {
-            if (k >= K) break;
-            v[k] += p[k];
-        }
-    }
+    // one sum at a time: the chunk loop of a sum unrolls into independent loads (a loop
+    // over the K sums of a row instead leaves one load in flight per thread behind its
+    // bound check, measured 60% slower)
 #pragma unroll
     for (int k = 0; k < RED_SLOTS; ++k) {
         if (k >= K) break;
-        double w = v[k];
+        double v = 0.0;
+        for (int ch = threadIdx.x; ch < S.chunk_count; ch += CTL_THREADS)
+            v += partials[(size_t)(S.chunk_begin + ch) * RED_SLOTS + k];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
-        if (lane == 0) red[warp][k] = w;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][k] = v;
     }
     __syncthreads();
     if (threadIdx.x < K) {
