@@ -1,7 +1,7 @@
 """GPU parity: the CUDA path (through the C ABI) against the CPU oracle on the
 same seeded inputs.  Tolerances (FP64 path): Phi/gradients and dF/drho 1e-10
-relative to the field's scale; converged profiles 1e-9 relative (the
-BASELINE bar), gamma 1e-9 relative."""
+relative to the field's scale; converged profiles 1e-9 relative (the FP64
+parity bar in rho), gamma 1e-9 relative."""
 import numpy as np
 import pytest
 
