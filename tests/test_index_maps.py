@@ -1,0 +1,178 @@
+"""CPU emulations of the index maps of two device kernels, step by step as the CUDA code
+computes them, against direct NumPy results (no GPU).
+
+- `pers_conv_dmma` (csrc/persistent.cuh): the exact circulant convolution of the persistent
+  engine as a sum of 8x8 Toeplitz tap blocks times 8-column input slabs on the FP64
+  m8n8k4 tensor-core path.  The forward stage reads the periodically extended copy, the
+  adjoint reads dPhi/dn in place through a branch-free wrapped index; both index ranges are
+  checked against their buffers.
+- `fft_lines` / `fft_reg` / the two-rows-in-one packing of `fft_x_r2c` and `fft_x_c2r`
+  (csrc/fft3d.cuh): L = R1 R2 two-pass Cooley-Tukey with radix-2 register DFTs.
+"""
+import numpy as np
+import pytest
+
+PERS_R = 8
+FFT_SPLIT = {32: (4, 8), 64: (8, 8), 128: (8, 16), 256: (16, 16)}   # FftSplit<L>
+
+
+def pers_extn(N):
+    return 2 * N + 32 * (PERS_R + 2)
+
+
+def pers_off(N):
+    return N + 32
+
+
+def dmma_conv(taps, x, periodic):
+    """out[j] = sum_q taps[q] x[(j - q) mod N] as pers_conv_dmma forms it: per warp task
+    (8 output columns u0..u0+7 of 8 outputs each), for d < D two m8n8k4 products
+    A_d[a][c] B_d[c][n] with A_d[a][c] = t(8d + a - c) and B_d[c][n] = x[8(u0 + n - d) + c],
+    c < 4 and c >= 4 in two accumulators."""
+    N = len(taps)
+    U = (N + 7) // 8
+    nut = (U + 7) // 8
+    D = (N + 14) // 8
+    EXTN, OFF = pers_extn(N), pers_off(N)
+    ext = np.array([x[(k - OFF) % N] for k in range(EXTN)])
+    out = np.zeros(N)
+
+    def t(q):
+        return taps[q] if 0 <= q < N else 0.0
+
+    for ut in range(nut):
+        u0 = 8 * ut
+        C0 = np.zeros((8, 8))
+        C1 = np.zeros((8, 8))
+        # lane (r, k): A row r / B column r, A column k / B row k
+        i0 = {(r, k): (8 * (u0 + r) + k) % N for r in range(8) for k in range(4)}
+        for d in range(D):
+            A0 = np.zeros((8, 4))
+            A1 = np.zeros((8, 4))
+            B0 = np.zeros((4, 8))
+            B1 = np.zeros((4, 8))
+            for r in range(8):
+                for k in range(4):
+                    q0 = 8 * d + r - k
+                    A0[r, k] = t(q0)
+                    A1[r, k] = t(q0 - 4)
+                    if periodic:
+                        j0 = i0[(r, k)]
+                        j1 = j0 + 4 - (N if j0 + 4 >= N else 0)
+                        assert 0 <= j0 < N and 0 <= j1 < N, (N, d, r, k, j0, j1)
+                        B0[k, r] = x[j0]
+                        B1[k, r] = x[j1]
+                        j0 -= 8
+                        j0 += N if j0 < 0 else 0
+                        i0[(r, k)] = j0
+                    else:
+                        p = OFF + 8 * (u0 + r) + k - 8 * d
+                        assert 0 <= p and p + 4 < EXTN, (N, d, r, k, p)
+                        B0[k, r] = ext[p]
+                        B1[k, r] = ext[p + 4]
+            C0 += A0 @ B0
+            C1 += A1 @ B1
+        Dm = C0 + C1
+        for a in range(8):
+            for n in range(8):
+                j = 8 * (u0 + n) + a
+                if j < N:
+                    out[j] = Dm[a, n]
+    return out
+
+
+@pytest.mark.parametrize("N", [8, 9, 15, 16, 17, 64, 100, 186, 257, 400])
+@pytest.mark.parametrize("periodic", [False, True])
+def test_dmma_circulant_index_map(N, periodic):
+    rng = np.random.default_rng(N)
+    taps = rng.standard_normal(N)
+    x = rng.standard_normal(N)
+    ref = np.array([sum(taps[q] * x[(j - q) % N] for q in range(N)) for j in range(N)])
+    got = dmma_conv(taps, x, periodic)
+    np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+
+
+def bitrev(i, R):
+    r, b = 0, 1
+    while b < R:
+        r = (r << 1) | (i & 1)
+        i >>= 1
+        b <<= 1
+    return r
+
+
+def fft_tw(L, m, inverse):
+    """w_L^m from the half table tw[q] = exp(-2 pi i q / L), q < L/2, as fft_tw reads it."""
+    w = np.exp(-2j * np.pi * (m & (L // 2 - 1)) / L)
+    if m >= L // 2:
+        w = -w
+    return np.conj(w) if inverse else w
+
+
+def fft_reg(v, L, inverse):
+    v = list(v)
+    R = len(v)
+    for i in range(R):
+        jr = bitrev(i, R)
+        if jr > i:
+            v[i], v[jr] = v[jr], v[i]
+    half = 1
+    while half < R:
+        for q in range(half):
+            w = fft_tw(L, q * (L // (2 * half)), inverse)
+            for b in range(0, R, 2 * half):
+                a, c = v[b + q], v[b + q + half] * w
+                v[b + q], v[b + q + half] = a + c, a - c
+        half <<= 1
+    return v
+
+
+def fft_lines(x, inverse):
+    L = len(x)
+    R1, R2 = FFT_SPLIT[L]
+    y = np.zeros(L, complex)
+    for t in range(R2):
+        u = fft_reg([x[t + R2 * s] for s in range(R1)], L, inverse)
+        for k1 in range(R1):
+            y[k1 * R2 + t] = u[k1] * fft_tw(L, t * k1, inverse)
+    X = np.zeros(L, complex)
+    for k1 in range(R1):
+        v = fft_reg([y[k1 * R2 + t] for t in range(R2)], L, inverse)
+        for k2 in range(R2):
+            X[k1 + R1 * k2] = v[k2]
+    return X
+
+
+@pytest.mark.parametrize("L", sorted(FFT_SPLIT))
+def test_fft_two_pass_split(L):
+    R1, R2 = FFT_SPLIT[L]
+    assert R1 * R2 == L and R1 & (R1 - 1) == 0 and R2 & (R2 - 1) == 0
+    rng = np.random.default_rng(L)
+    x = rng.standard_normal(L) + 1j * rng.standard_normal(L)
+    np.testing.assert_allclose(fft_lines(x, False), np.fft.fft(x), atol=1e-12 * L)
+    np.testing.assert_allclose(fft_lines(x, True), np.fft.ifft(x) * L, atol=1e-12 * L)
+
+
+@pytest.mark.parametrize("L", [32, 128])
+def test_fft_two_real_rows_packing(L):
+    """fft_x_r2c: rows a, b as z = a + i b, X_a = (Z_k + conj Z_{L-k}) / 2,
+    X_b = (Z_k - conj Z_{L-k}) / (2i); fft_x_c2r: the Hermitian extension of X_a + i X_b
+    back, real part L a, imaginary part L b."""
+    rng = np.random.default_rng(L + 1)
+    a, b = rng.standard_normal(L), rng.standard_normal(L)
+    Z = fft_lines(a + 1j * b, False)
+    KX = L // 2 + 1
+    Xa = np.array([(Z[k] + np.conj(Z[(L - k) % L])) / 2 for k in range(KX)])
+    Xb = np.array([(Z[k] - np.conj(Z[(L - k) % L])) / 2j for k in range(KX)])
+    np.testing.assert_allclose(Xa, np.fft.rfft(a), atol=1e-12 * L)
+    np.testing.assert_allclose(Xb, np.fft.rfft(b), atol=1e-12 * L)
+    z = np.zeros(L, complex)
+    for k in range(L):
+        kk = k if k <= L // 2 else L - k
+        xa, xb = Xa[kk], Xb[kk]
+        if k > L // 2:
+            xa, xb = np.conj(xa), np.conj(xb)
+        z[k] = xa + 1j * xb
+    back = fft_lines(z, True) / L
+    np.testing.assert_allclose(back.real, a, atol=1e-12)
+    np.testing.assert_allclose(back.imag, b, atol=1e-12)
