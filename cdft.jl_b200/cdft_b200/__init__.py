@@ -70,6 +70,25 @@ class Steele:
                                    - sg ** 4 / (3 * self.delta[s] * (zz + 0.61 * self.delta[s]) ** 3))
         return V / T
 
+    def potential_radial(self, model, r, T, lb, ub):
+        """V_ext / k_B T on a spherical or cylindrical grid (steele.jl:111-143): the planar
+        single-wall formula at the wall distance r - lb when lb > 0 (fluid outside a solid
+        sphere or cylinder of radius lb), ub - r otherwise (fluid inside a pore of radius
+        ub), clamped below at half the smallest fluid sigma; no second wall."""
+        nc = len(model)
+        r = np.asarray(r, dtype=float)
+        zw = np.maximum(r - lb if lb > 0 else ub - r, 0.5 * np.min(model.sigma))
+        V = np.zeros((nc, r.size))
+        for s in range(len(self.surface)):
+            eps_si = np.sqrt(self.epsilon[s] * model.epsilon)
+            sig_si = (self.sigma[s] + model.sigma) / 2
+            for i in range(nc):
+                sg = sig_si[i]
+                pre = 2 * np.pi * self.rho[s] * eps_si[i] * self.delta[s] * sg ** 2
+                V[i] += pre * (0.4 * (sg / zw) ** 10 - (sg / zw) ** 4
+                               - sg ** 4 / (3 * self.delta[s] * (zw + 0.61 * self.delta[s]) ** 3))
+        return V / T
+
 
 class HardSphereSolutes:
     """Hard spherical solutes in a periodic box (an external field the reference does
@@ -261,7 +280,12 @@ class DFTSystem:
         nd = structure.nd
         self.vext = None
         if self.external_field:
-            if nd == 1:
+            if nd == 1 and structure.coord != "cart":
+                r = structure.coords(0)
+                lb, ub = structure.bounds[0]
+                self.vext = sum(f.potential_radial(model, r, T, lb, ub) if isinstance(f, Steele)
+                                else f.potential(model, r, T) for f in self.external_field)
+            elif nd == 1:
                 z = structure.coords(0)
                 self.vext = sum(f.potential(model, z, T) for f in self.external_field)
             else:

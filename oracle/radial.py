@@ -96,10 +96,11 @@ def radial_derivative_matrix(r):
 
 
 class RadialStructure(fn.Structure):
-    """Uniform1DSphr / Uniform1DCyl: 1D radial grid = the QDHT sampling points on [0, ub]."""
+    """Uniform1DSphr / Uniform1DCyl: 1D radial grid = the QDHT sampling points on [0, ub];
+    lb only places a Steele wall (structure.jl:365-433, steele.jl:111-143)."""
 
-    def __init__(self, conditions, rho_bulk, ub, ngrid, coord):
-        super().__init__(conditions, rho_bulk, [(0.0, ub)], (ngrid,), kind="uniform")
+    def __init__(self, conditions, rho_bulk, ub, ngrid, coord, lb=0.0):
+        super().__init__(conditions, rho_bulk, [(float(lb), ub)], (ngrid,), kind="uniform")
         self.coord = coord
         self.qdht = QDHT(2 if coord == "sphr" else 1, ub, ngrid)
 
@@ -138,11 +139,26 @@ class RadialDFTSystem(fn.DFTSystem):
         return out
 
     def _build_vext(self):
+        """steele.jl:111-143: the planar single-wall Steele formula at the wall distance
+        r - lb (lb > 0: fluid outside a solid sphere/cylinder) or ub - r (lb = 0: fluid in a
+        pore of radius ub), clamped below at 0.5 min(sigma_i); the walls' widths play no part."""
         if self._vext_given is not None:
             return self._vext_given
-        if self.walls:
-            raise NotImplementedError("Steele walls are restated for 1D Cartesian grids")
-        return None
+        if not self.walls:
+            return None
+        r = self.structure.coords(0)
+        lb, ub = self.structure.bounds[0]
+        zw = np.maximum(r - lb if lb > 0 else ub - r, 0.5 * np.min(self.model.sigma))
+        V = np.zeros((self.nc, r.size))
+        for w in self.walls:
+            eps_si = np.sqrt(w.eps * self.model.eps)
+            sig_si = (w.sigma + self.model.sigma) / 2
+            for i in range(self.nc):
+                sg = sig_si[i]
+                pre = 2 * np.pi * w.rho * eps_si[i] * w.delta * sg ** 2
+                V[i] += pre * (2 / 5 * (sg / zw) ** 10 - (sg / zw) ** 4
+                               - sg ** 4 / (3 * w.delta * (zw + 0.61 * w.delta) ** 3))
+        return V / self.structure.T
 
     def weighted_densities(self, rho):
         NA = N_A * self.L ** 3

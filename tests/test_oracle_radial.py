@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 import _systems as S
+from oracle import functional as fn
 from oracle import pcsaft_bulk as pb
 from oracle import radial as rd
 
@@ -51,3 +52,31 @@ def test_product_radial_grid_matches_oracle():
         np.testing.assert_allclose(st.coords(0), ost.coords(0), rtol=1e-14)
         ang = 4 * np.pi if coord == "sphr" else 2 * np.pi
         np.testing.assert_allclose(st.weights, ang * ost.qdht.w, rtol=1e-13)
+
+
+@pytest.mark.parametrize("coord", ["sphr", "cyl"])
+@pytest.mark.parametrize("lb_L", [0.0, 2.0])
+def test_radial_steele_wall(coord, lb_L):
+    """steele.jl:111-143 on a radial grid: lb = 0 a pore wall at ub, lb > 0 a solid core
+    of radius lb; the package's V_ext against the oracle's, the clamp of the wall distance
+    at 0.5 sigma, and a finite potential everywhere."""
+    import cdft_b200 as cd
+    pm, om = S.models(["methane"])
+    T, p = 150.0, 1e7
+    rb = pb.density(om, p, T, [1.0])
+    L = om.length_scale()
+    lb, ub, N = lb_L * L, 10 * L, 151
+    make = cd.Uniform1DSphr if coord == "sphr" else cd.Uniform1DCyl
+    st = make((p, T), [rb], [lb, ub], N)
+    r = st.coords(0)
+    V = cd.Steele(["graphite"]).potential_radial(pm, r, T, *st.bounds[0])
+    so = rd.RadialDFTSystem(om, rd.RadialStructure((p, T), [rb], ub, N, coord, lb=lb),
+                            walls=[fn.SteeleWall.graphite()])
+    np.testing.assert_allclose(V, so.vext, rtol=1e-12)
+    assert np.all(np.isfinite(V))
+    zw = (r - lb) if lb > 0 else (ub - r)
+    clamped = zw <= 0.5 * om.sigma[0]
+    assert clamped.any() and (~clamped).any()
+    assert np.ptp(V[0, clamped]) == 0.0          # one value over the clamped points
+    far = np.argmax(zw)                           # the point farthest from the wall
+    assert abs(V[0, far]) < abs(V[0, clamped][0])
