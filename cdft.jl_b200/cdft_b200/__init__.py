@@ -8,7 +8,7 @@ argument meaning and error behaviour, Julia's ``!`` dropped):
     system    = DFTSystem(model, structure, Steele(["graphite"]))  # src/base/base.jl:75-90
     rho       = initialize_profiles(system)                        # src/structure/structure.jl:50-93
     converge(system, rho, beta=0.1, tol=1e-10, anderson_m=5)        # src/methods/converge.jl:214-254
-    gamma     = surface_tension(system, rho)                       # src/methods/surface_tension.jl:69-91
+    gamma     = surface_tension(system, rho)                       # src/methods/surface_tension.jl:31-53
 
 Every compute call (dF/drho, F_res, converge) runs in libcdft_b200.so on the
 GPU; importing this package raises if the library has not been built.
@@ -556,7 +556,7 @@ def free_energy(system, rho):
 
 
 def surface_tension(system, rho):
-    """surface_tension(system, ρ) (surface_tension.jl:69-91), J/m^2; the
+    """surface_tension(system, ρ) (surface_tension.jl:31-53), J/m^2; the
     periodic two-interface seed gives twice the tension (callers divide by 2)."""
     s = system.structure
     p, T = s.conditions
@@ -567,12 +567,12 @@ def surface_tension(system, rho):
 
 
 def interfacial_tension(system, rho):
-    """interfacial_tension(system, ρ) == surface_tension(system, ρ) (interfacial_tension.jl:155)."""
+    """interfacial_tension(system, ρ) == surface_tension(system, ρ) (interfacial_tension.jl:63)."""
     return surface_tension(system, rho)
 
 
 def adsorption(system, rho):
-    """adsorption(system, ρ) (adsorption.jl:182-188), mol/m^3 of the domain."""
+    """adsorption(system, ρ) (adsorption.jl:26-32), mol/m^3 of the domain."""
     st = system.structure
     V = st.volume() if hasattr(st, "volume") else np.prod([ub - lb for (lb, ub) in st.bounds])
     return np.array([integrate(rho[i], st) / V for i in range(system.nc)])

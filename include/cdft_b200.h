@@ -183,7 +183,7 @@ int cdft_converge_dev(cdft_plan* plan, double* d_rho_inout, const cdft_solver_op
  * sizes allowed) together, every kernel launch covering all of them.  The
  * reference converges one system per converge! call; this replaces a loop of
  * converge! calls over state points (e.g. an isotherm of adsorption(model,
- * surface, p, T), src/methods/adsorption.jl:204-222). */
+ * surface, p, T), src/methods/adsorption.jl:48-65). */
 int cdft_batch_converge(cdft_plan* const* plans, int nplans, double* const* rho_inout,
                         const cdft_solver_opts* opts, cdft_result* results);
 int cdft_batch_converge_dev(cdft_plan* const* plans, int nplans, double* const* d_rho_inout,

@@ -21,7 +21,7 @@ A NumPy FP64 restatement of the reference's converge! path:
 * get_new_profile! -- src/methods/converge.jl:108-153; converge! :220-254
 * free energies, Simpson rule, gamma, adsorption -- models.jl:72-91,
   BasicIdeal.jl:10-38, utils/integrals.jl:17-41 (``_∫``), methods/surface_tension.jl:31-53,
-  methods/adsorption.jl:178-188
+  methods/adsorption.jl:16-32
 
 Array layout: a profile is (nc, *grid) and weighted densities (nc, NF, *grid),
 grid axes in reverse order (..., Nz, Ny, Nx) so the memory order is the
@@ -322,7 +322,7 @@ class DFTSystem:
         return self.F_ideal(rho) + self.F_res(rho)
 
     def surface_tension(self, rho):
-        """surface_tension(system, ρ) (surface_tension.jl:69-91); the caller divides by 2."""
+        """surface_tension(system, ρ) (surface_tension.jl:31-53); the caller divides by 2."""
         s = self.structure
         F = self.free_energy(rho)
         mu = pb.mu_total(self.model, s.rho_bulk, s.T)

@@ -57,7 +57,7 @@ def methane_wall(N=201, width=0.0, precision="fp64", p=1e7, T=150.0):
 
 def slit_pore(H, p, N, T=150.0, precision="fp64"):
     """Methane in a graphite slit of width H (m): bounds [0.7 sigma, H - 0.7 sigma]
-    as adsorption(model, surface, p, T) builds them (adsorption.jl:204-222)."""
+    as adsorption(model, surface, p, T) builds them (adsorption.jl:48-65)."""
     _, om = models(["methane"])
     try:
         rb = pb.density(om, p, T, [1.0], "vapour")
