@@ -198,6 +198,48 @@ int validate_desc(const cdft_system_desc* d)
     return 0;
 }
 
+// Circulant taps (deriv: their derivatives in the kernel radius) of the 6 convolved
+// fields of every component of a 1D Cartesian system, written to out[(i*6 + f)*N + q]:
+// one launch (taps_table_kernel); grids above TAPS_TABLE_MAX_N points take the
+// per-output kernels.  Fields of get_fields(::PCSAFTModel) in 1D (PCSAFT.jl:55-61).
+int launch_taps(cudaStream_t stream, int N, double span, double L, int nc, const double* dred, double* out, bool deriv)
+{
+    const int types[6] = {1, 2, 3, 2, 1, 2};
+    const double wf[6] = {0.5, 0.5, 0.5, 1.0, 1.0, PSI_DISP};
+    if (nc * 6 > TAPS_MAX_TASKS) return set_error(CDFT_E_UNSUPPORTED, "nc=%d", nc);
+    if (N > TAPS_TABLE_MAX_N) {
+        for (int i = 0; i < nc; ++i)
+            for (int f = 0; f < 6; ++f) {
+                double* o = out + ((size_t)i * 6 + f) * N;
+                if (deriv) dtaps1d_kernel<<<(N + 127) / 128, 128, 0, stream>>>(N, span, L, types[f], wf[f] * dred[i], o);
+                else taps1d_kernel<<<(N + 127) / 128, 128, 0, stream>>>(N, span, L, types[f], wf[f] * dred[i], o);
+                g_launches += 1;
+            }
+        CHECK_LAUNCH();
+        return 0;
+    }
+    TapsArgs a;
+    memset(&a, 0, sizeof(a));
+    a.N = N;
+    a.ntask = nc * 6;
+    a.deriv = deriv ? 1 : 0;
+    a.span = span;
+    a.L = L;
+    for (int i = 0; i < nc; ++i)
+        for (int f = 0; f < 6; ++f) {
+            const int t = i * 6 + f;
+            a.type[t] = types[f];
+            a.R[t] = 2.0 * 3.14159265358979323846 * (wf[f] * dred[i]);
+            a.out[t] = out + (size_t)t * N;
+        }
+    const size_t smem = taps_smem_bytes(N);
+    CU(cudaFuncSetAttribute(taps_table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    taps_table_kernel<<<dim3(a.ntask, (N + TAPS_THREADS - 1) / TAPS_THREADS), TAPS_THREADS, smem, stream>>>(a);
+    CHECK_LAUNCH();
+    g_launches += 1;
+    return 0;
+}
+
 int plan_alloc_m(cdft_plan* p, int m)
 {
     if (m <= p->m_cap) return 0;
@@ -437,16 +479,9 @@ int plan_build(cdft_plan* p)
         return rc;
     }
     // kernels of get_fields(::PCSAFTModel) (PCSAFT.jl:55-61), fields 2..7 in 1D
-    const double psi = PSI_DISP;
-    const int types[6] = {1, 2, 3, 2, 1, 2};
-    const double wf[6] = {0.5, 0.5, 0.5, 1.0, 1.0, psi};
     const double span = d.bounds[0][1] - d.bounds[0][0];
-    for (int i = 0; i < nc; ++i)
-        for (int f = 0; f < S.nconv; ++f) {
-            const size_t off = ((size_t)i * S.nconv + f) * N;
-            taps1d_kernel<<<(N + 127) / 128, 128, 0, p->stream>>>(N, span, L, types[f], wf[f] * P.d[i], p->d_taps + off);
-            CHECK_LAUNCH();
-        }
+    int rc = launch_taps(p->stream, N, span, L, nc, P.d, p->d_taps, false);
+    if (rc) return rc;
     if (S.mixed) {
         CU(cudaMalloc(&p->d_taps32, ntap * sizeof(float)));
         to_float_kernel<<<(unsigned)((ntap + 255) / 256), 256, 0, p->stream>>>(p->d_taps, p->d_taps32, ntap);
@@ -1535,7 +1570,6 @@ int cdft_free_energy_res_grad(cdft_plan* plan, const double* rho, double* dF)
         CHECK_LAUNCH();
     }
     const int NP = 2 * nc + 2 * nc * nc + 2;
-    const int types[6] = {1, 2, 3, 2, 1, 2};
     const double wf[6] = {0.5, 0.5, 0.5, 1.0, 1.0, PSI_DISP};
     double *d_dt = nullptr, *d_dn = nullptr, *d_gp = nullptr, *d_kt = nullptr, *d_scale = nullptr;
     const size_t ntap = (size_t)nc * nconv * N;
@@ -1548,11 +1582,15 @@ int cdft_free_energy_res_grad(cdft_plan* plan, const double* rho, double* dF)
     for (int f = 0; f < nconv; ++f) scale[f] = S.NA * 2.0 * 3.14159265358979323846 * wf[f];   // N_A L^3 dR/dd
     CU(cudaMemcpyAsync(d_scale, scale, nconv * sizeof(double), cudaMemcpyHostToDevice, plan->stream));
     const double span = d.bounds[0][1] - d.bounds[0][0];
-    for (int i = 0; i < nc; ++i)
-        for (int f = 0; f < nconv; ++f)
-            dtaps1d_kernel<<<(N + 127) / 128, 128, 0, plan->stream>>>(N, span, L, types[f], wf[f] * S.phi.d[i],
-                                                                     d_dt + ((size_t)i * nconv + f) * N);
-    CHECK_LAUNCH();
+    rc = launch_taps(plan->stream, N, span, L, nc, S.phi.d, d_dt, true);
+    if (rc) {
+        cudaFree(d_dt);
+        cudaFree(d_dn);
+        cudaFree(d_gp);
+        cudaFree(d_kt);
+        cudaFree(d_scale);
+        return rc;
+    }
     dconv1d_kernel<<<dim3((N + 127) / 128, nc * nconv), 128, 0, plan->stream>>>(N, nconv, d_dt, S.rho, d_scale, d_dn);
     CHECK_LAUNCH();
     switch (nc) {
@@ -1830,14 +1868,9 @@ extern "C" int cdft_functional_derivative_noalloc(const cdft_system_desc* desc, 
         CU(cudaMemcpyAsync(base + o_vext, d.vext, sizeof(double) * S.n_elem, cudaMemcpyHostToDevice, stream));
 
     // kernels of get_fields(::PCSAFTModel) in 1D (PCSAFT.jl:55-61), same tables as plan creation
-    const int types[6] = {1, 2, 3, 2, 1, 2};
-    const double wf[6] = {0.5, 0.5, 0.5, 1.0, 1.0, PSI_DISP};
     const double span = d.bounds[0][1] - d.bounds[0][0];
-    for (int i = 0; i < nc; ++i)
-        for (int f = 0; f < S.nconv; ++f)
-            taps1d_kernel<<<(N + 127) / 128, 128, 0, stream>>>(N, span, L, types[f], wf[f] * P.d[i],
-                                                             base + o_taps + ((size_t)i * S.nconv + f) * N);
-    CHECK_LAUNCH();
+    rc = launch_taps(stream, N, span, L, nc, P.d, base + o_taps, false);
+    if (rc) return rc;
     const size_t smem = (size_t)(CONV_QC + CONV_TILE + CONV_QC + 31) * sizeof(double);
     conv1d_kernel<double><<<ntasks, CONV_WARPS * 32, smem, stream>>>(d_tasks, d_sys, nullptr, 0);
     switch (nc) {
@@ -1849,7 +1882,7 @@ extern "C" int cdft_functional_derivative_noalloc(const cdft_system_desc* desc, 
     conv1d_kernel<double><<<ntasks, CONV_WARPS * 32, smem, stream>>>(d_tasks, d_sys, nullptr, 1);
     dfdrho_out_kernel<double><<<nech, ELEM_THREADS, 0, stream>>>(d_ech, d_sys);
     CHECK_LAUNCH();
-    g_launches += 4 + (long long)nc * S.nconv;
+    g_launches += 4;
     CU(cudaStreamSynchronize(stream));
     return 0;
 }

@@ -907,6 +907,70 @@ __global__ void dtaps1d_kernel(int N, double span, double L, int type, double wi
     dtaps[q] = acc / (double)N;
 }
 
+// All circulant taps of one plan in one launch: block (task, q-range) tabulates the
+// closed forms Omega at the non-negative frequencies k <= N/2 and the twiddles
+// cos/sin(2 pi j / N), j < N, in shared memory once, then every thread sums its
+// output q from the tables.  Omega depends on |w| (types 1, 2: the even kernels) or is
+// odd in w (type 3, the vector kernel), so the frequencies k and N - k pair up:
+//   even: t[q] = (1/N) [Omega_0 + 2 sum_{k=1}^{M} Omega_k cos(2 pi k q / N) + (N even) Omega_{N/2} (-1)^q]
+//   odd:  t[q] = (1/N) [-2 sum_{k=1}^{M} Omega_k sin(2 pi k q / N)]          (M = (N-1)/2)
+// the same sum as taps1d_kernel / dtaps1d_kernel (Re of the inverse DFT of the sampled
+// kernel), with O(N) instead of O(N^2) transcendentals per field.  deriv: d Omega / dR.
+#define TAPS_MAX_TASKS 24          // 6 fields x CDFT_MAX_NC components
+#define TAPS_TABLE_MAX_N 8192      // shared tables: (2.5 N + 1) doubles <= 164 KB
+#define TAPS_THREADS 256
+struct TapsArgs {
+    int N, ntask, deriv;
+    double span, L;
+    int type[TAPS_MAX_TASKS];
+    double R[TAPS_MAX_TASKS];      // 2 pi x reduced kernel width
+    double* out[TAPS_MAX_TASKS];
+};
+
+__host__ __device__ __forceinline__ size_t taps_smem_bytes(int N) { return sizeof(double) * (2 * (size_t)N + N / 2 + 1); }
+
+__global__ void __launch_bounds__(TAPS_THREADS) taps_table_kernel(TapsArgs a)
+{
+    extern __shared__ double tsh[];
+    const int N = a.N, H = N / 2 + 1, M = (N - 1) / 2;
+    double* cs = tsh;
+    double* sn = tsh + N;
+    double* om = tsh + 2 * N;
+    const int task = blockIdx.x;
+    const int type = a.type[task];
+    const double R = a.R[task];
+    for (int j = threadIdx.x; j < N; j += TAPS_THREADS) sincospi(2.0 * (double)j / (double)N, &sn[j], &cs[j]);
+    for (int k = threadIdx.x; k < H; k += TAPS_THREADS) {
+        const double w = (double)k / a.span * a.L;
+        om[k] = a.deriv ? kernel_hat_1d_dR(type, w, R) : kernel_hat_1d(type, w, R, 0);
+    }
+    __syncthreads();
+    const int q = blockIdx.y * TAPS_THREADS + threadIdx.x;
+    if (q >= N) return;
+    const double* tab = (type == 3) ? sn : cs;
+    double acc0 = 0.0, acc1 = 0.0;
+    int j = 0;
+    int k = 1;
+    for (; k + 1 <= M; k += 2) {   // two accumulators: independent FMA chains
+        j += q; j -= (j >= N) ? N : 0;
+        acc0 = fma(om[k], tab[j], acc0);
+        j += q; j -= (j >= N) ? N : 0;
+        acc1 = fma(om[k + 1], tab[j], acc1);
+    }
+    if (k <= M) {
+        j += q; j -= (j >= N) ? N : 0;
+        acc0 = fma(om[k], tab[j], acc0);
+    }
+    double t;
+    if (type == 3) {
+        t = -2.0 * (acc0 + acc1);
+    } else {
+        t = om[0] + 2.0 * (acc0 + acc1);
+        if ((N & 1) == 0) t += (q & 1) ? -om[N / 2] : om[N / 2];
+    }
+    a.out[task][q] = t / (double)N;
+}
+
 // dn[(i*nconv + f)*N + j] = scale[f] * sum_q dtaps[(i*nconv + f)*N + q] rho[i*N + (j - q) mod N]
 __global__ void dconv1d_kernel(int N, int nconv, const double* __restrict__ dtaps, const double* __restrict__ rho,
                                const double* __restrict__ scale, double* __restrict__ dn)

@@ -97,6 +97,9 @@ class DFTSystem:
         self.structure = structure
         self.walls = list(walls or [])
         self._vext_given = None if vext is None else np.asarray(vext, dtype=np.float64)
+        # True: the reference's literal White-Bear bracket (FMT.jl:39-45) everywhere,
+        # including |n3| < 0.05 where the series form replaces it by default
+        self.wb_closed = False
         T = structure.T
         self.nc = model.nc
         self.nd = structure.nd
@@ -379,7 +382,7 @@ _WB_SERIES = [(j + 1.0) * (j + 3.0) / (j + 2.0) for j in range(16)]
 _WB_SMALL = 0.05
 
 
-def _wb_bracket(n3, dn, log1dn):
+def _wb_bracket(n3, dn, log1dn, closed_only=False):
     """B(n3) = ln(1-n3)/(12 pi n3^2) + 1/(12 pi n3 (1-n3)^2) (FMT.jl:42-43).
 
     The closed form cancels from O(1/n3) to O(1) as n3 -> 0 (its derivative from
@@ -390,7 +393,7 @@ def _wb_bracket(n3, dn, log1dn):
     with np.errstate(all="ignore"):
         closed = log1dn / (12 * np.pi * n3 * n3) + 1.0 / (12 * np.pi * n3 * dn * dn)
     small = np.abs(np.real(n3)) < _WB_SMALL
-    if not np.any(small):
+    if closed_only or not np.any(small):
         return closed
     ser = _WB_SERIES[-1] + 0 * n3
     for c in _WB_SERIES[-2::-1]:
@@ -426,7 +429,7 @@ def f_res(n, sys):
     nv2sq = sum(nv2[k] * nv2[k] for k in range(nd))
     dn = 1.0 - n3
     log1dn = _logabs(dn)
-    bkt = _wb_bracket(n3, dn, log1dn)
+    bkt = _wb_bracket(n3, dn, log1dn, getattr(sys, "wb_closed", False))
     res_hs = -n0 * log1dn + (n1 * n2 - nv1v2) / dn + (n2 * n2 * n2 / 3 - n2 * nv2sq) * bkt
     # --- f_hc (PCSAFT.jl:123-144) ---
     z3 = z2 = 0.0

@@ -14,30 +14,7 @@ def _rel(a, b):
     return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
 
 
-def _aligned_log_diff(rho, ref):
-    """Max |ln rho - ln ref| after removing the interface displacements.
-
-    A periodic box holding two interfaces at coexistence has two (near-)zero
-    modes: a common translation and a breathing mode (one phase grows while
-    the other shrinks), so two correct solvers can stop with the interfaces a
-    tiny distance apart.  Each half of the box holds one interface (the seed
-    puts them at +-H/4 around the centre); one displacement per half is fitted
-    by least squares with the exact spectral derivative of the periodic
-    N-point problem and removed before comparing.  Returns (max diff, shifts
-    in grid units)."""
-    N = ref.shape[-1]
-    k = np.fft.fftfreq(N) * N
-    lr = np.log(ref)
-    D = np.real(np.fft.ifft(2j * np.pi * k / N * np.fft.fft(lr, axis=-1), axis=-1))
-    d = np.log(rho) - lr
-    r = d.copy()
-    shifts = []
-    for half in (slice(0, N // 2), slice(N // 2, N)):
-        Dh, dh = D[:, half], d[:, half]
-        sh = -np.sum(dh * Dh) / np.sum(Dh * Dh)
-        r[:, half] = dh + sh * Dh
-        shifts.append(float(sh))
-    return float(np.max(np.abs(r))), shifts
+_aligned_log_diff = S.aligned_log_diff
 
 
 @pytest.mark.parametrize("case", ["methane", "water_octane", "octane"])

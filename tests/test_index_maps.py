@@ -176,3 +176,70 @@ def test_fft_two_real_rows_packing(L):
     back = fft_lines(z, True) / L
     np.testing.assert_allclose(back.real, a, atol=1e-12)
     np.testing.assert_allclose(back.imag, b, atol=1e-12)
+
+
+# ---------------------------------------------------------------------------
+# taps_table_kernel (csrc/kernels.cuh): the circulant taps from tabulated closed forms
+# at k <= N/2 and twiddles, frequencies k and N - k folded into one term.
+# ---------------------------------------------------------------------------
+def _kernel_hat_1d(ktype, w, R):
+    """kernel_hat_1d (type 3 returns the coefficient of i of the odd vector kernel)."""
+    two_pi = 2 * np.pi
+    wb = abs(w)
+    if ktype == 1:
+        return 2 * R / two_pi if wb == 0 else 2 * np.sin(wb * R) / wb / two_pi
+    if ktype == 2:
+        if wb == 0:
+            return 4 * np.pi * R ** 3 / 3 / two_pi ** 3
+        return 4 * np.pi / wb ** 3 * (np.sin(wb * R) - R * wb * np.cos(wb * R)) / two_pi ** 3
+    if wb == 0:
+        return 4 * np.pi * R / two_pi ** 3
+    return 4 * np.pi * w / wb ** 3 * (np.sin(wb * R) - R * wb * np.cos(wb * R)) / two_pi ** 3
+
+
+def taps_table(N, span, L, ktype, R):
+    """The kernel's arithmetic, thread by thread: om[k] for k <= N/2, the index j = k q
+    mod N advanced by q per step (two accumulators), the pair/Nyquist terms."""
+    H, M = N // 2 + 1, (N - 1) // 2
+    cs = np.cos(2 * np.pi * np.arange(N) / N)
+    sn = np.sin(2 * np.pi * np.arange(N) / N)
+    om = np.array([_kernel_hat_1d(ktype, k / span * L, R) for k in range(H)])
+    tab = sn if ktype == 3 else cs
+    out = np.empty(N)
+    for q in range(N):
+        acc = [0.0, 0.0]
+        j = 0
+        k = 1
+        while k + 1 <= M:
+            j = (j + q) - (N if j + q >= N else 0)
+            assert 0 <= j < N
+            acc[0] += om[k] * tab[j]
+            j = (j + q) - (N if j + q >= N else 0)
+            acc[1] += om[k + 1] * tab[j]
+            k += 2
+        if k <= M:
+            j = (j + q) - (N if j + q >= N else 0)
+            acc[0] += om[k] * tab[j]
+        if ktype == 3:
+            t = -2 * (acc[0] + acc[1])
+        else:
+            t = om[0] + 2 * (acc[0] + acc[1])
+            if N % 2 == 0:
+                t += -om[N // 2] if q % 2 else om[N // 2]
+        out[q] = t / N
+    return out
+
+
+@pytest.mark.parametrize("N", [8, 9, 100, 143, 201, 256])
+@pytest.mark.parametrize("ktype", [1, 2, 3])
+def test_taps_table_equals_inverse_dft(N, ktype):
+    """Re(ifft(Omega sampled at L fftfreq(N, N/span))) of the reference's sampled kernel
+    (weighted_densities.jl:28-80,193-246; fftfreq convention of structure.jl:153-162)."""
+    span, L = 4.0 * 3.7, 3.7
+    R = 2 * np.pi * 0.5 * 0.95
+    w = np.fft.fftfreq(N) * N / span * L
+    K = np.array([_kernel_hat_1d(ktype, x, R) for x in w])
+    spec = 1j * K if ktype == 3 else K.astype(complex)
+    ref = np.real(np.fft.ifft(spec))
+    got = taps_table(N, span, L, ktype, R)
+    assert np.max(np.abs(got - ref)) <= 1e-14 * np.max(np.abs(ref))
