@@ -8,7 +8,7 @@ cdft_batch_converge.  A step converges all 64 systems from their initial
 profiles.  Metric: state points per second (whole job, all ranks).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
-    python bench.py --impl reference ...   # CPU oracle port of the reference on host cores
+    python bench.py --impl reference ...   # the reference's algorithm compiled for the host cores
 
 Multi-GPU (torchrun): every rank converges its own 64-point isotherm (weak
 scaling, no collective on the data path); the timed region is bracketed by a
@@ -135,6 +135,27 @@ def measured_peaks():
     return None
 
 
+def accuracy_vs_oracle(systems, rhos):
+    """Largest relative errors of converged isotherm results against the oracle fixture
+    of the same 64 state points (tests/golden/c3_isotherm64.npz: the CPU oracle converged
+    to 1e-13): profiles, adsorption and the excess grand potential Omega_ex (the
+    numerator of surface_tension)."""
+    import cdft_b200 as cd
+    path = os.path.join(ROOT, "tests", "golden", "c3_isotherm64.npz")
+    if not os.path.exists(path):
+        return None
+    f = np.load(path)
+    off = f["offsets"]
+    e_rho = e_ads = e_om = 0.0
+    for k, (sy, r) in enumerate(zip(systems, rhos)):
+        ref = f["rho"][off[k]:off[k + 1]]
+        e_rho = max(e_rho, float(np.max(np.abs(r[0] / ref - 1))))
+        e_ads = max(e_ads, abs(cd.adsorption(sy, r)[0] / f["adsorption"][k] - 1))
+        e_om = max(e_om, abs(cd.surface_tension(sy, r) / f["omega_ex"][k] - 1))
+    return {"rho_rel_err_max": e_rho, "adsorption_rel_err_max": e_ads, "omega_ex_rel_err_max": e_om,
+            "oracle": "tests/golden/c3_isotherm64.npz (CPU oracle, FP64, tol 1e-13)"}
+
+
 def run_ours(args, rank, world, local_rank):
     import ctypes
     import torch
@@ -148,35 +169,10 @@ def run_ours(args, rank, world, local_rank):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     lib = _lib.load()
-
     specs = isotherm_specs(rank)
-    systems, rho0 = build_systems(specs, args.precision)
-    n = len(systems)
     stream = torch.cuda.Stream()
-    for s in systems:
-        _lib.check(lib.cdft_plan_set_stream(s._plan, ctypes.c_void_p(stream.cuda_stream)))
-    method = cd.AASol.for_system(None, **SOLVER)
-    opts = method.c_opts(engine=args.engine)
-    plans = (ctypes.c_void_p * n)(*[s._plan.value for s in systems])
-    init_dev = [torch.from_numpy(r).cuda() for r in rho0]
-    work_dev = [torch.empty_like(t) for t in init_dev]
-    ptrs = (ctypes.c_void_p * n)(*[t.data_ptr() for t in work_dev])
-    results = (_lib.Result * n)()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # > 126 MB L2
-
-    def step_dev():
-        with torch.cuda.stream(stream):
-            for w, i in zip(work_dev, init_dev):
-                w.copy_(i, non_blocking=True)
-        _lib.check(lib.cdft_batch_converge_dev(plans, n, ptrs, ctypes.byref(opts), results))
-
-    host_in = [r.copy() for r in rho0]
-    host_work = [np.empty_like(r) for r in rho0]
-
-    def step_e2e():
-        for w, i in zip(host_work, host_in):
-            w[...] = i
-        cd.batch_converge(systems, host_work, method=method, engine=args.engine)
+    method = cd.AASol.for_system(None, **SOLVER)
 
     def timed(fn, steps, warmup):
         for _ in range(warmup):
@@ -201,20 +197,82 @@ def run_ours(args, rank, world, local_rank):
             total = max_over_ranks(total, dist, "cuda")
         return total / steps
 
-    cd.launch_count(reset=True)
+    def device_isotherm(precision, steps, warmup):
+        """Converge the 64 systems from device-resident initial profiles
+        (cdft_batch_converge_dev); CUDA events on the plans' stream."""
+        systems, rho0 = build_systems(specs, precision)
+        n = len(systems)
+        for sy in systems:
+            _lib.check(lib.cdft_plan_set_stream(sy._plan, ctypes.c_void_p(stream.cuda_stream)))
+        opts = method.c_opts(engine=args.engine)
+        plans = (ctypes.c_void_p * n)(*[sy._plan.value for sy in systems])
+        init_dev = [torch.from_numpy(r).cuda() for r in rho0]
+        work_dev = [torch.empty_like(t) for t in init_dev]
+        ptrs = (ctypes.c_void_p * n)(*[t.data_ptr() for t in work_dev])
+        results = (_lib.Result * n)()
+
+        def step():
+            with torch.cuda.stream(stream):
+                for w, i in zip(work_dev, init_dev):
+                    w.copy_(i, non_blocking=True)
+            _lib.check(lib.cdft_batch_converge_dev(plans, n, ptrs, ctypes.byref(opts), results))
+
+        cd.launch_count(reset=True)
+        ms = timed(step, steps, warmup)
+        launches = cd.launch_count(reset=True)
+        evals = [results[i].evaluations for i in range(n)]
+        errc = [results[i].errcode for i in range(n)]
+        rho_out = [t.cpu().numpy() for t in work_dev]
+        return dict(systems=systems, rho0=rho0, plans=plans, ms=ms, evals=evals, errc=errc, rho=rho_out,
+                    launches=int(round(launches * steps / (steps + warmup))))
+
     with ClockSampler(local_rank) as clk:
-        ms_dev = timed(step_dev, args.steps, args.warmup)
-    launches = cd.launch_count(reset=True)
-    # launches of the timed steps only (warm-up launches are identical per step)
-    launches_timed = int(round(launches * args.steps / (args.steps + args.warmup)))
-    iters = [results[i].evaluations for i in range(n)]
-    errc = [results[i].errcode for i in range(n)]
+        run = device_isotherm(args.precision, args.steps, args.warmup)
+    systems, rho0, plans, n = run["systems"], run["rho0"], run["plans"], len(run["systems"])
+    iters, errc, ms_dev = run["evals"], run["errc"], run["ms"]
+
+    # e2e through the public host API: host profiles in, converged host profiles out
+    host_in = [r.copy() for r in rho0]
+    host_work = [np.empty_like(r) for r in rho0]
+
+    def step_e2e():
+        for w, i in zip(host_work, host_in):
+            w[...] = i
+        cd.batch_converge(systems, host_work, method=method, engine=args.engine)
+
     ms_e2e = timed(step_e2e, max(1, args.steps), 1)
 
-    rho_out = [t.cpu().numpy() for t in work_dev]
-    accuracy = None
-    if args.precision == "mixed" and rank == 0:
-        accuracy = mixed_accuracy(specs, systems, rho_out, method)
+    # the user's whole isotherm: adsorption(model, surface, p, T) builds a DFTSystem per state
+    # point (src/methods/adsorption.jl:48-65): plan creation (device tables), initial profiles,
+    # the batched converge and the host copies; host wall clock around synchronised work
+    def step_setup():
+        sy, r0 = build_systems(specs, args.precision)
+        cd.batch_converge(sy, r0, method=method, engine=args.engine)
+        for x in sy:
+            x.close()
+
+    step_setup()
+    torch.cuda.synchronize()
+    t_set = []
+    for _ in range(max(1, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        step_setup()
+        torch.cuda.synchronize()
+        t_set.append(time.perf_counter() - t0)
+    ms_setup = 1e3 * float(np.mean(t_set))
+
+    accuracy = accuracy_vs_oracle(systems, run["rho"]) if rank == 0 else None
+    mixed = None
+    if rank == 0 and args.precision == "fp64" and args.mixed:
+        mr = device_isotherm("mixed", max(2, args.steps // 4), 2)
+        mixed = {"value": round(n / (mr["ms"] * 1e-3), 3), "unit": "state points/s",
+                 "ms_per_step": round(mr["ms"], 4), "speedup_vs_fp64": round(ms_dev / mr["ms"], 3),
+                 "evaluations_per_system": {"min": min(mr["evals"]), "max": max(mr["evals"]),
+                                            "mean": float(np.mean(mr["evals"]))},
+                 "errcodes": sorted(set(mr["errc"])),
+                 "accuracy_vs_oracle": accuracy_vs_oracle(mr["systems"], mr["rho"])}
+        for sy in mr["systems"]:
+            sy.close()
 
     # convolution stage alone (one launch covering all systems), timed with CUDA events
     ms_conv = ctypes.c_double()
@@ -256,7 +314,11 @@ def run_ours(args, rank, world, local_rank):
             },
             "e2e": {"value": round(total_units / (ms_e2e * 1e-3), 3), "unit": "state points/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
-            "gpu_launches": launches_timed,
+            "e2e_with_setup": {
+                "value": round(n / (ms_setup * 1e-3), 3), "unit": "state points/s", "ms_per_step": round(ms_setup, 2),
+                "how": ("64 x (DFTSystem: host bulk thermodynamics + plan creation with its device kernel "
+                        "tables; initialize_profiles) + batched converge with host arrays, host wall clock")},
+            "gpu_launches": run["launches"],
             "roofline": {
                 "kernel": ("persistent_kernel (whole batched converge, 1 launch per step; circulant "
                            "convolutions on the FP64 tensor cores, mma.sync m8n8k4 f64)" if args.engine != "grid"
@@ -275,8 +337,10 @@ def run_ours(args, rank, world, local_rank):
             },
             "clocks": clk.summary(),
         }
-    if rank == 0 and accuracy is not None:
-        line["accuracy_vs_fp64"] = accuracy
+        if accuracy is not None:
+            line["accuracy_vs_oracle"] = accuracy
+        if mixed is not None:
+            line["mixed_isotherm"] = mixed
     if rank == 0 and plain is not None:
         line["plain_fp64_gpu_path"] = plain
     if rank == 0 and args.with3d:
@@ -430,20 +494,6 @@ def run_3d_only(args):
             "config": {"workload": f"solutes3d {N}^3", "solver": SOLVER_3D}, "solutes3d": r}
 
 
-def mixed_accuracy(specs, systems_mixed, rho_mixed, method):
-    """Errors of the mixed-precision results against an FP64 batch of the same systems."""
-    import cdft_b200 as cd
-    s64, r64 = build_systems(specs, "fp64")
-    cd.batch_converge(s64, r64, method=method)
-    e_rho = max(float(np.max(np.abs(a / b - 1))) for a, b in zip(rho_mixed, r64))
-    e_ads = max(abs(cd.adsorption(a, ra)[0] / cd.adsorption(b, rb)[0] - 1)
-                for a, ra, b, rb in zip(systems_mixed, rho_mixed, s64, r64))
-    e_gam = max(abs(cd.surface_tension(a, ra) / cd.surface_tension(b, rb) - 1)
-                for a, ra, b, rb in zip(systems_mixed, rho_mixed, s64, r64))
-    return {"rho_rel_err_max": e_rho, "adsorption_rel_err_max": e_ads,
-            "surface_grand_potential_rel_err_max": e_gam}
-
-
 def plain_fp64_gpu(specs):
     """The plain FP64 GPU path: the same 64 systems converged one converge! call at a
     time with per-stage kernels (the reference's CUDA path structure), wall time."""
@@ -463,65 +513,80 @@ def plain_fp64_gpu(specs):
                    "in an untimed warm-up pass"}
 
 
-def _oracle_converge_one(spec):
-    """Converge one isotherm state point with the CPU oracle (port of the reference)."""
+def _oracle_isotherm_systems(specs):
+    """The isotherm's state points as oracle systems (bulk density of the stable phase)."""
     sys.path.insert(0, ROOT)
     from oracle import functional as fn, pcsaft_bulk as pb
-    H, p, N = spec
     om = pb.PCSAFTModel(["methane"], METHANE["m"], METHANE["sigma"], METHANE["epsilon"])
-    rl = pb.density(om, p, T_ISO, [1.0], "liquid")
-    rv = pb.density(om, p, T_ISO, [1.0], "vapour")
-    if abs(rl / rv - 1) > 1e-10:
-        g = [pb.mu_total(om, [r], T_ISO)[0] for r in (rl, rv)]
-        rb = rl if g[0] <= g[1] else rv
-    else:
-        rb = rl
     s = om.sigma[0]
-    st = fn.Structure((p, T_ISO), [rb], [(0.7 * s, H - 0.7 * s)], (N,))
-    so = fn.DFTSystem(om, st, [fn.SteeleWall.graphite(H)])
-    t = time.perf_counter()
-    r, out = so.converge(so.initialize_profiles(), **SOLVER)
-    return time.perf_counter() - t, out.errcode
+    out = []
+    for H, p, N in specs:
+        roots = []
+        for ph in ("liquid", "vapour"):
+            try:
+                roots.append(pb.density(om, p, T_ISO, [1.0], ph))
+            except RuntimeError:
+                pass
+        rb = roots[0]
+        if len(roots) == 2 and abs(roots[0] / roots[1] - 1) > 1e-10:
+            g = [pb.mu_total(om, [r], T_ISO)[0] for r in roots]
+            rb = roots[0] if g[0] <= g[1] else roots[1]
+        st = fn.Structure((p, T_ISO), [rb], [(0.7 * s, H - 0.7 * s)], (N,))
+        out.append(fn.DFTSystem(om, st, [fn.SteeleWall.graphite(H)]))
+    return out
+
+
+def _cpu_isotherm_step(systems, rho0, threads):
+    """One converge of all state points by the C++ restatement of the reference's
+    converge! (oracle/cpu_converge.cpp) on `threads` host threads; seconds."""
+    from oracle import cpu
+    rhos = [r.copy() for r in rho0]
+    t0 = time.perf_counter()
+    res, _ = cpu.batch_converge(systems, rhos, nthreads=threads, **SOLVER)
+    dt = time.perf_counter() - t0
+    return dt, [r.errcode for r in res]
 
 
 def cpu_baseline(specs, budget_s=20.0):
-    """Oracle (NumPy port of the reference) on one host core over a bounded sample."""
-    done, t_total = 0, 0.0
-    order = specs[::9] + [s for i, s in enumerate(specs) if i % 9]   # spread over widths/pressures first
-    for spec in order:
-        dt, _ = _oracle_converge_one(spec)
-        t_total += dt
-        done += 1
-        if t_total > budget_s:
-            break
-    return {"value": round(done / t_total, 4), "unit": "state points/s", "cores": 1, "kind": "port",
-            "sample": f"{done} of the 64 isotherm state points, oracle converge! (NumPy FP64), 1 thread"}
+    """The reference's algorithm compiled for the host (C++ restatement, FFT convolutions,
+    forward-mode dPhi/dn, aasol) on all host cores: whole 64-point isotherm per step,
+    repeated while the budget lasts (at least once)."""
+    from oracle import cpu
+    cpu.build()
+    cores = os.cpu_count() or 1
+    systems = _oracle_isotherm_systems(specs)
+    rho0 = [so.initialize_profiles() for so in systems]
+    times = []
+    while not times or (sum(times) < budget_s and len(times) < 5):
+        dt, errc = _cpu_isotherm_step(systems, rho0, cores)
+        times.append(dt)
+    return {"value": round(len(specs) / float(np.mean(times)), 3), "unit": "state points/s", "cores": cores,
+            "kind": "port", "errcodes": sorted(set(errc)),
+            "sample": (f"all {len(specs)} isotherm state points per step, {len(times)} steps; C++17 OpenMP "
+                       "restatement of converge! (oracle/cpu_converge.cpp: Bluestein-FFT convolutions, "
+                       "forward-mode dual-number dPhi/dn, aasol), one thread per state point, FP64")}
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference's CPU implementation of the path.  Julia is
-    not available here, so this is the oracle port, run with one process per
-    host core; each step converges one bounded sample of state points."""
+    """--impl reference: the reference's converge! on the host cores.  Julia is not
+    available, so this is the compiled restatement of the reference's algorithm
+    (oracle/cpu_converge.cpp) on all host threads, each step the whole 64-point
+    isotherm (the configuration of the GPU arm)."""
     if rank != 0:
         return None
-    import multiprocessing as mp
+    from oracle import cpu
+    cpu.build()
     cores = os.cpu_count() or 1
     specs = isotherm_specs(0)
-    ctx = mp.get_context("spawn")
-    per_step = cores
+    systems = _oracle_isotherm_systems(specs)
+    rho0 = [so.initialize_profiles() for so in systems]
     times = []
-    with ctx.Pool(cores) as pool:
-        k = 0
-        for it in range(args.warmup + args.steps):
-            sample = [specs[(k + j) % len(specs)] for j in range(per_step)]
-            k += per_step
-            t0 = time.perf_counter()
-            pool.map(_oracle_converge_one, sample)
-            dt = time.perf_counter() - t0
-            if it >= args.warmup:
-                times.append(dt)
+    for it in range(args.warmup + args.steps):
+        dt, errc = _cpu_isotherm_step(systems, rho0, cores)
+        if it >= args.warmup:
+            times.append(dt)
     ms = 1e3 * float(np.mean(times))
-    value = per_step / (ms * 1e-3)
+    value = len(specs) / (ms * 1e-3)
     return {
         "impl": "reference",
         "metric": "state points/s (64-point slit-pore adsorption isotherm, batched converge!)",
@@ -537,9 +602,10 @@ def run_reference(args, rank, world):
         "dtype": "f64",
         "data": "synthetic: seeded isotherm state points, PC-SAFT methane parameters",
         "config": {"workload": "isotherm64: methane 150 K, graphite slit pores 2-8 nm x 1e3-1e7 Pa, N=100..400",
-                   "solver": SOLVER, "sample_per_step": per_step},
+                   "solver": SOLVER, "state_points_per_step": len(specs), "errcodes": sorted(set(errc))},
         "cpu_baseline": {"value": round(value, 4), "unit": "state points/s", "cores": cores, "kind": "port",
-                         "sample": f"{per_step} state points per step, one per process (spawn pool)"},
+                         "sample": (f"all {len(specs)} state points per step on {cores} OpenMP threads; C++17 "
+                                    "restatement of the reference's converge! (oracle/cpu_converge.cpp)")},
         "e2e": {"value": round(value, 4), "unit": "state points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -555,6 +621,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-plain", dest="plain", action="store_false", help="skip the sequential FP64 comparison")
+    ap.add_argument("--no-mixed", dest="mixed", action="store_false", help="skip the mixed-precision isotherm")
     ap.add_argument("--no-3d", dest="with3d", action="store_false", help="skip the 3D solutes configuration")
     ap.add_argument("--grid3d", type=int, nargs="+", default=[128, 256])
     ap.add_argument("--only3d", action="store_true",

@@ -30,7 +30,7 @@ __all__ = [
     "initialize_profiles", "converge", "batch_converge", "dFdrho_res", "F_res", "F_ideal",
     "free_energy", "surface_tension", "interfacial_tension", "adsorption", "integrate",
     "F_res_grad", "grad_params", "dgamma_dtheta",
-    "CDFTError", "launch_count",
+    "CDFTError", "launch_count", "tuning",
 ]
 
 PSI = 1.3862
@@ -615,6 +615,16 @@ def dgamma_dtheta(system, rho):
     from .thermo import coexistence_sensitivity
     dmu, dp = coexistence_sensitivity(system.model, T, s.rho_bulk, s.rho_bulk2, p=p)
     return grad_params(system, rho, dmu, dp) / 2
+
+
+def tuning(name, value=None):
+    """Get (and with ``value``, first set) a launch shape of the autotuner by name,
+    process-wide (cdft_tuning_get / cdft_tuning_set)."""
+    if value is not None:
+        _lib.check(_LIB.cdft_tuning_set(name.encode(), int(value)))
+    out = ctypes.c_int()
+    _lib.check(_LIB.cdft_tuning_get(name.encode(), ctypes.byref(out)))
+    return out.value
 
 
 def launch_count(reset=False):

@@ -37,6 +37,7 @@ EXPORTED = [
     "cdft_converge", "cdft_converge_dev",
     "cdft_batch_converge", "cdft_batch_converge_dev",
     "cdft_plan_set_stream", "cdft_batch_time_stage", "cdft_functional_derivative_noalloc",
+    "cdft_tuning_get", "cdft_tuning_set",
     "cdft_launch_count", "cdft_last_error", "cdft_version",
 ]
 
@@ -130,6 +131,8 @@ def load(path=LIB_PATH):
     lib.cdft_plan_set_stream.argtypes = [P, P]
     lib.cdft_batch_time_stage.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
     lib.cdft_functional_derivative_noalloc.argtypes = [ctypes.POINTER(SystemDesc), P, P, P]
+    lib.cdft_tuning_get.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]
+    lib.cdft_tuning_set.argtypes = [ctypes.c_char_p, ctypes.c_int]
     lib.cdft_launch_count.argtypes = [ctypes.c_int]
     lib.cdft_launch_count.restype = ctypes.c_longlong
     lib.cdft_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]

@@ -18,6 +18,7 @@
 
 #include "persistent.cuh"
 #include "fft3d.cuh"
+#include "tuning.cuh"
 
 namespace {
 
@@ -248,13 +249,15 @@ int plan_alloc_m(cdft_plan* p, int m)
     p->d_Q = p->d_DG = nullptr;
     const size_t ne = (size_t)p->sys.n_elem;
     const size_t cols = (size_t)(m > 0 ? m : 1);
-    CU(cudaMalloc(&p->d_Q, ne * cols * sizeof(double)));
+    const int qs = (int)(cols + (cols & 1));   // row-major QR history, 16-byte aligned rows
+    CU(cudaMalloc(&p->d_Q, ne * qs * sizeof(double)));
     CU(cudaMalloc(&p->d_DG, ne * cols * sizeof(double)));
-    CU(cudaMemsetAsync(p->d_Q, 0, ne * cols * sizeof(double), p->stream));
+    CU(cudaMemsetAsync(p->d_Q, 0, ne * qs * sizeof(double), p->stream));
     CU(cudaMemsetAsync(p->d_DG, 0, ne * cols * sizeof(double), p->stream));
     p->m_cap = m;
     p->sys.Q = p->d_Q;
     p->sys.DG = p->d_DG;
+    p->sys.qs = qs;
     return 0;
 }
 
@@ -865,7 +868,8 @@ int launch_persistent_nc(Batch* b, int max_evals, size_t smem, int vec_m)
 {
     auto kern = persistent_kernel<T, NC, 1>;
     CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<b->nsys, PERS_THREADS, smem, b->stream>>>(b->d_sys, b->d_st, b->d_done, max_evals, vec_m);
+    kern<<<b->nsys, PERS_THREADS, smem, b->stream>>>(b->d_sys, b->d_st, b->d_done, max_evals, vec_m,
+                                                     g_tuned.pers_warp_aa_max_elem);
     CHECK_LAUNCH();
     g_launches += 1;
     return 0;
@@ -1032,10 +1036,13 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
     if (b->nd == 1 && b->coord == CDFT_COORD_CART &&
         (opts->engine == CDFT_ENGINE_AUTO || opts->engine == CDFT_ENGINE_PERSISTENT)) {
         const size_t need = persistent_smem_need(b), limit = persistent_smem_limit(b);
-        use_persistent = need <= limit;
-        if (!use_persistent && opts->engine == CDFT_ENGINE_PERSISTENT)
+        use_persistent = need <= limit && opts->m <= PERS_MAX_M;
+        if (!use_persistent && opts->engine == CDFT_ENGINE_PERSISTENT) {
+            if (opts->m > PERS_MAX_M)
+                return set_error(CDFT_E_UNSUPPORTED, "persistent engine takes Anderson depths m <= %d", PERS_MAX_M);
             return set_error(CDFT_E_UNSUPPORTED, "persistent engine needs %zu B of shared memory per system (limit %zu)",
                              need, limit);
+        }
     }
     int rc = 0;
     if (use_persistent) {
@@ -1530,7 +1537,26 @@ int cdft_last_error(char* buf, size_t len)
     return g_err_code;
 }
 
-const char* cdft_version(void) { return "cdft_b200 0.1 (sm_100a)"; }
+const char* cdft_version(void) { return "cdft_b200 0.2 (sm_100a)"; }
+
+int cdft_tuning_get(const char* name, int* value)
+{
+    g_err_code = 0;
+    const TunedEntry* e = tuned_entry(name);
+    if (!e || !value) return set_error(CDFT_E_INVALID, "unknown tuning entry %s", name ? name : "(null)");
+    *value = g_tuned.*(e->field);
+    return 0;
+}
+
+int cdft_tuning_set(const char* name, int value)
+{
+    g_err_code = 0;
+    const TunedEntry* e = tuned_entry(name);
+    if (!e) return set_error(CDFT_E_INVALID, "unknown tuning entry %s", name ? name : "(null)");
+    if (value < e->lo || value > e->hi) return set_error(CDFT_E_INVALID, "%s=%d out of [%d, %d]", name, value, e->lo, e->hi);
+    g_tuned.*(e->field) = value;
+    return 0;
+}
 
 // ---------------------------------------------------------------------------
 // Parameter gradient of F_res and of the excess grand potential (1D)

@@ -27,18 +27,20 @@
 // solver modes (the phase of aasol a system is in when its next G evaluation runs)
 enum { MODE_EVAL_INIT = 0, MODE_EVAL_PICARD = 1, MODE_EVAL_AA = 2, MODE_DONE = 3 };
 
-// vector-slot operations between two fixed-point evaluations (see ctl_kernel)
+// vector-slot operations between two fixed-point evaluations (see ctl_kernel): the CGS2
+// QR update of aa_qr_update! (anderson.jl:498-540) in three passes over the elements, and
+// the solution update
 enum {
     OP_NONE = 0,
-    OP_NORM_DF = 1,        // partial ||df||^2
-    OP_DOT_H1 = 2,         // [Q <- Q*Qx if downdate]; partial Q^T df
-    OP_SUB_DOT = 3,        // df -= Q h1; partial Q^T df
-    OP_SUB_NORM = 4,       // df -= Q h2; partial ||df||^2
-    OP_SETQ_DOT_TRES = 5,  // Q[:,kq] = df / r; partial Q[:, :mk]^T res
-    OP_SOL_AA = 6,         // sol = gx - DG theta; rho = exp(sol)
-    OP_SOL_COPY = 7        // sol = gx; rho = exp(sol)
+    OP_NORM_DF = 1,        // partial ||df||^2 (first column of the QR factor)
+    OP_DOT_H1 = 2,         // partial h1 = Q^T df
+    OP_SUB_DOT_NORM = 3,   // df <- df - Q h1; partial h2 = Q^T df and ||df||^2
+    OP_SETQ_DOT_TRES = 4,  // q = (df - Q h2) / r; partial [Q q]^T res; store q, or [Q q] Qx
+                           // when the next step starts with the QR downdate
+    OP_SOL_AA = 5,         // sol = gx - DG theta; rho = exp(sol)
+    OP_SOL_COPY = 6        // sol = gx; rho = exp(sol)
 };
-#define N_VEC_SLOTS 5
+#define N_VEC_SLOTS 4
 
 struct PhiParams {
     int nc, nd;
@@ -71,8 +73,9 @@ struct SysDev {
     double* gx;
     double* res;
     double* df;
-    double* Q;                   // [c*n_elem + e]
+    double* Q;                   // QR history, row-major: [e*qs + c]
     double* DG;                  // [slot*n_elem + e]
+    int qs;                      // row stride of Q (doubles, even: rows start 16-byte aligned)
     void* part;                  // convolution partials [((i*nconv+f)*ksplit+ks)*N + j] (double or float)
     void* dfield;                // dPhi/dn [(i*NF+a)*N + j] (double or float)
     double* fval;                // Phi per point
@@ -86,7 +89,8 @@ struct AAState {
     int errcode, idid, toosoon, m;
     int maxit, picard_maxit;
     int head, dg_slot, kq, mk;
-    int downdate, pad0;
+    int downdate;                // the next Anderson step starts from the downdated QR (Rn, Qx)
+    int pad0;                    // persistent engine: a warp-parallel downdate is pending
     int op[N_VEC_SLOTS + 1];
     double beta, picard_beta, rtol, atol, picard_rtol, picard_atol;
     double resnorm, tol, picard_tol, up_bd;
@@ -94,7 +98,9 @@ struct AAState {
     double coef[CDFT_MAX_M];     // coefficients of the current slot op
     double h1[CDFT_MAX_M];
     double R[CDFT_MAX_M * CDFT_MAX_M];     // column-major m x m
+    double Rn[CDFT_MAX_M * CDFT_MAX_M];    // the downdated R of the next step (column-major m x m)
     double Qx[CDFT_MAX_M * CDFT_MAX_M];    // column-major m x (m-1)
+    double tau[CDFT_MAX_M], v1[CDFT_MAX_M];  // Householder reflectors of the downdate
     double* history;
     int history_cap, pad1;
 };

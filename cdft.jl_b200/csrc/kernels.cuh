@@ -264,15 +264,37 @@ el_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
 // Applies slot operation `op` to the elements e = e0, e0 + stride, ... < e1 of
 // one system and accumulates this thread's partial sums into acc[0..K).
 // Returns K (0 for the solution updates, which reduce nothing).
-// Column loops are unrolled to the compile-time bound MB (>= m) and left early, so
-// the per-element history row and the partial sums stay in registers; dot products
-// use the values just computed instead of reading them back.
+// The history Q is row-major (one element's row of Q contiguous, qs doubles, 16-byte
+// aligned), so a row arrives in 16-byte loads and stays in registers; column loops are
+// unrolled to the compile-time bound MB (>= m) and left early.
+//
+// One Anderson step's CGS2 update (Orthogonalize!, anderson.jl:525-540) in three passes:
+//   DOT_H1:        h1 = Q^T df
+//   SUB_DOT_NORM:  df1 = df - Q h1 (stored);  h2 = Q^T df1,  ||df1||^2
+//   SETQ_DOT_TRES: df2 = df1 - Q h2,  q = df2 / r,  tres = [Q q]^T res
+// with r = ||df2|| = sqrt(||df1||^2 - ||h2||^2), exact for orthonormal Q (the reference
+// forms df2 in a third pass and takes its norm).  When the next step starts with the QR
+// downdate (downdate_aaqr!, anderson.jl:552-583), its Qx is known before SETQ_DOT_TRES,
+// which then stores the rotated row [Q q] Qx instead of q alone.
+template <int MB>
+__device__ __forceinline__ void load_qrow(const double* __restrict__ p, int cnt, double (&row)[MB])
+{
+#pragma unroll
+    for (int c = 0; c < MB; c += 2) {
+        if (c >= cnt) break;
+        const double2 v = *reinterpret_cast<const double2*>(p + c);
+        row[c] = v.x;
+        if (c + 1 < MB) row[c + 1] = v.y;
+    }
+}
+
 template <int MB = CDFT_MAX_M>
 __device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AAState& A, int e0, int e1, int stride,
                                             double* acc)
 {
     const int n = S.n_elem;
     const int m = A.m;
+    const int qs = S.qs;
     double* __restrict__ Q = S.Q;
     switch (op) {
     case OP_NORM_DF:
@@ -282,80 +304,93 @@ __device__ __forceinline__ int vec_op_range(int op, const SysDev& S, const AASta
         }
         return 1;
     case OP_DOT_H1: {
-        const int K = A.kq;
-        const bool down = A.downdate;
-        for (int e = e0; e < e1; e += stride) {
-            const double dv = S.df[e];
-            if (down) {   // Q[:, 1:m-1] = Q * Qx; Q[:, m] = 0  (downdate_aaqr!)
-                double row[MB];
-#pragma unroll
-                for (int r = 0; r < MB; ++r) {
-                    if (r >= m) break;
-                    row[r] = Q[(size_t)r * n + e];
-                }
-#pragma unroll
-                for (int cc = 0; cc < MB - 1; ++cc) {
-                    if (cc >= m - 1) break;
-                    double v = 0.0;
-#pragma unroll
-                    for (int r = 0; r < MB; ++r) {
-                        if (r >= m) break;
-                        v += row[r] * A.Qx[r + cc * m];
-                    }
-                    Q[(size_t)cc * n + e] = v;
-                    if (cc < K) acc[cc] += v * dv;
-                }
-                Q[(size_t)(m - 1) * n + e] = 0.0;
-            } else {
-#pragma unroll
-                for (int cc = 0; cc < MB; ++cc) {
-                    if (cc >= K) break;
-                    acc[cc] += Q[(size_t)cc * n + e] * dv;
-                }
-            }
-        }
-        return K;
-    }
-    case OP_SUB_DOT:
-    case OP_SUB_NORM: {
         const int kq = A.kq;
         for (int e = e0; e < e1; e += stride) {
             double q[MB];
+            load_qrow<MB>(Q + (size_t)e * qs, kq, q);
+            const double dv = S.df[e];
+#pragma unroll
+            for (int cc = 0; cc < MB; ++cc) {
+                if (cc >= kq) break;
+                acc[cc] += q[cc] * dv;
+            }
+        }
+        return kq;
+    }
+    case OP_SUB_DOT_NORM: {
+        const int kq = A.kq;
+        for (int e = e0; e < e1; e += stride) {
+            double q[MB];
+            load_qrow<MB>(Q + (size_t)e * qs, kq, q);
             double v = S.df[e];
 #pragma unroll
             for (int cc = 0; cc < MB; ++cc) {
                 if (cc >= kq) break;
-                q[cc] = Q[(size_t)cc * n + e];
                 v += (-A.coef[cc]) * q[cc];   // gemv, alpha = -1
             }
             S.df[e] = v;
-            if (op == OP_SUB_DOT) {
 #pragma unroll
-                for (int cc = 0; cc < MB; ++cc) {
-                    if (cc >= kq) break;
-                    acc[cc] += q[cc] * v;
-                }
-            } else {
-                acc[0] += v * v;
+            for (int cc = 0; cc < MB; ++cc) {
+                if (cc >= kq) break;
+                acc[cc] += q[cc] * v;
             }
+#pragma unroll
+            for (int cc = 0; cc <= MB; ++cc)
+                if (cc == kq) acc[cc] += v * v;   // ||df1||^2 in slot kq
         }
-        return (op == OP_SUB_DOT) ? kq : 1;
+        return kq + 1;
     }
     case OP_SETQ_DOT_TRES: {
-        const int kq = A.kq;
-        const int K = A.mk;
+        const int kq = A.kq;   // the new column's index; mk = kq + 1 columns enter tres
         const double r = A.rnorm;
+        const bool down = A.downdate;
         for (int e = e0; e < e1; e += stride) {
-            const double qn = S.df[e] / r;
-            Q[(size_t)kq * n + e] = qn;
+            double q[MB];
+            double* row = Q + (size_t)e * qs;
+            load_qrow<MB>(row, kq, q);
+            double v = S.df[e];
+#pragma unroll
+            for (int cc = 0; cc < MB; ++cc) {
+                if (cc >= kq) break;
+                v += (-A.coef[cc]) * q[cc];   // df2 = df1 - Q h2
+            }
+            const double qn = v / r;
             const double rv = S.res[e];
 #pragma unroll
             for (int cc = 0; cc < MB; ++cc) {
-                if (cc >= K) break;
-                acc[cc] += (cc == kq ? qn : Q[(size_t)cc * n + e]) * rv;
+                if (cc >= kq) break;
+                acc[cc] += q[cc] * rv;
+            }
+#pragma unroll
+            for (int cc = 0; cc <= MB; ++cc)
+                if (cc == kq) acc[cc] += qn * rv;
+            if (down) {   // next step's Q[:, 1:m-1] = [Q q] Qx (here kq = m - 1)
+#pragma unroll
+                for (int cc = 0; cc < MB; cc += 2) {
+                    if (cc >= kq) break;
+                    const double* x0 = A.Qx + cc * m;
+                    double o0 = qn * x0[kq], o1 = 0.0;
+#pragma unroll
+                    for (int rr = 0; rr < MB; ++rr) {
+                        if (rr >= kq) break;
+                        o0 += q[rr] * x0[rr];
+                    }
+                    if (cc + 1 < kq) {
+                        const double* x1 = x0 + m;
+                        o1 = qn * x1[kq];
+#pragma unroll
+                        for (int rr = 0; rr < MB; ++rr) {
+                            if (rr >= kq) break;
+                            o1 += q[rr] * x1[rr];
+                        }
+                    }
+                    *reinterpret_cast<double2*>(row + cc) = make_double2(o0, o1);
+                }
+            } else {
+                row[kq] = qn;
             }
         }
-        return K;
+        return kq + 1;
     }
     case OP_SOL_AA: {
         const int mk = A.mk;
@@ -399,13 +434,13 @@ vec_kernel(const Chunk* __restrict__ echunks, const SysDev* __restrict__ sys,
     const int op = A.op[slot];
     if (op == OP_NONE) return;
     const SysDev& S = sys[c.sys];
-    double acc[MB];
+    double acc[MB + 1];
 #pragma unroll
-    for (int k = 0; k < MB; ++k) acc[k] = 0.0;
+    for (int k = 0; k < MB + 1; ++k) acc[k] = 0.0;
     const int e1 = min(c.begin + ELEM_CHUNK, S.n_elem);
     const int K = vec_op_range<MB>(op, S, A, c.begin + threadIdx.x, e1, ELEM_THREADS, acc);
     if (K == 0) return;   // block-uniform
-    block_reduce_store<ELEM_THREADS, MB>(acc, K, partials + (size_t)blockIdx.x * RED_SLOTS);
+    block_reduce_store<ELEM_THREADS, MB + 1>(acc, K, partials + (size_t)blockIdx.x * RED_SLOTS);
 }
 
 // Euler-Lagrange step on a range of elements: ln G = mu - dF/drho, clamp, betafix!,
@@ -479,12 +514,17 @@ __device__ void aa_anderson_start(AAState& A)
 // upper Hessenberg, and every reflector keeps it so: the vector below the
 // diagonal of column j has the single entry at row j+1, each reflector touches
 // rows j and j+1 only.  The loops run over those rows (the dense loops add
-// exact zeros), in place on R with the column offset of the slice.
+// exact zeros).  The downdate of the NEXT Anderson step is formed while this
+// step still needs R for its solve: it works on the copy Rn (with the column
+// offset of the slice) and leaves the thin Q factor in Qx; after this step's
+// solve Rn replaces R (aa_apply_downdate).
 __device__ void aa_downdate(AAState& A)
 {
     const int m = A.m, n = m - 1;
-    double* R = A.R;
-    double tau[CDFT_MAX_M], v1[CDFT_MAX_M];
+    double* R = A.Rn;
+    for (int k = 0; k < m * m; ++k) R[k] = A.R[k];
+    double* tau = A.tau;
+    double* v1 = A.v1;
     for (int j = 0; j < n; ++j) {
         const double alpha = R[j + (j + 1) * m];
         const double x = R[j + 1 + (j + 1) * m];
@@ -516,24 +556,23 @@ __device__ void aa_downdate(AAState& A)
             Qx[j + 1 + c * m] = fma(-(tau[j] * v1[j]), w, Qx[j + 1 + c * m]);
         }
     }
-    // R[1:m-1, 1:m-1] = upper triangle of the slice; R[:, m] = 0
+    // Rn[1:m-1, 1:m-1] = upper triangle of the slice; Rn[:, m] = 0
     for (int c = 0; c < n; ++c)
         for (int r = 0; r < m; ++r) R[r + c * m] = (r <= c) ? R[r + (c + 1) * m] : 0.0;
     for (int r = 0; r < m; ++r) R[r + (m - 1) * m] = 0.0;
 }
 
-// defer_downdate: leave the QR downdate to the caller (flagged in A.pad0), which runs it
-// warp-parallel (aa_downdate_warp)
-// aa_downdate by one warp: lane 0 forms each 2-row reflector, the lanes update the
-// trailing columns and build Qx column by column; per element the arithmetic of
-// aa_downdate (a reflector with tau = v1 = 0 leaves the columns unchanged).  A lives in
-// shared memory; the reflectors go to A.h1 / A.coef, which the next slots overwrite.
+// aa_downdate by one warp: lane 0 forms each reflector, the lanes update the trailing
+// columns and build Qx column by column; per element the arithmetic of aa_downdate (a
+// reflector with tau = v1 = 0 leaves the columns unchanged).  A lives in shared memory.
 __device__ void aa_downdate_warp(AAState& A, int lane)
 {
     const int m = A.m, n = m - 1;
-    double* R = A.R;
-    double* tau = A.h1;
-    double* v1 = A.coef;
+    double* R = A.Rn;
+    for (int k = lane; k < m * m; k += 32) R[k] = A.R[k];
+    __syncwarp();
+    double* tau = A.tau;
+    double* v1 = A.v1;
     for (int j = 0; j < n; ++j) {
         if (lane == 0) {
             const double alpha = R[j + (j + 1) * m];
@@ -568,7 +607,7 @@ __device__ void aa_downdate_warp(AAState& A, int lane)
             Qx[j + 1 + c * m] = fma(-(tau[j] * v1[j]), w, Qx[j + 1 + c * m]);
         }
     }
-    // R[1:m-1, 1:m-1] = upper triangle of the slice; R[:, m] = 0 (read all, then write)
+    // Rn[1:m-1, 1:m-1] = upper triangle of the slice; Rn[:, m] = 0 (read all, then write)
     double v[8];
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
@@ -588,7 +627,7 @@ __device__ void aa_downdate_warp(AAState& A, int lane)
     __syncwarp();
 }
 
-__device__ void aa_after_eval(AAState& A, double r, int* done_counter, bool defer_downdate = false)
+__device__ void aa_after_eval(AAState& A, double r, int* done_counter)
 {
     A.resnorm = r;
     if (A.history && A.nevals < A.history_cap) A.history[A.nevals] = r;
@@ -649,16 +688,12 @@ __device__ void aa_after_eval(AAState& A, double r, int* done_counter, bool defe
         if (A.m > 1 && A.k > A.m) A.head = (A.head + 1) % A.m;   // BuildDG! shift
         const int kqr = A.k - 1;
         A.mk = min(A.m, A.k);
+        // the QR downdate of this step (kqr > m - 1) was applied to Q and R at the end of
+        // the previous step, as soon as that step's R column was known
         if (kqr == 0 || A.m == 1) {
             A.kq = 0;
-            A.downdate = 0;
             A.op[1] = OP_NORM_DF;
             return;
-        }
-        A.downdate = (kqr > A.m - 1) ? 1 : 0;
-        if (A.downdate) {
-            if (defer_downdate) A.pad0 = 1;
-            else aa_downdate(A);
         }
         A.kq = min(kqr, A.m - 1);
         A.op[1] = OP_DOT_H1;
@@ -673,10 +708,23 @@ __device__ void aa_after_eval(AAState& A, double r, int* done_counter, bool defe
 __device__ __forceinline__ int ctl_nsums(const AAState& A, int op)
 {
     switch (op) {
-    case -1: case OP_NORM_DF: case OP_SUB_NORM: return 1;
-    case OP_DOT_H1: case OP_SUB_DOT: return A.kq;
-    case OP_SETQ_DOT_TRES: return A.mk;
+    case -1: case OP_NORM_DF: return 1;
+    case OP_DOT_H1: return A.kq;
+    case OP_SUB_DOT_NORM: case OP_SETQ_DOT_TRES: return A.kq + 1;
     default: return 0;
+    }
+}
+
+// After this step's R column: when the next Anderson step starts with a full history
+// (its counter k + 1 > m), its QR downdate is formed now (Rn, Qx) so that the SETQ pass
+// can store the rotated Q.  defer: leave it to the caller (flag pad0), which runs it
+// warp-parallel (aa_downdate_warp).
+__device__ __forceinline__ void aa_plan_downdate(AAState& A, bool defer)
+{
+    A.downdate = (A.m > 1 && A.k >= A.m) ? 1 : 0;
+    if (A.downdate) {
+        if (defer) A.pad0 = 1;
+        else aa_downdate(A);
     }
 }
 
@@ -688,31 +736,33 @@ __device__ void ctl_apply(AAState& A, int op, int slot_done, const double* sums,
     const int next = slot_done + 1;
     switch (op) {
     case -1:
-        aa_after_eval(A, sqrt(sums[0]), done_counter, defer_downdate);
+        aa_after_eval(A, sqrt(sums[0]), done_counter);
         break;
     case OP_NORM_DF: {   // k == 0 branch of aa_qr_update!: R[1,1] = norm(df)
         const double r = sqrt(sums[0]);
         A.R[0] = r;
         A.rnorm = r;
         A.kq = 0;
+        aa_plan_downdate(A, defer_downdate);
         if (next <= N_VEC_SLOTS) A.op[next] = OP_SETQ_DOT_TRES;
         break;
     }
     case OP_DOT_H1:
         for (int k = 0; k < A.kq; ++k) { A.h1[k] = sums[k]; A.coef[k] = sums[k]; }
-        if (next <= N_VEC_SLOTS) A.op[next] = OP_SUB_DOT;
+        if (next <= N_VEC_SLOTS) A.op[next] = OP_SUB_DOT_NORM;
         break;
-    case OP_SUB_DOT:
+    case OP_SUB_DOT_NORM: {
+        // hv[1:k] = h1 + h2; hv[k+1] = norm(df2), ||df2||^2 = ||df1||^2 - ||h2||^2
+        double h2sq = 0.0;
         for (int k = 0; k < A.kq; ++k) {
-            A.R[k + A.kq * A.m] = A.h1[k] + sums[k];   // hv[1:k] = h1 + h2
+            A.R[k + A.kq * A.m] = A.h1[k] + sums[k];
             A.coef[k] = sums[k];
+            h2sq += sums[k] * sums[k];
         }
-        if (next <= N_VEC_SLOTS) A.op[next] = OP_SUB_NORM;
-        break;
-    case OP_SUB_NORM: {
-        const double r = sqrt(sums[0]);
+        const double r = sqrt(fmax(sums[A.kq] - h2sq, 0.0));
         A.R[A.kq + A.kq * A.m] = r;
         A.rnorm = r;
+        aa_plan_downdate(A, defer_downdate);
         if (next <= N_VEC_SLOTS) A.op[next] = OP_SETQ_DOT_TRES;
         break;
     }
@@ -726,6 +776,8 @@ __device__ void ctl_apply(AAState& A, int op, int slot_done, const double* sums,
             th[i] = v / A.R[i + i * m];
         }
         for (int i = 0; i < mk; ++i) A.coef[i] = th[i];
+        if (A.downdate)   // the next step starts from the downdated factor
+            for (int k = 0; k < m * m; ++k) A.R[k] = A.Rn[k];
         if (next <= N_VEC_SLOTS) A.op[next] = OP_SOL_AA;
         A.k++;
         A.mode = MODE_EVAL_AA;

@@ -17,6 +17,7 @@
 #define PERS_WARPS (PERS_THREADS / 32)
 #define PERS_R 8
 #define PERS_TILE (32 * PERS_R)
+#define PERS_MAX_M 8           // Anderson depth bound of the persistent engine (deeper: grid engine)
 
 // extended periodic window of one convolution input: ext[k] = in[(k - OFF) mod N]
 __host__ __device__ __forceinline__ int pers_extn(int N) { return 2 * N + 32 * (PERS_R + 2); }
@@ -31,14 +32,16 @@ __host__ __device__ __forceinline__ size_t pers_smem_bytes(int N, int nc, int nc
 }
 
 // byte offset of the shared-memory Anderson vectors, and their size for n_elem
-// elements and m history columns (rho, sol, gx, res, df, V_ext, Q, DG)
+// elements and m history columns (rho, sol, gx, res, df, V_ext, Q row-major, DG)
 __host__ __device__ __forceinline__ size_t pers_vec_offset(int N, int nc, int nconv, int NF, size_t esz)
 {
     return (pers_smem_bytes(N, nc, nconv, NF, esz) + 15) & ~(size_t)15;
 }
+// row stride of the shared-memory QR history: m rounded up to even (16-byte aligned rows)
+__host__ __device__ __forceinline__ int pers_qs(int m) { return m + (m & 1); }
 __host__ __device__ __forceinline__ size_t pers_vec_bytes(int n_elem, int m)
 {
-    return sizeof(double) * (size_t)n_elem * (6 + 2 * (size_t)m);
+    return sizeof(double) * (size_t)n_elem * (6 + (size_t)pers_qs(m) + (size_t)m);
 }
 
 // Sums of K per-thread values over the block into sums[0..K), for thread 0 only: the
@@ -214,10 +217,49 @@ __device__ __forceinline__ void pers_conv_any(const T* __restrict__ ext, bool sh
         pers_conv<T, NC>(ext, shared_input, taps, out, out_comp_stride, N, nconv, scale);
 }
 
+// The Anderson section of one fixed-point step (the QR downdate and the vector slots
+// between two evaluations) on one warp: each slot's partial sums are reduced by
+// shuffles and lane 0 applies the step, so the slots need no block barrier.  For the
+// small systems of a batch (a few hundred elements per system) the slots are bound by
+// those barriers and the serial control step, not by the element loops.
+__device__ __forceinline__ void pers_anderson_warp(const SysDev& S, AAState& A, double* sums, int* done_counter,
+                                                   int lane)
+{
+    for (int slot = 1; slot <= N_VEC_SLOTS; ++slot) {
+        const int op = A.op[slot];
+        if (op == OP_NONE) break;
+        double acc[RED_SLOTS];
+#pragma unroll
+        for (int k = 0; k < RED_SLOTS; ++k) acc[k] = 0.0;
+        const int K = vec_op_range<PERS_MAX_M>(op, S, A, lane, S.n_elem, 32, acc);
+        if (K > 0) {
+#pragma unroll
+            for (int c = 0; c < RED_SLOTS; ++c) {
+                if (c >= K) break;
+                double v = acc[c];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) sums[c] = v;
+            }
+            __syncwarp();
+            if (lane == 0) ctl_apply(A, op, slot, sums, done_counter, true);
+            __syncwarp();
+            if (A.pad0) {   // the next step's QR downdate, from this step's R
+                aa_downdate_warp(A, lane);
+                if (lane == 0) A.pad0 = 0;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// warp_aa_max_elem: a system of at most this many elements (N * nc) runs the Anderson
+// section on warp 0 (pers_anderson_warp), a larger one on the whole block.  The choice
+// depends on the system alone, so a system gets the same arithmetic alone or in a batch.
 template <typename T, int NC, int ND>
 __global__ void __launch_bounds__(PERS_THREADS, 1)
 persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int* done_counter, int max_evals,
-                  int vec_m)
+                  int vec_m, int warp_aa_max_elem)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ AAState sA;
@@ -260,11 +302,13 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
         sS.df = vs + 4 * (size_t)n_elem;
         if (G.vext) sS.vext = vs + 5 * (size_t)n_elem;
         sS.Q = vs + 6 * (size_t)n_elem;
-        sS.DG = vs + (6 + (size_t)vec_m) * n_elem;
+        sS.qs = pers_qs(vec_m);
+        sS.DG = vs + (6 + (size_t)pers_qs(vec_m)) * n_elem;
     }
     __syncthreads();
     const SysDev& S = sS;
     const T NA = T(S.NA);
+    const bool warp_aa = n_elem <= warp_aa_max_elem;
     for (int it = 0; it < max_evals; ++it) {
         if (sA.mode == MODE_DONE) break;
         // ---- weighted densities (evaluate_field!) ----
@@ -345,25 +389,30 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
             block_reduce_to_smem<PERS_THREADS>(ss, 1, sums, n_elem);
             if (tid == 0) ctl_apply(sA, -1, 0, sums, done_counter, true);
             __syncthreads();
-            if (sA.pad0) {   // the QR downdate of this Anderson step, on warp 0
-                if (tid < 32) aa_downdate_warp(sA, tid);
-                __syncthreads();
-                if (tid == 0) sA.pad0 = 0;
-            }
         }
         // ---- Anderson vector slots ----
+        if (warp_aa) {
+            if (tid < 32) pers_anderson_warp(S, sA, sums, done_counter, tid);
+            __syncthreads();
+            continue;
+        }
         for (int slot = 1; slot <= N_VEC_SLOTS; ++slot) {
             const int op = sA.op[slot];
             if (op == OP_NONE) break;
             double acc[RED_SLOTS];
 #pragma unroll
             for (int k = 0; k < RED_SLOTS; ++k) acc[k] = 0.0;
-            const int K = vec_op_range(op, S, sA, tid, n_elem, PERS_THREADS, acc);
+            const int K = vec_op_range<PERS_MAX_M>(op, S, sA, tid, n_elem, PERS_THREADS, acc);
             if (K > 0) {
                 block_reduce_to_smem<PERS_THREADS>(acc, K, sums, n_elem);
-                if (tid == 0) ctl_apply(sA, op, slot, sums, done_counter);
+                if (tid == 0) ctl_apply(sA, op, slot, sums, done_counter, true);
             }
             __syncthreads();
+            if (sA.pad0) {   // the next step's QR downdate, from this step's R, on warp 0
+                if (tid < 32) aa_downdate_warp(sA, tid);
+                __syncthreads();
+                if (tid == 0) sA.pad0 = 0;
+            }
         }
     }
     if (vec_m >= 0) {

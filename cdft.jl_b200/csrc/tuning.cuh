@@ -1,0 +1,38 @@
+// Launch shapes chosen by the project's autotuner (cdft.jl_b200/tune.py).
+//
+// Every entry changes how work is mapped onto the B200, never which arithmetic a
+// system sees for a given problem: entries that could move a reduction order are
+// per-system rules (a threshold on the system's own size), so a system converged
+// alone or inside a batch still gets bit-identical results.  The defaults are the
+// values the sweep measured on B200; cdft_tuning_set overrides one for the process
+// (the sweep itself uses it).
+#pragma once
+#include <cstring>
+
+struct TunedShapes {
+    // persistent engine: a system of at most this many elements (N * nc) runs the Anderson
+    // vector slots on one warp (no block barriers); larger systems use the whole block.
+    // Measured on the 64-point isotherm (N = 100..400, m = 5): the whole block is faster at
+    // every size (Anderson section 5.6 vs 10.7 us per evaluation on average), so 0.
+    int pers_warp_aa_max_elem = 0;
+};
+
+static TunedShapes g_tuned;
+
+struct TunedEntry {
+    const char* name;
+    int TunedShapes::*field;
+    int lo, hi;
+};
+
+static const TunedEntry kTunedEntries[] = {
+    {"pers_warp_aa_max_elem", &TunedShapes::pers_warp_aa_max_elem, 0, 1 << 30},
+};
+
+inline const TunedEntry* tuned_entry(const char* name)
+{
+    if (!name) return nullptr;
+    for (const TunedEntry& e : kTunedEntries)
+        if (std::strcmp(e.name, name) == 0) return &e;
+    return nullptr;
+}

@@ -231,6 +231,14 @@ int cdft_batch_time_stage(cdft_plan* const* plans, int nplans, int stage, int re
 int cdft_functional_derivative_noalloc(const cdft_system_desc* desc, const double* d_rho, double* d_dFdrho,
                                        void* stream);
 
+/* Launch shapes of the autotuner (cdft.jl_b200/tune.py), process-wide, by name: e.g.
+ * "pers_warp_aa_max_elem" (persistent engine: systems of at most this many elements run
+ * the Anderson vector slots on one warp).  The defaults are the tuned values; _set
+ * overrides one (CDFT_E_INVALID for an unknown name or a value out of range).  No
+ * counterpart in the reference (KernelAbstractions picks its own launch shapes). */
+int cdft_tuning_get(const char* name, int* value);
+int cdft_tuning_set(const char* name, int value);
+
 /* Number of our kernel launches issued by the calling thread since the last
  * reset (instrumentation for benchmarks). */
 long long cdft_launch_count(int reset);

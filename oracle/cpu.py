@@ -83,6 +83,8 @@ def load():
         lib.cdft_cpu_batch_converge.argtypes = [ctypes.POINTER(SystemDesc), ctypes.c_int, ctypes.c_void_p,
                                                 ctypes.POINTER(SolverOpts), ctypes.POINTER(Result), ctypes.c_int]
         lib.cdft_cpu_max_threads.restype = ctypes.c_int
+        lib.cdft_cpu_set_wb_closed.argtypes = [ctypes.c_int]
+        lib.cdft_cpu_set_wb_closed.restype = None
         _LIB = lib
     return _LIB
 
@@ -161,6 +163,12 @@ def batch_converge(systems, rhos, nthreads=0, history_cap=0, **solver):
     if rc:
         raise RuntimeError(f"cdft_cpu_batch_converge: {rc}")
     return [res[k] for k in range(n)], hist
+
+
+def set_wb_closed(closed):
+    """Evaluate the reference's closed White-Bear bracket everywhere (True) or the series
+    form near n3 = 0 (False, the default)."""
+    load().cdft_cpu_set_wb_closed(1 if closed else 0)
 
 
 def max_threads():

@@ -206,13 +206,17 @@ struct Params {
     double aK;                                // (sigma_ij/L)^3 (exp(eps_AB/T) - 1) kappa_AB
 };
 
+// true: the reference's closed White-Bear bracket everywhere (FMT.jl:39-45), including
+// |n3| < 0.05 where the series form replaces it by default
+bool g_wb_closed = false;
+
 template <typename T>
 T wb_bracket(const T& n3, const T& dn, const T& log1dn)
 {
     // B(n3) = ln(1-n3)/(12 pi n3^2) + 1/(12 pi n3 (1-n3)^2) (FMT.jl:42-43); for |n3| < 0.05 its
     // Taylor series 12 pi B = sum_j (j+1)(j+3)/(j+2) n3^j (16 terms), where the closed form
     // cancels (the oracle's and the library's form)
-    if (std::fabs(val(n3)) < 0.05) {
+    if (!g_wb_closed && std::fabs(val(n3)) < 0.05) {
         T s = n3 * 0.0 + (16.0 * 18.0 / 17.0);
         for (int j = 14; j >= 0; --j) s = s * n3 + ((j + 1.0) * (j + 3.0) / (j + 2.0));
         return s / (12.0 * PI);
@@ -747,5 +751,8 @@ int cdft_cpu_batch_converge(const cdft_system_desc* descs, int n, double* const*
 }
 
 int cdft_cpu_max_threads(void) { return omp_get_max_threads(); }
+
+// 1: evaluate the reference's closed White-Bear bracket everywhere; 0: the series near n3 = 0
+void cdft_cpu_set_wb_closed(int closed) { g_wb_closed = closed != 0; }
 
 }  // extern "C"
