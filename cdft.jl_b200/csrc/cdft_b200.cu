@@ -1795,6 +1795,13 @@ extern "C" int cdft_functional_derivative_noalloc(const cdft_system_desc* desc, 
                          "system too large for the allocation-free scratch: N=%d nc=%d (limits N<=%d, N*nc<=%d)",
                          N, nc, CDFT_NOALLOC_MAX_N, CDFT_NOALLOC_MAX_ELEM);
     cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    if (stream) {   // the stream must belong to the current device, where the scratch address is looked up
+        int dev = 0, sdev = 0;
+        CU(cudaGetDevice(&dev));
+        CU(cudaStreamGetDevice(stream, &sdev));
+        if (sdev != dev)
+            return set_error(CDFT_E_INVALID, "stream belongs to device %d, the current device is %d", sdev, dev);
+    }
     rc = upload_constants();
     if (rc) return rc;
     double* base = nullptr;

@@ -213,7 +213,9 @@ int cdft_batch_time_stage(cdft_plan* const* plans, int nplans, int stage, int re
  * system comes as a descriptor, d_rho and d_dFdrho are caller-owned device
  * arrays of N*nc doubles, desc->vext is a host array or NULL, stream is a
  * cudaStream_t or NULL for the default stream; the call returns after the
- * stream has finished its work.
+ * stream has finished its work.  The call runs on the calling thread's current
+ * CUDA device; the arrays and the stream must belong to that device (a stream
+ * of another device is rejected with CDFT_E_INVALID).
  *
  * Scratch (kernel tables, weighted densities, partial sums) lives in one
  * fixed array of CDFT_NOALLOC_SCRATCH_BYTES inside the library, which every
@@ -221,7 +223,10 @@ int cdft_batch_time_stage(cdft_plan* const* plans, int nplans, int stage, int re
  * Cartesian, FP64, N <= CDFT_NOALLOC_MAX_N and N*nc <= CDFT_NOALLOC_MAX_ELEM;
  * larger systems are rejected with CDFT_E_UNSUPPORTED.  The first call on a
  * device looks up the array's device address (once per device); make that
- * first call before any stream capture.  All calls share the one array, so
+ * first call before any stream capture.  That address is kept for the life of
+ * the process: do not call this entry point again after cudaDeviceReset on that
+ * device (the reset ends the context the address belongs to; plans are likewise
+ * invalid after a reset).  All calls share the one array, so
  * calls that overlap on the GPU (from two host threads or two streams) race
  * and must be serialised by the caller.  Every value a call reads from the
  * array is written earlier in the same call, so no clearing is needed. */

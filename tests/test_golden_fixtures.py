@@ -71,10 +71,22 @@ def test_c3_fixture_covers_the_isotherm():
         assert so.adsorption(rho)[0] == pytest.approx(float(f["adsorption"][k]), rel=1e-13)
 
 
-def test_c4_c5_fixtures_present():
+def test_c4_fixture_is_a_converged_interface():
+    """c4 comes from the oracle's C++ restatement (the NumPy run takes hours at 4096 points):
+    its stored profile must be a fixed point of the NumPy oracle's map as well."""
+    from oracle import functional as fn
     f = _load("c4_water_octane_lle_4096")
     assert int(f["errcode"]) == 0 and int(f["N"]) == 4096 and f["rho"].shape == (2, 4096)
     assert float(f["gamma"]) > 0
+    om = mf.oracle_model(["water", "octane"])
+    st = fn.Structure((float(f["p"]), float(f["T"])), list(f["rho_bulk"]), [tuple(f["bounds"])], (int(f["N"]),),
+                      kind="twophase", rho_bulk2=list(f["rho_bulk2"]))
+    so = fn.DFTSystem(om, st)
+    assert _fixed_point_residual(so, f["rho"], 0.01) < 1e-12
+    assert so.surface_tension(f["rho"]) / 2 == pytest.approx(float(f["gamma"]), rel=1e-12)
+
+
+def test_c5_fixture_present():
     g = _load("c5_solutes_128")
     assert int(g["errcode"]) == 0 and int(g["N"]) == 128 and g["rho_sub"].shape == (1, 32, 32, 32)
     assert g["centres"].shape == (27, 3)

@@ -84,3 +84,30 @@ def test_radial_runs_on_the_grid_engine():
     with pytest.raises(CDFTError):
         cd.converge(sp, rho, beta=0.05, tol=1e-8, engine="persistent")
     assert cd.converge(sp, rho, beta=0.05, tol=1e-8, engine="auto").errcode == 0
+
+
+@pytest.mark.parametrize("coord,lb_L", [("sphr", 0.0), ("cyl", 2.0)])
+def test_converge_radial_steele_wall(coord, lb_L):
+    """A curved Steele wall (steele.jl:111-143): methane inside a spherical graphite pore
+    (lb = 0, wall at ub) and around a graphite rod (lb > 0), converged on the grid engine
+    with the clamped V_ext of the package; the oracle's RadialDFTSystem, given the Steele
+    wall itself, reaches the same fixed point."""
+    import cdft_b200 as cd
+    from oracle import functional as fn, pcsaft_bulk as pb
+    from oracle import radial as rd
+    pm, om = S.models(["methane"])
+    rb = [pb.density(om, P_M, T_M, [1.0])]
+    L = om.length_scale()
+    lb, ub, N = lb_L * L, 10.0 * L, 121
+    make = cd.Uniform1DSphr if coord == "sphr" else cd.Uniform1DCyl
+    sp = cd.DFTSystem(pm, make((P_M, T_M), rb, [lb, ub], N), cd.Steele(["graphite"]))
+    so = rd.RadialDFTSystem(om, rd.RadialStructure((P_M, T_M), rb, ub, N, coord, lb=lb),
+                            walls=[fn.SteeleWall.graphite()])
+    np.testing.assert_allclose(sp.vext, so.vext, rtol=1e-12)
+    rho = cd.initialize_profiles(sp)
+    r0 = rho.copy()
+    kw = dict(beta=0.1, tol=1e-12, anderson_m=5, maxit=5000)
+    res = cd.converge(sp, rho, engine="grid", **kw)
+    ro, out = so.converge(r0, **kw)
+    assert res.errcode == 0 and out.errcode == 0, (res, out.errcode)
+    assert float(np.max(np.abs(rho / ro - 1))) < 1e-8

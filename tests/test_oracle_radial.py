@@ -80,3 +80,38 @@ def test_radial_steele_wall(coord, lb_L):
     assert np.ptp(V[0, clamped]) == 0.0          # one value over the clamped points
     far = np.argmax(zw)                           # the point farthest from the wall
     assert abs(V[0, far]) < abs(V[0, clamped][0])
+
+
+@pytest.mark.parametrize("coord", ["sphr", "cyl"])
+@pytest.mark.parametrize("lb_L", [0.0, 2.0])
+def test_radial_steele_equals_planar_wall_at_wall_distance(coord, lb_L):
+    """Independent of both restatements: on a radial grid the Steele potential is the
+    planar single-wall 10-4-3 value (steele.jl:49-81, graphite: sigma_s 3.40 A, eps_s 28 K,
+    rho_s 0.114 A^-3, Delta 3.35 A; Lorentz-Berthelot fluid-solid pair) evaluated at the
+    wall distance r - lb (solid core, lb > 0) or ub - r (pore, lb = 0), with the distance
+    clamped below at half the smallest fluid sigma (steele.jl:125-126)."""
+    import cdft_b200 as cd
+    pm, om = S.models(["methane"])
+    T, p = 150.0, 1e7
+    rb = pb.density(om, p, T, [1.0])
+    L = om.length_scale()
+    lb, ub, N = lb_L * L, 10 * L, 151
+    make = cd.Uniform1DSphr if coord == "sphr" else cd.Uniform1DCyl
+    st = make((p, T), [rb], [lb, ub], N)
+    r = st.coords(0)
+    V = cd.Steele(["graphite"]).potential_radial(pm, r, T, *st.bounds[0])
+
+    sig_s, eps_s, rho_s, delta = 3.40e-10, 28.0, 0.114e30, 3.35e-10
+    sig_f, eps_f = 3.7039e-10, 150.03
+    s, e = 0.5 * (sig_s + sig_f), np.sqrt(eps_s * eps_f)
+
+    def planar(z):
+        return (2 * np.pi * rho_s * e * delta * s * s
+                * (0.4 * (s / z) ** 10 - (s / z) ** 4 - s ** 4 / (3 * delta * (z + 0.61 * delta) ** 3)) / T)
+
+    zw = (r - lb) if lb > 0 else (ub - r)
+    zc = np.maximum(zw, 0.5 * sig_f)
+    np.testing.assert_allclose(V[0], planar(zc), rtol=1e-12)
+    clamped = zw <= 0.5 * sig_f
+    assert clamped.any()
+    np.testing.assert_allclose(V[0, clamped], planar(0.5 * sig_f), rtol=1e-12)

@@ -40,19 +40,23 @@ def test_noalloc_matches_plan_path_twice():
     import cdft_b200 as cd
     from cdft_b200 import _lib
     rng = np.random.default_rng(7)
-    # two different systems: the second call must not depend on what the first left in the scratch
-    cases = [S.water_octane_lle(N=256)[0], S.methane_wall(N=201)[0]]
-    rhos = [S.random_smooth_profile(cases[0], rng), cd.initialize_profiles(cases[1])]
+    # different systems: a call must not depend on what the one before left in the scratch.
+    # The third (4096 points, two components) is the largest the scratch takes: its
+    # convolutions are split over 4 tap chunks whose partial sums meet in the scratch.
+    cases = [S.water_octane_lle(N=256)[0], S.methane_wall(N=201)[0], S.water_octane_lle(N=4096)[0]]
+    rhos = [S.random_smooth_profile(cases[0], rng), cd.initialize_profiles(cases[1]),
+            S.random_smooth_profile(cases[2], rng)]
     rho_dev = [torch.from_numpy(np.ascontiguousarray(r)).cuda() for r in rhos]
     expect = [_reference_path(sp, r) for sp, r in zip(cases, rho_dev)]
     out_dev = [torch.full_like(r, float("nan")) for r in rho_dev]
     torch.cuda.synchronize()
-    # two calls in a row
+    # calls in a row
     _lib.check(_noalloc(cases[0], rho_dev[0], out_dev[0]))
     free_before = torch.cuda.mem_get_info()[0]
     _lib.check(_noalloc(cases[1], rho_dev[1], out_dev[1]))
+    _lib.check(_noalloc(cases[2], rho_dev[2], out_dev[2]))
     torch.cuda.synchronize()
-    assert torch.cuda.mem_get_info()[0] == free_before   # the second call allocated nothing
+    assert torch.cuda.mem_get_info()[0] == free_before   # the later calls allocated nothing
     for sp, e, o in zip(cases, expect, out_dev):
         got = o.cpu().numpy()
         for i in range(sp.nc):
