@@ -10,9 +10,12 @@ profiles.  Metric: state points per second (whole job, all ranks).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
     python bench.py --impl reference ...   # the reference's algorithm compiled for the host cores
 
-Multi-GPU (torchrun): every rank converges its own 64-point isotherm (weak
-scaling, no collective on the data path); the timed region is bracketed by a
-barrier and the device time is the max over ranks.
+Multi-GPU (torchrun): the job is one 64-point isotherm per rank (pressures shifted by
+0.1 % per isotherm; weak scaling), its state points split across ranks by longest
+processing time first on their estimated cost (cdft_b200.shard); every rank converges
+its share as one batch with no collective on the data path, the timed region is
+bracketed by a barrier, the device time is the max over ranks, and rank 0 gathers
+(adsorption, Omega_ex, status, rho) of every state point afterwards.
 """
 import argparse
 import json
@@ -44,6 +47,11 @@ def isotherm_specs(rank=0):
         for p in PRESSURES:
             out.append((float(H), float(p) * (1 + 1e-3 * rank), N_OF_WIDTH[k]))
     return out
+
+
+def job_specs(world):
+    """All state points of a job on `world` ranks: one isotherm per rank."""
+    return [s for r in range(world) for s in isotherm_specs(r)]
 
 
 def max_over_ranks(value, dist, device):
@@ -168,8 +176,12 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from cdft_b200 import shard
     lib = _lib.load()
-    specs = isotherm_specs(rank)
+    all_specs = job_specs(world)
+    parts = shard.lpt_partition([shard.estimated_cost(N) for _, _, N in all_specs], world)
+    mine = parts[rank]
+    specs = [all_specs[i] for i in mine]
     stream = torch.cuda.Stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # > 126 MB L2
     method = cd.AASol.for_system(None, **SOLVER)
@@ -261,7 +273,11 @@ def run_ours(args, rank, world, local_rank):
         t_set.append(time.perf_counter() - t0)
     ms_setup = 1e3 * float(np.mean(t_set))
 
-    accuracy = accuracy_vs_oracle(systems, run["rho"]) if rank == 0 else None
+    # host gather of every state point's results to rank 0 (outside the timed region)
+    records = [(float(cd.adsorption(sy, r)[0]), float(cd.surface_tension(sy, r)), int(e), r)
+               for sy, r, e in zip(systems, run["rho"], errc)]
+    gathered = shard.gather_results(dist, rank, world, mine, records, len(all_specs))
+    accuracy = accuracy_vs_oracle(systems, run["rho"]) if world == 1 else None
     mixed = None
     if rank == 0 and args.precision == "fp64" and args.mixed:
         mr = device_isotherm("mixed", max(2, args.steps // 4), 2)
@@ -286,8 +302,8 @@ def run_ours(args, rank, world, local_rank):
     step_flops = sum(2.0 * 2.0 * s.nc * 6 * s.ngrid[0] ** 2 * ev for s, ev in zip(systems, iters))
     achieved = step_flops / (ms_dev * 1e-3) / 1e12
     plain = plain_fp64_gpu(specs) if (rank == 0 and args.plain) else None
-    total_units = n * world
-    value = whole_job_rate(n, world, ms_dev)
+    total_units = len(all_specs)
+    value = total_units / (ms_dev * 1e-3)
     h2d = sum(r.nbytes for r in rho0)
     line = None
     if rank == 0:
@@ -306,7 +322,12 @@ def run_ours(args, rank, world, local_rank):
             "data": "synthetic: seeded isotherm state points, PC-SAFT methane parameters",
             "config": {
                 "workload": "isotherm64: methane 150 K, graphite slit pores 2-8 nm x 1e3-1e7 Pa, N=100..400",
-                "systems_per_gpu": n, "grid_points": sum(s.ngrid[0] for s in systems),
+                "state_points": total_units, "systems_per_gpu": n, "grid_points": sum(s.ngrid[0] for s in systems),
+                "sharding": {"ranks": world, "partition": "LPT on N^2 per state point",
+                             "balance_max_over_mean": round(shard.balance(
+                                 parts, [shard.estimated_cost(N) for _, _, N in all_specs]), 4),
+                             "gathered_state_points": len(gathered),
+                             "gathered_errcodes": sorted(set(g[2] for g in gathered))},
                 "solver": SOLVER, "precision": args.precision, "engine": args.engine,
                 "l2": "flushed between steps (256 MB write, untimed)",
                 "evaluations_per_system": {"min": min(iters), "max": max(iters), "mean": float(np.mean(iters))},

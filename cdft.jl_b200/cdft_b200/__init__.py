@@ -245,13 +245,17 @@ def TwoPhase1DCart(conditions, rho_bulk, rho_bulk2, bounds, ngrid):
 
 class DFTOptions:
     """src/base/devices.jl:29-40: ``precision`` is "fp64" (Float64) or "mixed"
-    (FP32 convolutions and Phi, FP64 solver and integrals)."""
+    (FP32 convolutions and Phi, FP64 solver and integrals, an FP64 polish).  The
+    reference's Float32 runs everything in FP32; the library has no FP32 solver, so
+    float32 is refused rather than mapped onto "mixed"."""
 
     def __init__(self, precision="fp64"):
         if precision in ("fp64", np.float64, float):
             self.precision = PREC_FP64
-        elif precision in ("mixed", np.float32):
+        elif precision == "mixed":
             self.precision = PREC_MIXED
+        elif precision in ("fp32", np.float32):
+            raise ValueError('precision float32 (all-FP32) is not offered: use "fp64" or "mixed"')
         else:
             raise ValueError(f"unknown precision {precision!r}")
 
@@ -433,12 +437,19 @@ def _check_rho(system, rho):
 
 
 def converge(system, rho, method=None, time_budget_s=0.0, iters_per_launch=0, keep_history=True, engine="auto",
-             mixed_switch_rtol=0.0, **kwargs):
+             mixed_switch_rtol=0.0, log_interval=0, save_interval=0, save_callback=None, **kwargs):
     """converge!(system, ρ; kwargs...) / converge!(system, ρ, solver): converges
     ``rho`` in place (converge.jl:214-254) and returns the aasol status.
-    ``engine``: "auto", "grid" (per-stage kernels) or "persistent" (one CTA per system)."""
+    ``engine``: "auto", "grid" (per-stage kernels) or "persistent" (one CTA per system).
+    ``save_interval`` / ``save_callback(it, rho)`` and ``log_interval`` are DFTProblem's
+    hooks (converge.jl:31-60,256-267): the profile after every ``save_interval``
+    evaluations goes to the callback, and the free energy of every ``log_interval``-th
+    profile is logged (computed once converge returns: the callback runs while the plan is
+    busy)."""
     _check_rho(system, rho)
     method = method or AASol.for_system(system, **kwargs)
+    if save_interval > 0 and save_callback is None:
+        raise ValueError("save_interval > 0 needs a save_callback")
     res = _lib.Result()
     hist = None
     if keep_history:
@@ -447,7 +458,24 @@ def converge(system, rho, method=None, time_budget_s=0.0, iters_per_launch=0, ke
         res.history = _lib.dptr(hist)
         res.history_cap = cap
     opts = method.c_opts(time_budget_s, iters_per_launch, engine, mixed_switch_rtol)
+    every = int(np.gcd(log_interval, save_interval)) if (log_interval and save_interval) else (log_interval or save_interval)
+    logged = []
+    if every > 0:
+        shape = rho.shape
+
+        def on_snapshot(user, s, it, ptr):
+            prof = np.ctypeslib.as_array(ptr, shape=(rho.size,)).reshape(shape).copy()
+            if save_interval and it % save_interval == 0:
+                save_callback(it, prof)
+            if log_interval and it % log_interval == 0:
+                logged.append((it, prof))
+
+        cb = _lib.SNAPSHOT_FN(on_snapshot)
+        opts.snapshot_every = every
+        opts.snapshot = ctypes.cast(cb, ctypes.c_void_p)
     _lib.check(_LIB.cdft_converge(system._plan, _lib.dptr(rho), ctypes.byref(opts), ctypes.byref(res)))
+    for it, prof in logged:
+        print(f"DFT iter {it:5d} | F = {free_energy(system, prof):.6g}")
     out = ConvergeResult(res, None if hist is None else hist[: res.history_len].copy())
     if method.verbose:
         msg = "DFT converged" if out.idid else "DFT did not converge"

@@ -82,7 +82,14 @@ class SolverOpts(ctypes.Structure):
         ("iters_per_launch", ctypes.c_int),
         ("engine", ctypes.c_int),
         ("mixed_switch_rtol", ctypes.c_double),
+        ("snapshot_every", ctypes.c_int),
+        ("snapshot", ctypes.c_void_p),
+        ("snapshot_user", ctypes.c_void_p),
     ]
+
+
+# void (*)(void* user, int system, int evaluations, const double* rho)
+SNAPSHOT_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double))
 
 
 class Result(ctypes.Structure):

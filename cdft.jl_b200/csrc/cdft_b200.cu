@@ -18,6 +18,7 @@
 
 #include "persistent.cuh"
 #include "fft3d.cuh"
+#include "fft3d_tma.cuh"
 #include "tuning.cuh"
 
 namespace {
@@ -94,6 +95,8 @@ struct cdft_plan {
     void* d_R = nullptr;          // 3D: spectrum of rho / accumulated adjoint spectrum
     void* d_adj = nullptr;        // 3D: adjoint sum in real space
     double* d_ktab = nullptr;     // 3D: kernel tables by |k|^2
+    CUtensorMap tmaps[2][2][2];   // 3D: [FP32][R, spec][y box, z box] tensor maps of the spectra
+    int tma_ready = 0;
     int L3 = 0, k2max = 0;        // 3D: points per dimension, max |k|^2 index
     double w0 = 0.0;              // 3D: reduced frequency per index
     Batch* self = nullptr;        // batch of this plan alone
@@ -540,6 +543,58 @@ double kernel_hat(int type, double wb, double R)
     return 4.0 * PI / (wb * wb * wb) * (std::sin(wb * R) - R * wb * std::cos(wb * R)) / (TWO_PI * TWO_PI * TWO_PI);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int get_encode_tiled(EncodeTiledFn* out)
+{
+    static std::mutex mu;
+    static EncodeTiledFn fn = nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        CU(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !p)
+            return set_error(CDFT_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+        fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    *out = fn;
+    return 0;
+}
+
+// Tensor map of `nfields` half spectra of L^3 points in precision fp32/fp64 at `base`:
+// a 4D tensor {2 KX, L, L, nfields} of reals with rows of 2 KXP reals (KXP = L/2 + 2, so every
+// stride is a multiple of 16 bytes), box {2 lines, L, 1, 1} (axis 1, y) or {2 lines, 1, L, 1}.
+int make_spectrum_map(CUtensorMap* m, bool fp32, void* base, int L, int lines, int nfields, int axis)
+{
+    EncodeTiledFn enc = nullptr;
+    int rc = get_encode_tiled(&enc);
+    if (rc) return rc;
+    const size_t es = fp32 ? sizeof(float) : sizeof(double);
+    const int KX = L / 2 + 1, KXP = L / 2 + 2;
+    const cuuint64_t dims[4] = {(cuuint64_t)(2 * KX), (cuuint64_t)L, (cuuint64_t)L, (cuuint64_t)nfields};
+    const cuuint64_t strides[3] = {(cuuint64_t)(2 * KXP * es), (cuuint64_t)(2 * KXP * es) * L,
+                                   (cuuint64_t)(2 * KXP * es) * L * L};
+    const cuuint32_t box[4] = {(cuuint32_t)(2 * lines), (cuuint32_t)(axis == 1 ? L : 1), (cuuint32_t)(axis == 1 ? 1 : L), 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    if (((uintptr_t)base & 15) || (strides[0] & 15) || ((2 * lines * es) & 15))
+        return set_error(CDFT_E_INVALID, "spectrum tensor map: 16-byte alignment violated");
+    const CUresult r = enc(m, fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims,
+                           strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(CDFT_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return 0;
+}
+
+// lines per tile of the transforms of L points in each precision (FftLines of fft3d.cuh)
+int fft_lines_of(bool fp32, int L)
+{
+    return fp32 ? ((L * 4 <= 512) ? 16 : 8) : ((L * 8 <= 512) ? 16 : 8);
+}
+
 // 3D periodic cubic box: FFT weighted densities (fft3d.cuh)
 int plan_build3d(cdft_plan* p)
 {
@@ -548,7 +603,7 @@ int plan_build3d(cdft_plan* p)
     memset(&S, 0, sizeof(S));
     const int L3 = d.ngrid[0], nc = d.nc;
     const size_t npts = (size_t)L3 * L3 * L3;
-    const size_t nspec = (size_t)(L3 / 2 + 1) * L3 * L3;
+    const size_t nspec = (size_t)(L3 / 2 + 2) * L3 * L3;   // rows padded to KXP = L/2 + 2
     p->N = (int)npts;
     p->L3 = L3;
     S.nd = 3;
@@ -593,6 +648,15 @@ int plan_build3d(cdft_plan* p)
         }
     CU(cudaMalloc(&p->d_ktab, tab.size() * sizeof(double)));
     CU(cudaMemcpyAsync(p->d_ktab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    // tensor maps of the spectra for the TMA y/z passes, both precisions (mixed plans run both)
+    for (int f32 = 0; f32 < 2; ++f32)
+        for (int axis = 1; axis <= 2; ++axis) {
+            const int lines = fft_lines_of(f32 != 0, L3);
+            int rc = make_spectrum_map(&p->tmaps[f32][0][axis - 1], f32 != 0, p->d_R, L3, lines, nc, axis);
+            if (!rc) rc = make_spectrum_map(&p->tmaps[f32][1][axis - 1], f32 != 0, p->d_spec, L3, lines, nc * S.nconv, axis);
+            if (rc) return rc;
+        }
+    p->tma_ready = 1;
     S.rho = p->d_vec;
     S.sol = p->d_vec + ne;
     S.gx = p->d_vec + 2 * ne;
@@ -687,8 +751,8 @@ int batch_build(const std::vector<cdft_plan*>& plans, Batch** out)
     BCU(cudaMalloc(&b->d_pchunks, sizeof(Chunk) * pch.size()));
     BCU(cudaMalloc(&b->d_echunks, sizeof(Chunk) * ech.size()));
     BCU(cudaMalloc(&b->d_partials, sizeof(double) * RED_SLOTS * ech.size()));
-    BCU(cudaMalloc(&b->d_done, sizeof(int)));
-    BCU(cudaMallocHost(&b->h_done, sizeof(int)));
+    BCU(cudaMalloc(&b->d_done, 2 * sizeof(int)));        // [0] finished systems, [1] kernel error word
+    BCU(cudaMallocHost(&b->h_done, 2 * sizeof(int)));
     if (!tasks.empty())
         BCU(cudaMemcpy(b->d_tasks, tasks.data(), sizeof(ConvTask) * tasks.size(), cudaMemcpyHostToDevice));
     BCU(cudaMemcpy(b->d_pchunks, pch.data(), sizeof(Chunk) * pch.size(), cudaMemcpyHostToDevice));
@@ -734,6 +798,49 @@ int fft_attr(K kern, size_t smem)
     return 0;
 }
 
+// Grid of a persistent tile kernel: as many blocks as are resident at once (occupancy x SMs),
+// at most one per tile.  Cached per (kernel, device).
+int persistent_grid(const void* kern, int threads, size_t smem, int ntiles, int* grid)
+{
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> cache;
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    int per = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find({kern, dev});
+        if (it != cache.end()) per = it->second;
+    }
+    if (!per) {
+        int occ = 0, nsm = 0;
+        CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem));
+        CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        per = std::max(occ, 1) * nsm;
+        std::lock_guard<std::mutex> lk(mu);
+        cache[{kern, dev}] = per;
+    }
+    *grid = std::min(ntiles, per);
+    return 0;
+}
+
+// the fused inverse x pass + Phi + forward x pass (fft_x_phi_fused) for nc components
+template <typename T, int L, int NC>
+int launch_fused_nc(Batch* b, const AAState* st, typename V2<T>::t* spec, size_t nspec, int* err)
+{
+    constexpr int LF = FusedLines<T, L, NC>::value;
+    constexpr size_t smem = fused_smem_bytes<T, L, NC, LF>();
+    static_assert(smem <= FUSED_SMEM_MAX, "fused x pass does not fit one block");
+    const SysDev& S = b->plans[0]->sys;
+    const size_t npts = (size_t)L * L * L;
+    CU(cudaFuncSetAttribute(fft_x_phi_fused<T, L, NC, LF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    fft_x_phi_fused<T, L, NC, LF><<<L * L / (2 * LF), FUSED_THREADS, smem, b->stream>>>(
+        spec, nspec, b->d_sys, T(S.NA / (double)npts), st, err);
+    g_launches += 1;
+    return 0;
+}
+
 // weighted densities, Phi and (with_int) the adjoint of a 3D system by FFT
 template <typename T, int L>
 int launch_eval3d_L(Batch* b, const AAState* st, bool with_int)
@@ -744,7 +851,7 @@ int launch_eval3d_L(Batch* b, const AAState* st, bool with_int)
     const SysDev& S = p->sys;
     const int nc = S.nc;
     const int KX = L / 2 + 1;
-    const size_t npts = (size_t)L * L * L, nspec = (size_t)KX * L * L;
+    const size_t npts = (size_t)L * L * L, nspec = (size_t)Spec3<L>::KXP * L * L;
     const int ntile = (KX + LINES - 1) / LINES;
     const int xblocks = L * L / (2 * LINES);
     const size_t smem2 = (size_t)(2 * L * (LINES + 1) + L / 2) * sizeof(C);
@@ -765,25 +872,74 @@ int launch_eval3d_L(Batch* b, const AAState* st, bool with_int)
     K.w0 = p->w0;
     K.nconv = S.nconv;
     cudaStream_t str = b->stream;
+    // the strided y and z passes: TMA tile kernels (fft3d_tma.cuh) or the per-thread-load kernels
+    const bool tma = g_tuned.fft3d_tma && p->tma_ready;
+    const int f32 = (sizeof(T) == 4) ? 1 : 0;
+    int* err = b->d_done + 1;
+    const size_t sm_yz = fft_tma_smem_yz<T, L, LINES>(), sm_ze = fft_tma_smem_zeval<T, L, LINES>(),
+                 sm_za = fft_tma_smem_zadj<T, L, LINES>();
+    const int tiles1 = L * ntile;   // tiles of one field in a y or z pass
+    auto yz_pass = [&](int buf, int nfields, int axis, int inverse) -> int {
+        if (!tma) {
+            C* d = buf ? spec : R;
+            fft_yz<T, L, LINES><<<dim3(L * ntile, nfields), FFT_THREADS, smem2, str>>>(d, nspec, axis, inverse, st);
+            return 0;
+        }
+        int grid = 0;
+        int r = persistent_grid((const void*)fft_yz_tma<T, L, LINES>, FFT_TMA_THREADS, sm_yz, tiles1 * nfields, &grid);
+        if (r) return r;
+        fft_yz_tma<T, L, LINES><<<grid, FFT_TMA_THREADS, sm_yz, str>>>(p->tmaps[f32][buf][axis - 1], axis, inverse,
+                                                                      nfields, st, err);
+        return 0;
+    };
     fft_x_r2c<T, double, L, LINES><<<dim3(xblocks, nc), FFT_THREADS, smem2, str>>>(S.rho, npts, R, nspec, st);
-    fft_yz<T, L, LINES><<<dim3(L * ntile, nc), FFT_THREADS, smem2, str>>>(R, nspec, 1, 0, st);
-    fft_z_eval<T, L, LINES><<<dim3(L * ntile, nc), FFT_THREADS, smem3, str>>>(R, nspec, spec, nspec, K, st);
-    fft_yz<T, L, LINES><<<dim3(L * ntile, nc * S.nconv), FFT_THREADS, smem2, str>>>(spec, nspec, 1, 1, st);
-    fft_x_c2r<T, L, LINES><<<dim3(xblocks, nc * S.nconv), FFT_THREADS, smem2, str>>>(spec, nspec, part, npts,
-                                                                                    T(S.NA / (double)npts), st);
-    rc = launch_phi<T>(b, st);
-    if (rc) return rc;
-    g_launches += 6;
+    if ((rc = yz_pass(0, nc, 1, 0))) return rc;
+    if (tma) {
+        int grid = 0;
+        if ((rc = persistent_grid((const void*)fft_z_eval_tma<T, L, LINES>, FFT_TMA_THREADS, sm_ze, tiles1 * nc, &grid)))
+            return rc;
+        fft_z_eval_tma<T, L, LINES><<<grid, FFT_TMA_THREADS, sm_ze, str>>>(p->tmaps[f32][0][1], p->tmaps[f32][1][1], K,
+                                                                          nc, st, err);
+    } else {
+        fft_z_eval<T, L, LINES><<<dim3(L * ntile, nc), FFT_THREADS, smem3, str>>>(R, nspec, spec, nspec, K, st);
+    }
+    if ((rc = yz_pass(1, nc * S.nconv, 1, 1))) return rc;
+    // the functional derivative takes the fused x pass (weighted densities, Phi and dPhi/dn
+    // stay in shared memory); the free energy needs Phi in global memory: separate kernels
+    const bool fused = with_int && g_tuned.fft3d_fused_phi && p->tma_ready;
+    g_launches += 4;
+    if (fused) {
+        rc = (nc == 1) ? launch_fused_nc<T, L, 1>(b, st, spec, nspec, err) : launch_fused_nc<T, L, 2>(b, st, spec, nspec, err);
+        if (rc) return rc;
+    } else {
+        fft_x_c2r<T, L, LINES><<<dim3(xblocks, nc * S.nconv), FFT_THREADS, smem2, str>>>(spec, nspec, part, npts,
+                                                                                        T(S.NA / (double)npts), st);
+        rc = launch_phi<T>(b, st);
+        if (rc) return rc;
+        g_launches += 2;
+    }
     if (with_int) {
-        for (int i = 0; i < nc; ++i)
-            fft_x_r2c<T, T, L, LINES><<<dim3(xblocks, S.nconv), FFT_THREADS, smem2, str>>>(
-                dfield + ((size_t)i * S.NF + 1) * npts, npts, spec + (size_t)i * S.nconv * nspec, nspec, st);
-        fft_yz<T, L, LINES><<<dim3(L * ntile, nc * S.nconv), FFT_THREADS, smem2, str>>>(spec, nspec, 1, 0, st);
-        fft_z_adjoint<T, L, LINES><<<dim3(L * ntile, nc), FFT_THREADS, smem3, str>>>(spec, nspec, R, nspec, K, st);
-        fft_yz<T, L, LINES><<<dim3(L * ntile, nc), FFT_THREADS, smem2, str>>>(R, nspec, 1, 1, st);
+        if (!fused) {
+            for (int i = 0; i < nc; ++i)
+                fft_x_r2c<T, T, L, LINES><<<dim3(xblocks, S.nconv), FFT_THREADS, smem2, str>>>(
+                    dfield + ((size_t)i * S.NF + 1) * npts, npts, spec + (size_t)i * S.nconv * nspec, nspec, st);
+            g_launches += nc;
+        }
+        if ((rc = yz_pass(1, nc * S.nconv, 1, 0))) return rc;
+        if (tma) {
+            int grid = 0;
+            if ((rc = persistent_grid((const void*)fft_z_adjoint_tma<T, L, LINES>, FFT_TMA_THREADS, sm_za, tiles1 * nc,
+                                      &grid)))
+                return rc;
+            fft_z_adjoint_tma<T, L, LINES><<<grid, FFT_TMA_THREADS, sm_za, str>>>(p->tmaps[f32][1][1],
+                                                                                 p->tmaps[f32][0][1], K, nc, st, err);
+        } else {
+            fft_z_adjoint<T, L, LINES><<<dim3(L * ntile, nc), FFT_THREADS, smem3, str>>>(spec, nspec, R, nspec, K, st);
+        }
+        if ((rc = yz_pass(0, nc, 1, 1))) return rc;
         fft_x_c2r<T, L, LINES><<<dim3(xblocks, nc), FFT_THREADS, smem2, str>>>(R, nspec, adj, npts,
                                                                               T(1.0 / (double)npts), st);
-        g_launches += nc + 4;
+        g_launches += 4;
     }
     CHECK_LAUNCH();
     return 0;
@@ -1022,7 +1178,7 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
         A.history_cap = b->hist_cap - off;
     }
     CU(cudaMemcpyAsync(b->d_st, st.data(), sizeof(AAState) * b->nsys, cudaMemcpyHostToDevice, b->stream));
-    CU(cudaMemsetAsync(b->d_done, 0, sizeof(int), b->stream));
+    CU(cudaMemsetAsync(b->d_done, 0, 2 * sizeof(int), b->stream));
     init_kernel<<<b->nechunks, ELEM_THREADS, 0, b->stream>>>(b->d_echunks, b->d_sys);
     CHECK_LAUNCH();
     g_launches += 1;
@@ -1033,7 +1189,10 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
         return set_error(CDFT_E_INVALID, "engine=%d", opts->engine);
     if (b->coord != CDFT_COORD_CART && opts->engine == CDFT_ENGINE_PERSISTENT)
         return set_error(CDFT_E_UNSUPPORTED, "spherical and cylindrical systems run on the grid engine");
-    if (b->nd == 1 && b->coord == CDFT_COORD_CART &&
+    const bool snapshots = opts->snapshot_every > 0 && opts->snapshot;
+    if (snapshots && opts->engine == CDFT_ENGINE_PERSISTENT)
+        return set_error(CDFT_E_UNSUPPORTED, "snapshots run on the grid engine (one graph launch per interval)");
+    if (!snapshots && b->nd == 1 && b->coord == CDFT_COORD_CART &&
         (opts->engine == CDFT_ENGINE_AUTO || opts->engine == CDFT_ENGINE_PERSISTENT)) {
         const size_t need = persistent_smem_need(b), limit = persistent_smem_limit(b);
         use_persistent = need <= limit && opts->m <= PERS_MAX_M;
@@ -1065,7 +1224,7 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
         rc = b->cur32 ? launch_persistent<float>(b, cap, smem, vec_m) : launch_persistent<double>(b, cap, smem, vec_m);
         if (rc) return rc;
     } else {
-        const int K = opts->iters_per_launch > 0 ? opts->iters_per_launch : 16;
+        const int K = snapshots ? opts->snapshot_every : (opts->iters_per_launch > 0 ? opts->iters_per_launch : 16);
         // the vector kernel instance whose history bound covers m (8, 12 or CDFT_MAX_M)
         b->vec_mb = (opts->m <= 8) ? 8 : (opts->m <= 12) ? 12 : CDFT_MAX_M;
         rc = batch_capture(b, K);
@@ -1075,8 +1234,23 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
             CU(cudaGraphLaunch(b->graph[b->cur32], b->stream));
             g_launches += b->graph_launches[b->cur32];
             launched_evals += K;
-            CU(cudaMemcpyAsync(b->h_done, b->d_done, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+            CU(cudaMemcpyAsync(b->h_done, b->d_done, 2 * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
             CU(cudaStreamSynchronize(b->stream));
+            if (b->h_done[1])
+                return set_error(CDFT_E_CUDA, "a tensor-memory transfer did not complete in time (kernel error %d)",
+                                 b->h_done[1]);
+            if (snapshots && *b->h_done < b->nsys) {
+                // every system still running has made K more evaluations: hand its iterate out
+                CU(cudaMemcpyAsync(st.data(), b->d_st, sizeof(AAState) * b->nsys, cudaMemcpyDeviceToHost, b->stream));
+                CU(cudaStreamSynchronize(b->stream));
+                for (int s = 0; s < b->nsys; ++s) {
+                    if (st[s].mode == MODE_DONE) continue;
+                    cdft_plan* p = b->plans[s];
+                    std::vector<double> h((size_t)p->sys.n_elem);
+                    CU(cudaMemcpy(h.data(), p->sys.rho, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+                    opts->snapshot(opts->snapshot_user, s, st[s].nevals + hist_off[s], h.data());
+                }
+            }
             if (*b->h_done >= b->nsys) break;
             if (launched_evals > max_evals + K) break;   // cannot happen: aasol's caps end every system
             if (opts->time_budget_s > 0) {
@@ -1255,6 +1429,23 @@ int launch_stage(Batch* b, int stage)
     return 0;
 }
 
+// the kernel error word of a batch (d_done[1]): cleared before a stand-alone evaluation and
+// checked after it (the converge loop checks it with every poll)
+int clear_kernel_error(Batch* b)
+{
+    CU(cudaMemsetAsync(b->d_done + 1, 0, sizeof(int), b->stream));
+    return 0;
+}
+
+int check_kernel_error(Batch* b)
+{
+    int e = 0;
+    CU(cudaMemcpyAsync(&e, b->d_done + 1, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    CU(cudaStreamSynchronize(b->stream));
+    if (e) return set_error(CDFT_E_CUDA, "a tensor-memory transfer did not complete in time (kernel error %d)", e);
+    return 0;
+}
+
 int functional_derivative(cdft_plan* p, const double* rho, double* out, bool is_dev)
 {
     if (!p || !rho || !out) return set_error(CDFT_E_INVALID, "NULL argument");
@@ -1264,6 +1455,7 @@ int functional_derivative(cdft_plan* p, const double* rho, double* out, bool is_
     if (rc) return rc;
     const size_t bytes = (size_t)p->sys.n_elem * sizeof(double);
     CU(cudaMemcpyAsync(p->sys.rho, rho, bytes, is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, p->stream));
+    if ((rc = clear_kernel_error(b))) return rc;
     rc = p->sys.mixed ? launch_eval_stages<float>(b, nullptr, true) : launch_eval_stages<double>(b, nullptr, true);
     if (rc) return rc;
     if (p->sys.mixed)
@@ -1274,7 +1466,7 @@ int functional_derivative(cdft_plan* p, const double* rho, double* out, bool is_
     g_launches += 1;
     CU(cudaMemcpyAsync(out, p->sys.out, bytes, is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, p->stream));
     CU(cudaStreamSynchronize(p->stream));
-    return 0;
+    return check_kernel_error(b);
 }
 
 // compensated (Neumaier) sum
@@ -1372,9 +1564,11 @@ int cdft_free_energy_res(cdft_plan* plan, const double* rho, double* F)
     if (rc) return rc;
     const size_t bytes = (size_t)plan->sys.n_elem * sizeof(double);
     CU(cudaMemcpyAsync(plan->sys.rho, rho, bytes, cudaMemcpyHostToDevice, plan->stream));
+    if ((rc = clear_kernel_error(b))) return rc;
     // the free-energy integral is FP64 in every precision mode
     rc = launch_eval_stages<double>(b, nullptr, false);
     if (rc) return rc;
+    if ((rc = check_kernel_error(b))) return rc;
     std::vector<double> f(plan->N);
     CU(cudaMemcpyAsync(f.data(), plan->sys.fval, sizeof(double) * plan->N, cudaMemcpyDeviceToHost, plan->stream));
     CU(cudaStreamSynchronize(plan->stream));

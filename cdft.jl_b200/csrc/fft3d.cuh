@@ -4,7 +4,9 @@
 // FFTs (convolve!, src/utils/integrals.jl:88-96) with the analytic kernels of
 // weighted_densities.jl:28-80,193-246 sampled at L*fftfreq.  Here the same
 // operator runs on the half spectrum (x is the real-to-complex axis):
-//   spectrum layout [field][z][y][kx], kx in [0, N/2], y and z in [0, N)
+//   spectrum layout [field][z][y][kx], kx in [0, N/2] valid, rows padded to KXP = N/2 + 2
+//   entries (a row of either precision is a multiple of 16 bytes: tensor-map strides),
+//   y and z in [0, N)
 //   x pass: two real rows packed into one complex N-point FFT and split
 //   y, z passes: in place, LINES consecutive kx per block (coalesced rows)
 // The kernel multiply is fused into the z pass: one kernel turns the spectrum
@@ -145,6 +147,12 @@ __device__ __forceinline__ typename V2<T>::t* fft_lines(typename V2<T>::t* x, ty
     return x;
 }
 
+// row length of the half spectrum: KX = L/2 + 1 valid entries, KXP = L/2 + 2 stored
+template <int L> struct Spec3 {
+    static constexpr int KX = L / 2 + 1;
+    static constexpr int KXP = L / 2 + 2;
+};
+
 struct Grid3 {
     int N;          // points per dimension
     int Kx;         // N/2 + 1
@@ -183,7 +191,8 @@ fft_x_r2c(const Tin* __restrict__ in, size_t in_stride, typename V2<T>::t* __res
     }
     __syncthreads();
     const C* Z = fft_lines<T, L, LINES, LS>(bufA, bufB, tw, false);
-    C* dst = out + field * out_stride + row0 * KX;
+    constexpr int KXP = Spec3<L>::KXP;
+    C* dst = out + field * out_stride + row0 * KXP;
     for (int idx = threadIdx.x; idx < LINES * KX; idx += blockDim.x) {
         const int line = idx / KX, k = idx - line * KX;
         const C zk = Z[k * LS + line];
@@ -193,8 +202,8 @@ fft_x_r2c(const Tin* __restrict__ in, size_t in_stride, typename V2<T>::t* __res
         a.y = T(0.5) * (zk.y + zm.y);
         b.x = T(0.5) * (zk.y - zm.y);
         b.y = T(-0.5) * (zk.x - zm.x);
-        dst[(size_t)(2 * line) * KX + k] = a;
-        dst[(size_t)(2 * line + 1) * KX + k] = b;
+        dst[(size_t)(2 * line) * KXP + k] = a;
+        dst[(size_t)(2 * line + 1) * KXP + k] = b;
     }
 }
 
@@ -217,12 +226,13 @@ fft_x_c2r(const typename V2<T>::t* __restrict__ in, size_t in_stride, T* __restr
     fft_twiddles<T, L>(tw);
     const int field = blockIdx.y;
     const size_t row0 = (size_t)blockIdx.x * 2 * LINES;
-    const C* src = in + field * in_stride + row0 * KX;
+    constexpr int KXP = Spec3<L>::KXP;
+    const C* src = in + field * in_stride + row0 * KXP;
     for (int idx = threadIdx.x; idx < LINES * L; idx += blockDim.x) {
         const int line = idx / L, k = idx - line * L;
         const int kk = (k <= L / 2) ? k : L - k;
-        C a = src[(size_t)(2 * line) * KX + kk];
-        C b = src[(size_t)(2 * line + 1) * KX + kk];
+        C a = src[(size_t)(2 * line) * KXP + kk];
+        C b = src[(size_t)(2 * line + 1) * KXP + kk];
         if (k > L / 2) { a = cconj(a); b = cconj(b); }
         C z;   // Z = X_a + i X_b
         z.x = a.x - b.y;
@@ -246,8 +256,8 @@ fft_x_c2r(const typename V2<T>::t* __restrict__ in, size_t in_stride, T* __restr
 template <typename T, int L, int LINES>
 __device__ __forceinline__ size_t yz_base(int axis, int outer, int kx0)
 {
-    constexpr int KX = L / 2 + 1;
-    return axis == 1 ? (size_t)outer * L * KX + kx0 : (size_t)outer * KX + kx0;
+    constexpr int KXP = Spec3<L>::KXP;
+    return axis == 1 ? (size_t)outer * L * KXP + kx0 : (size_t)outer * KXP + kx0;
 }
 
 template <typename T, int L, int LINES>
@@ -266,7 +276,7 @@ fft_yz(typename V2<T>::t* __restrict__ data, size_t stride, int axis, int invers
     const int ntile = (KX + LINES - 1) / LINES;
     const int kx0 = (blockIdx.x % ntile) * LINES;
     const int outer = blockIdx.x / ntile;
-    const size_t estride = axis == 1 ? KX : (size_t)L * KX;
+    const size_t estride = axis == 1 ? Spec3<L>::KXP : (size_t)L * Spec3<L>::KXP;
     C* d = data + blockIdx.y * stride + yz_base<T, L, LINES>(axis, outer, kx0);
     const int nl = min(LINES, KX - kx0);
     for (int idx = threadIdx.x; idx < L * LINES; idx += blockDim.x) {
@@ -340,8 +350,8 @@ fft_z_eval(const typename V2<T>::t* __restrict__ R, size_t r_stride, typename V2
     const int kx0 = (blockIdx.x % ntile) * LINES;
     const int y = blockIdx.x / ntile;
     const int comp = blockIdx.y;
-    const size_t estride = (size_t)L * KX;
-    const size_t base = (size_t)y * KX + kx0;
+    const size_t estride = (size_t)L * Spec3<L>::KXP;
+    const size_t base = (size_t)y * Spec3<L>::KXP + kx0;
     const int nl = min(LINES, KX - kx0);
     const C* src = R + comp * r_stride + base;
     for (int idx = threadIdx.x; idx < L * LINES; idx += blockDim.x) {
@@ -394,8 +404,8 @@ fft_z_adjoint(const typename V2<T>::t* __restrict__ in, size_t in_stride, typena
     const int kx0 = (blockIdx.x % ntile) * LINES;
     const int y = blockIdx.x / ntile;
     const int comp = blockIdx.y;
-    const size_t estride = (size_t)L * KX;
-    const size_t base = (size_t)y * KX + kx0;
+    const size_t estride = (size_t)L * Spec3<L>::KXP;
+    const size_t base = (size_t)y * Spec3<L>::KXP + kx0;
     const int nl = min(LINES, KX - kx0);
     // every slot of the padded [n * LS + line] layout starts at zero
     for (int idx = threadIdx.x; idx < L * LS; idx += blockDim.x) { acc[idx].x = T(0); acc[idx].y = T(0); }

@@ -19,14 +19,22 @@
 #define PERS_TILE (32 * PERS_R)
 #define PERS_MAX_M 8           // Anderson depth bound of the persistent engine (deeper: grid engine)
 
-// extended periodic window of one convolution input: ext[k] = in[(k - OFF) mod N]
-__host__ __device__ __forceinline__ int pers_extn(int N) { return 2 * N + 32 * (PERS_R + 2); }
-__host__ __device__ __forceinline__ int pers_off(int N) { return N + 32; }
+// extended periodic window of one convolution input: logical ext[k] = in[(k - OFF) mod N],
+// k < EXTN; OFF is a multiple of 16.  The FP64 (tensor-core) path stores logical element k at
+// pers_pos(k) = k + 4 floor(k / 16): a warp's 8 x 4 B-fragment loads then fall on each
+// double-wide bank pair exactly twice (2 wavefronts, the minimum for 32 doubles).  Rows are
+// pers_extp(N) long.  Taps of a field are stored with PERS_TPAD zeros on either side.
+#define PERS_TPAD 16
+__host__ __device__ __forceinline__ int pers_off(int N) { return (N + 32 + 15) & ~15; }
+__host__ __device__ __forceinline__ int pers_extn(int N) { return pers_off(N) + N + 32 * (PERS_R + 1) + 16; }
+__host__ __device__ __forceinline__ int pers_pos(int k) { return k + 4 * (k >> 4); }
+__host__ __device__ __forceinline__ int pers_extp(int N) { return pers_extn(N) + 4 * ((pers_extn(N) + 15) >> 4); }
+__host__ __device__ __forceinline__ int pers_ts(int N) { return N + 2 * PERS_TPAD; }
 
 __host__ __device__ __forceinline__ size_t pers_smem_bytes(int N, int nc, int nconv, int NF, size_t esz)
 {
-    return esz * ((size_t)nc * nconv * N              // taps
-                  + (size_t)nc * nconv * pers_extn(N)  // extended inputs
+    return esz * ((size_t)nc * nconv * pers_ts(N)      // taps (zero-padded)
+                  + (size_t)nc * nconv * pers_extp(N)  // extended inputs
                   + (size_t)nc * NF * N                // n, then dPhi/dn
                   + (size_t)nc * nconv * N);           // adjoint partials
 }
@@ -88,7 +96,7 @@ __device__ __forceinline__ void pers_conv(const T* __restrict__ ext, bool shared
                                           T* __restrict__ out, int out_comp_stride, int N, int nconv, T scale)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int EXTN = pers_extn(N), OFF = pers_off(N);
+    const int EXTN = pers_extp(N), OFF = pers_off(N);   // FP32 rows: logical positions, row stride extp
     const int ntiles = (N + PERS_TILE - 1) / PERS_TILE;
     const int ntask = NC * nconv * ntiles;
     for (int task = warp; task < ntask; task += PERS_WARPS) {
@@ -96,7 +104,7 @@ __device__ __forceinline__ void pers_conv(const T* __restrict__ ext, bool shared
         const int f = (task / ntiles) % nconv;
         const int i = task / (ntiles * nconv);
         const T* in = ext + (size_t)(shared_input ? i : i * nconv + f) * EXTN + OFF;
-        const T* tp = taps + (size_t)(i * nconv + f) * N;
+        const T* tp = taps + (size_t)(i * nconv + f) * pers_ts(N) + PERS_TPAD;
         const int j0 = tile * PERS_TILE + lane;
         T acc[PERS_R];
 #pragma unroll
@@ -145,16 +153,16 @@ __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, do
                  : "d"(a), "d"(b));
 }
 
-// PERIODIC = true: the inputs are read in place, input (i, f) = ext + i * in_comp_stride
-// + f * N, with the index taken mod N (no extended copy); false: the extended inputs.
-template <int NC, bool PERIODIC = false>
+// Extended inputs at bank-spread positions (pers_pos), taps zero-padded: the loop has no
+// bounds test.  The d loop runs two tap blocks per step into four independent accumulator
+// pairs (even / odd d, c < 4 / c >= 4), summed at the end.
+template <int NC>
 __device__ __forceinline__ void pers_conv_dmma(const double* __restrict__ ext, bool shared_input,
                                                const double* __restrict__ taps, double* __restrict__ out,
-                                               int out_comp_stride, int N, int nconv, double scale,
-                                               int in_comp_stride = 0)
+                                               int out_comp_stride, int N, int nconv, double scale)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int EXTN = pers_extn(N), OFF = pers_off(N);
+    const int EXTP = pers_extp(N), OFF = pers_off(N), TS = pers_ts(N);
     const int U = (N + 7) / 8;          // 8-output columns
     const int nut = (U + 7) / 8;        // warp tiles of 8 columns
     const int D = (N + 14) / 8;         // tap blocks: 8 (D - 1) + 7 >= N - 1
@@ -164,46 +172,34 @@ __device__ __forceinline__ void pers_conv_dmma(const double* __restrict__ ext, b
         const int ut = task % nut;
         const int f = (task / nut) % nconv;
         const int i = task / (nut * nconv);
-        const double* tp = taps + (size_t)(i * nconv + f) * N;
+        const double* tp = taps + (size_t)(i * nconv + f) * TS + PERS_TPAD;   // tp[q] = 0 outside [0, N)
+        const double* in = ext + (size_t)(shared_input ? i : i * nconv + f) * EXTP;
         const int u0 = ut * 8;
-        double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
-        // B: e[8 (u0 + r - d) + c], column n = r; A: t(8 d + r - c)
-        if constexpr (PERIODIC) {
-            const double* in = ext + (size_t)i * in_comp_stride + (size_t)f * N;
-            // N >= 8 (checked by the caller): one conditional add/subtract keeps the
-            // index in [0, N) and the loop free of branches
-            int i0 = (8 * (u0 + r) + k) % N;   // index of d = 0, c = k; c = k + 4 is 4 further
-            for (int d = 0; d < D; ++d) {
-                const int q0 = 8 * d + r - k;
-                const int q1 = q0 - 4;
-                const double a0 = (q0 >= 0 && q0 < N) ? tp[q0] : 0.0;
-                const double a1 = (q1 >= 0 && q1 < N) ? tp[q1] : 0.0;
-                const int i1 = i0 + 4 - ((i0 + 4 >= N) ? N : 0);
-                const double b0 = in[i0];
-                const double b1 = in[i1];
-                dmma_m8n8k4(c0, c1, a0, b0);
-                dmma_m8n8k4(e0, e1, a1, b1);
-                i0 -= 8;
-                i0 += (i0 < 0) ? N : 0;
-            }
-        } else {
-            const double* in = ext + (size_t)(shared_input ? i : i * nconv + f) * EXTN + OFF;
-            const double* bp = in + 8 * (u0 + r) + k;
-            for (int d = 0; d < D; ++d) {
-                const int q0 = 8 * d + r - k;        // c = k
-                const int q1 = q0 - 4;               // c = k + 4
-                const double a0 = (q0 >= 0 && q0 < N) ? tp[q0] : 0.0;
-                const double a1 = (q1 >= 0 && q1 < N) ? tp[q1] : 0.0;
-                const double b0 = bp[-8 * d];
-                const double b1 = bp[-8 * d + 4];
-                dmma_m8n8k4(c0, c1, a0, b0);
-                dmma_m8n8k4(e0, e1, a1, b1);
-            }
+        double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0, g0 = 0.0, g1 = 0.0, h0 = 0.0, h1 = 0.0;
+        // B: e[8 (u0 + r - d) + c] at logical OFF + 8 (u0 + r) + c - 8 d; A: t(8 d + r - c)
+        const int xb = OFF + 8 * (u0 + r) + k;
+        int d = 0;
+        for (; d + 1 < D; d += 2) {
+            const int q0 = 8 * d + r - k;
+            const int x0 = xb - 8 * d, x1 = x0 - 8;
+            const double a0 = tp[q0], a1 = tp[q0 - 4], a2 = tp[q0 + 8], a3 = tp[q0 + 4];
+            const double b0 = in[pers_pos(x0)], b1 = in[pers_pos(x0 + 4)];
+            const double b2 = in[pers_pos(x1)], b3 = in[pers_pos(x1 + 4)];
+            dmma_m8n8k4(c0, c1, a0, b0);
+            dmma_m8n8k4(e0, e1, a1, b1);
+            dmma_m8n8k4(g0, g1, a2, b2);
+            dmma_m8n8k4(h0, h1, a3, b3);
+        }
+        if (d < D) {
+            const int q0 = 8 * d + r - k;
+            const int x0 = xb - 8 * d;
+            dmma_m8n8k4(c0, c1, tp[q0], in[pers_pos(x0)]);
+            dmma_m8n8k4(e0, e1, tp[q0 - 4], in[pers_pos(x0 + 4)]);
         }
         double* o = out + (size_t)i * out_comp_stride + (size_t)f * N;
         const int j0 = 8 * (u0 + 2 * k) + r, j1 = j0 + 8;
-        if (j0 < N) o[j0] = (c0 + e0) * scale;
-        if (j1 < N) o[j1] = (c1 + e1) * scale;
+        if (j0 < N) o[j0] = ((c0 + e0) + (g0 + h0)) * scale;
+        if (j1 < N) o[j1] = ((c1 + e1) + (g1 + h1)) * scale;
     }
 }
 
@@ -268,11 +264,11 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
     constexpr int NF = 6 + ND, NCONV = 5 + ND;
     const SysDev& G = sys[blockIdx.x];
     const int N = G.N, n_elem = G.n_elem;
-    const int EXTN = pers_extn(N), OFF = pers_off(N);
+    const int EXTN = pers_extn(N), EXTP = pers_extp(N), OFF = pers_off(N), TS = pers_ts(N);
     const int tid = threadIdx.x;
     T* taps = reinterpret_cast<T*>(smem_raw);
-    T* ext = taps + (size_t)NC * NCONV * N;
-    T* nf = ext + (size_t)NC * NCONV * EXTN;
+    T* ext = taps + (size_t)NC * NCONV * TS;
+    T* nf = ext + (size_t)NC * NCONV * EXTP;
     T* ip = nf + (size_t)NC * NF * N;
     if (tid == 0) {
         sA = st[blockIdx.x];
@@ -280,7 +276,10 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
     }
     {
         const T* src = (sizeof(T) == 8) ? reinterpret_cast<const T*>(G.taps) : reinterpret_cast<const T*>(G.taps32);
-        for (int k = tid; k < NC * NCONV * N; k += PERS_THREADS) taps[k] = src[k];
+        for (int k = tid; k < NC * NCONV * TS; k += PERS_THREADS) {
+            const int slot = k / TS, q = k - slot * TS - PERS_TPAD;
+            taps[k] = (q >= 0 && q < N) ? src[(size_t)slot * N + q] : T(0);
+        }
     }
     // vec_m >= 0: the Anderson vectors (rho, sol, gx, res, df, V_ext, vec_m columns
     // of Q and of DG) live in shared memory after the convolution buffers; rho and
@@ -316,7 +315,7 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
             const int i = k / EXTN, u = k - i * EXTN;
             int j = (u - OFF) % N;
             j += (j < 0) ? N : 0;
-            ext[k] = T(S.rho[i * N + j]);
+            ext[(size_t)i * EXTP + (sizeof(T) == 8 ? pers_pos(u) : u)] = T(S.rho[i * N + j]);
         }
         for (int e = tid; e < n_elem; e += PERS_THREADS) {
             const int i = e / N, j = e - i * N;
@@ -350,18 +349,13 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
         }
         __syncthreads();
         // ---- adjoint convolutions (integrate_field!) ----
-        if (sizeof(T) == 8 && N >= 8) {
-            // FP64: the tensor-core convolution reads dPhi/dn in place, periodically indexed
-            pers_conv_dmma<NC, true>(reinterpret_cast<const double*>(nf + N), false,
-                                     reinterpret_cast<const double*>(taps), reinterpret_cast<double*>(ip),
-                                     NCONV * N, N, NCONV, 1.0, NF * N);
-        } else {
+        {
             for (int k = tid; k < NC * NCONV * EXTN; k += PERS_THREADS) {
                 const int slot = k / EXTN, u = k - slot * EXTN;
                 const int i = slot / NCONV, f = slot - i * NCONV;
                 int j = (u - OFF) % N;
                 j += (j < 0) ? N : 0;
-                ext[k] = nf[(i * NF + f + 1) * N + j];
+                ext[(size_t)slot * EXTP + (sizeof(T) == 8 ? pers_pos(u) : u)] = nf[(i * NF + f + 1) * N + j];
             }
             __syncthreads();
             pers_conv_any<T, NC>(ext, false, taps, ip, NCONV * N, N, NCONV, T(1));

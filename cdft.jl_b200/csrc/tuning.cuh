@@ -15,6 +15,12 @@ struct TunedShapes {
     // Measured on the 64-point isotherm (N = 100..400, m = 5): the whole block is faster at
     // every size (Anderson section 5.6 vs 10.7 us per evaluation on average), so 0.
     int pers_warp_aa_max_elem = 0;
+    // 3D grids: the strided y and z FFT passes as persistent TMA tile kernels (1) or as one
+    // block per tile with per-thread loads (0); both compute the same arithmetic
+    int fft3d_tma = 1;
+    // 3D grids: the inverse x pass of the 8 convolved fields, Phi and the forward x pass in one
+    // kernel (1) or three (0); both compute the same arithmetic
+    int fft3d_fused_phi = 1;
 };
 
 static TunedShapes g_tuned;
@@ -27,6 +33,8 @@ struct TunedEntry {
 
 static const TunedEntry kTunedEntries[] = {
     {"pers_warp_aa_max_elem", &TunedShapes::pers_warp_aa_max_elem, 0, 1 << 30},
+    {"fft3d_tma", &TunedShapes::fft3d_tma, 0, 1},
+    {"fft3d_fused_phi", &TunedShapes::fft3d_fused_phi, 0, 1},
 };
 
 inline const TunedEntry* tuned_entry(const char* name)

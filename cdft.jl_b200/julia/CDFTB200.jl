@@ -12,12 +12,26 @@ module CDFTB200
 using cDFT
 using cDFT: DFTSystem, DFTOptions, DFTProblem, AASol
 using Clapeyron: PCSAFTModel
+using ChainRulesCore
+using CUDA
 
 const LIB = get(ENV, "CDFT_B200_LIB", joinpath(@__DIR__, "..", "cdft_b200", "libcdft_b200.so"))
 const MAX_NC = 4
 const MAX_ASSOC = 1
 
-struct B200Device end
+"""
+    B200Device(; mixed = false)
+
+The device of `DFTOptions` that routes a PC-SAFT system to libcdft_b200.  `mixed = true`
+selects the mixed-precision path (FP32 convolutions and Φ; FP64 Anderson, norms and
+integrals; an FP64 polish to the FP64 fixed point).  `DFTOptions(B200Device(); precision =
+Float64)` is the default; `precision = Float32` (the reference's all-FP32 mode,
+devices.jl:29-40) is refused: the library computes no FP32 solver.
+"""
+struct B200Device
+    mixed::Bool
+end
+B200Device(; mixed::Bool = false) = B200Device(mixed)
 export B200Device
 
 struct CDFTAssocPair
@@ -62,6 +76,9 @@ struct CDFTSolverOpts
     iters_per_launch::Cint
     engine::Cint
     mixed_switch_rtol::Cdouble
+    snapshot_every::Cint
+    snapshot::Ptr{Cvoid}            # void (*)(void* user, int system, int evaluations, const double* rho)
+    snapshot_user::Ptr{Cvoid}
 end
 
 mutable struct CDFTResult
@@ -119,7 +136,9 @@ function system_desc(system::DFTSystem{<:PCSAFTModel}, vext::Union{Nothing,Array
     coord = st isa cDFT.DFTStructByCoord{cDFT.Cartesian} ? 0 :
             st isa cDFT.DFTStructByCoord{cDFT.Spherical} ? 1 :
             st isa cDFT.DFTStructByCoord{cDFT.Cylindrical} ? 2 : error("unsupported coordinates")
-    prec = cDFT.fptype(system.options) == Float64 ? Cint(0) : Cint(1)
+    cDFT.fptype(system.options) == Float64 ||
+        error("B200Device computes in FP64 or mixed precision (B200Device(mixed = true)); precision = Float32 is not offered")
+    prec = system.options.device.mixed ? Cint(1) : Cint(0)
     CDFTSystemDesc(nd, ng, Tuple(b), coord, nc, pad(model.params.segment.values, MAX_NC),
                    pad(sp.size, MAX_NC), sigma, epsv, cDFT.length_scale(model), T, nassoc, pairs,
                    pad(sp.chempot_res .+ log.(sp.bulk_density), MAX_NC),
@@ -157,21 +176,115 @@ end
 
 const B200System = DFTSystem{<:PCSAFTModel,<:Any,<:Any,<:Any,<:Any,<:Any,<:DFTOptions{B200Device}}
 
-# converge!(prob::DFTProblem, method::AASol, ρ), src/methods/converge.jl:220-254
-function cDFT.converge!(prob::DFTProblem{<:B200System}, method::AASol, ρ::Array{Float64})
-    opts = CDFTSolverOpts(method.m, method.maxit, method.rtol, method.atol, method.beta,
-                          method.picard_maxit, method.picard_beta, method.picard_rtol,
-                          method.picard_atol, 0.0, 0, 0, 0.0)
-    res = CDFTResult()
-    check(ccall((:cdft_converge, LIB), Cint,
-                (Ptr{Cvoid}, Ptr{Float64}, Ref{CDFTSolverOpts}, Ref{CDFTResult}),
-                plan_for(prob.system), ρ, opts, res))
+solver_opts(method::AASol; every = 0, cb = C_NULL, user = C_NULL) =
+    CDFTSolverOpts(method.m, method.maxit, method.rtol, method.atol, method.beta, method.picard_maxit,
+                   method.picard_beta, method.picard_rtol, method.picard_atol, 0.0, 0, 0, 0.0,
+                   every, cb, user)
+
+# DFTProblem's save_callback / log_interval (converge.jl:31-60,256-267): the library hands out the
+# profile every gcd(save_interval, log_interval) evaluations; the free energy of the logged
+# profiles is computed once converge! returns (the callback runs while the plan is busy)
+mutable struct Hooks
+    prob::Any
+    shape::Tuple
+    logged::Vector{Tuple{Int,Array{Float64}}}
+end
+
+function snapshot_hook(user::Ptr{Cvoid}, s::Cint, it::Cint, rho::Ptr{Cdouble})
+    h = unsafe_pointer_to_objref(user)::Hooks
+    ρ = copy(reshape(unsafe_wrap(Array, rho, prod(h.shape)), h.shape))
+    p = h.prob
+    p.save_interval > 0 && it % p.save_interval == 0 && p.save_callback(Int(it), ρ)
+    p.log_interval > 0 && it % p.log_interval == 0 && push!(h.logged, (Int(it), ρ))
+    return nothing
+end
+
+function report(prob, method, res, hooks)
+    if hooks !== nothing
+        for (it, ρ) in hooks.logged
+            @info "DFT iter $(lpad(it, 5)) | F = $(round(cDFT.free_energy(prob.system, ρ); sigdigits=6))"
+        end
+    end
     if method.verbose
         msg = res.idid != 0 ? "DFT converged" : "DFT did not converge"
         @info "$msg after $(res.evaluations) evaluations: err = $(round(res.resnorm; sigdigits=3))"
     end
+end
+
+function with_hooks(f, prob, method, shape)
+    every = prob.log_interval > 0 && prob.save_interval > 0 ? gcd(prob.log_interval, prob.save_interval) :
+            max(prob.log_interval, prob.save_interval)
+    every == 0 && return f(solver_opts(method), nothing)
+    hooks = Hooks(prob, shape, Tuple{Int,Array{Float64}}[])
+    cb = @cfunction(snapshot_hook, Cvoid, (Ptr{Cvoid}, Cint, Cint, Ptr{Cdouble}))
+    GC.@preserve hooks f(solver_opts(method; every = every, cb = cb, user = pointer_from_objref(hooks)), hooks)
+end
+
+# converge!(prob::DFTProblem, method::AASol, ρ), src/methods/converge.jl:220-254
+function cDFT.converge!(prob::DFTProblem{<:B200System}, method::AASol, ρ::Array{Float64})
+    res = CDFTResult()
+    with_hooks(prob, method, size(ρ)) do opts, hooks
+        check(ccall((:cdft_converge, LIB), Cint,
+                    (Ptr{Cvoid}, Ptr{Float64}, Ref{CDFTSolverOpts}, Ref{CDFTResult}),
+                    plan_for(prob.system), ρ, opts, res))
+        report(prob, method, res, hooks)
+    end
     return nothing
 end
+
+# the same for a profile in device memory (CUDA.jl): the plan runs on the task's stream
+function cDFT.converge!(prob::DFTProblem{<:B200System}, method::AASol, ρ::CuArray{Float64})
+    res = CDFTResult()
+    plan = plan_for(prob.system)
+    check(ccall((:cdft_plan_set_stream, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), plan, CUDA.stream().handle))
+    with_hooks(prob, method, size(ρ)) do opts, hooks
+        check(ccall((:cdft_converge_dev, LIB), Cint,
+                    (Ptr{Cvoid}, CuPtr{Float64}, Ref{CDFTSolverOpts}, Ref{CDFTResult}),
+                    plan, pointer(ρ), opts, res))
+        report(prob, method, res, hooks)
+    end
+    return nothing
+end
+
+"""
+    converge_batch!(systems, ρs; kwargs...)
+
+Converge many independent B200 systems (state points, pore widths; uneven grids) in one
+batch: every kernel launch covers all of them (cdft_batch_converge).  The keywords are
+converge!'s (`AASol(system; kwargs...)`, converge.jl:3-13), shared by the batch; the
+systems must agree in the number of components, dimension and precision.  `ρs` are
+`Array{Float64}` (host) or `CuArray{Float64}` (device) profiles, converged in place.
+Returns the per-system (idid, errcode, evaluations).
+"""
+function converge_batch!(systems::AbstractVector, ρs::AbstractVector; kwargs...)
+    n = length(systems)
+    n == length(ρs) || error("systems and profiles differ in length")
+    method = AASol(first(systems); kwargs...)
+    opts = solver_opts(method)
+    plans = Ptr{Cvoid}[plan_for(s) for s in systems]
+    # cdft_result records are laid out contiguously for the library
+    buf = Vector{UInt8}(undef, n * sizeof(CDFTResult))
+    if all(r -> r isa CuArray, ρs)
+        check(ccall((:cdft_plan_set_stream, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), plans[1], CUDA.stream().handle))
+        for p in plans[2:end]
+            check(ccall((:cdft_plan_set_stream, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), p, CUDA.stream().handle))
+        end
+        ptrs = [reinterpret(Ptr{Float64}, pointer(r)) for r in ρs]
+        check(ccall((:cdft_batch_converge_dev, LIB), Cint,
+                    (Ptr{Ptr{Cvoid}}, Cint, Ptr{Ptr{Float64}}, Ref{CDFTSolverOpts}, Ptr{UInt8}),
+                    plans, n, ptrs, opts, buf))
+    else
+        GC.@preserve ρs begin
+            ptrs = [pointer(r) for r in ρs]
+            check(ccall((:cdft_batch_converge, LIB), Cint,
+                        (Ptr{Ptr{Cvoid}}, Cint, Ptr{Ptr{Float64}}, Ref{CDFTSolverOpts}, Ptr{UInt8}),
+                        plans, n, ptrs, opts, buf))
+        end
+    end
+    out = [unsafe_load(Ptr{CDFTResult}(pointer(buf)) + (k - 1) * sizeof(CDFTResult)) for k in 1:n]
+    return [(r.idid != 0, Int(r.errcode), Int(r.evaluations)) for r in out]
+end
+export converge_batch!
 
 # δFδρ_res(system, ρ), src/models/models.jl:194-200
 function cDFT.δFδρ_res(system::B200System, ρ::Array{Float64})
@@ -187,6 +300,58 @@ function cDFT.F_res(system::B200System, ρ::Array{Float64})
     check(ccall((:cdft_free_energy_res, LIB), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ref{Cdouble}),
                 plan_for(system), ρ, F))
     return F[]
+end
+
+# δFδρ_res for a device profile (CuArray): cdft_functional_derivative_dev on the task's stream
+function cDFT.δFδρ_res(system::B200System, ρ::CuArray{Float64})
+    out = similar(ρ)
+    plan = plan_for(system)
+    check(ccall((:cdft_plan_set_stream, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), plan, CUDA.stream().handle))
+    check(ccall((:cdft_functional_derivative_dev, LIB), Cint, (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}),
+                plan, pointer(ρ), pointer(out)))
+    return out
+end
+
+# ---------------------------------------------------------------------------
+# dγ/dθ: the interfacial tension of a converged two-interface box as a function of the
+# model parameters θ = (σ_k [Å], ε_k/k_B [K], m_k), k = 1..nc, with its reverse rule.
+# At the converged profile δΩ/δρ = 0, so the pullback needs no pass through converge!:
+# dγ/dθ = [k_B T ∂F_res/∂θ|ρ − Σ_i dμ_i/dθ ∫ρ_i + dp/dθ ∫1] / 2  (cdft_grad_params).
+# ---------------------------------------------------------------------------
+"""
+    interface_tension(θ, system, ρ; dμdθ = nothing, dpdθ = nothing)
+
+γ of the converged TwoPhase1DCart profile `ρ` of `system`, whose model has the parameters
+`θ` (checked): surface_tension(system, ρ) / 2, the two interfaces of the periodic box
+(interfacial_tension.jl:30, surface_tension.jl:28).  `dμdθ` (nc × 3nc, J/mol per unit of θ)
+and `dpdθ` (3nc, Pa) describe how the bulk state follows θ (e.g. along the LLE, from
+Clapeyron with ForwardDiff); `nothing` holds it fixed.  Differentiable with ChainRulesCore.
+"""
+function interface_tension(θ::AbstractVector, system::B200System, ρ::Array{Float64}; dμdθ = nothing, dpdθ = nothing)
+    model = system.model
+    nc = length(model)
+    θm = reduce(vcat, [[model.params.sigma.values[k, k] * 1e10, model.params.epsilon.values[k, k],
+                        model.params.segment.values[k]] for k in 1:nc])
+    isapprox(θ, θm; rtol = 1e-12) || error("θ differs from the parameters of the system's model")
+    return cDFT.surface_tension(system, ρ) / 2
+end
+export interface_tension
+
+function ChainRulesCore.rrule(::typeof(interface_tension), θ::AbstractVector, system::B200System,
+                              ρ::Array{Float64}; dμdθ = nothing, dpdθ = nothing)
+    γ = interface_tension(θ, system, ρ; dμdθ, dpdθ)
+    nt = 3 * length(system.model)
+    dΩ = zeros(nt)
+    μ = dμdθ === nothing ? C_NULL : Matrix{Float64}(transpose(dμdθ))   # row-major nc x 3nc for C
+    p = dpdθ === nothing ? C_NULL : Vector{Float64}(dpdθ)
+    GC.@preserve μ p check(ccall((:cdft_grad_params, LIB), Cint,
+                                 (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                                 plan_for(system), ρ, μ === C_NULL ? C_NULL : pointer(μ),
+                                 p === C_NULL ? C_NULL : pointer(p), dΩ))
+    function interface_tension_pullback(γ̄)
+        return (NoTangent(), unthunk(γ̄) .* dΩ ./ 2, NoTangent(), NoTangent())
+    end
+    return γ, interface_tension_pullback
 end
 
 end # module

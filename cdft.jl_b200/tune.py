@@ -1,0 +1,117 @@
+"""Autotuner of the library's launch shapes (the entries of csrc/tuning.cuh).
+
+Every entry is swept on the workload it governs, timed with CUDA events after warm-up,
+and the fastest value is reported with the time of every candidate:
+
+* pers_warp_aa_max_elem -- persistent engine, Anderson section on one warp for systems of
+  at most this many elements: the 64-point slit-pore isotherm (N = 100..400), batched.
+* fft3d_tma, fft3d_fused_phi -- 3D grids: TMA tile kernels for the y/z passes, the fused
+  x pass with Phi: one functional derivative of the 27-solute argon box at 64^3 and
+  128^3, FP64 and mixed.
+
+    python cdft.jl_b200/tune.py [--out tuning.json]
+
+The entries that change arithmetic (the warp Anderson section reduces in another order)
+are per-system rules, so a sweep can set them freely; the defaults compiled into the
+library are the winners of this sweep on B200.
+"""
+import argparse
+import ctypes
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+for p in (HERE, ROOT):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def _events(fn, reps, warm=2):
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def sweep_isotherm(values=(0, 256, 512, 1024)):
+    import cdft_b200 as cd
+    import bench
+    systems, rho0 = bench.build_systems(bench.isotherm_specs(0), "fp64")
+    method = cd.AASol.for_system(None, **bench.SOLVER)
+    out = {}
+    for v in values:
+        cd.tuning("pers_warp_aa_max_elem", v)
+
+        def run():
+            rr = [r.copy() for r in rho0]
+            cd.batch_converge(systems, rr, method=method)
+
+        out[v] = _events(run, 3)
+    return out
+
+
+def sweep_3d(sizes=(64, 128), precisions=("fp64", "mixed")):
+    import cdft_b200 as cd
+    import bench
+    from cdft_b200 import _lib
+    lib = _lib.load()
+    out = {}
+    for N in sizes:
+        for prec in precisions:
+            sy = bench._solutes3d_system(N, prec)
+            rho = cd.initialize_profiles(sy)
+            plans = (ctypes.c_void_p * 1)(sy._plan.value)
+            cd.dFdrho_res(sy, rho)   # the plan's device profile
+            for tma, fused in ((0, 0), (1, 0), (1, 1)):
+                cd.tuning("fft3d_tma", tma)
+                cd.tuning("fft3d_fused_phi", fused)
+                ms = ctypes.c_double()
+                _lib.check(lib.cdft_batch_time_stage(plans, 1, 3, 20, ctypes.byref(ms)))
+                out[f"{N}^3 {prec} tma={tma} fused={fused}"] = ms.value
+            sy.close()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=None)
+    args = ap.parse_args()
+    import cdft_b200 as cd
+    defaults = {k: cd.tuning(k) for k in ("pers_warp_aa_max_elem", "fft3d_tma", "fft3d_fused_phi")}
+    res = {"isotherm64_ms_per_batch": sweep_isotherm(), "solutes3d_ms_per_functional_derivative": sweep_3d()}
+    for k, v in defaults.items():
+        cd.tuning(k, v)
+    iso = res["isotherm64_ms_per_batch"]
+    best = {"pers_warp_aa_max_elem": min(iso, key=iso.get)}
+    d3 = res["solutes3d_ms_per_functional_derivative"]
+    totals = {}
+    for key, ms in d3.items():
+        shape = key.split(" ", 2)[2]
+        totals[shape] = totals.get(shape, 0.0) + ms
+    shape = min(totals, key=totals.get)
+    best["fft3d_tma"] = int(shape.split()[0].split("=")[1])
+    best["fft3d_fused_phi"] = int(shape.split()[1].split("=")[1])
+    res["best"] = best
+    res["defaults_compiled"] = defaults
+    res["when"] = time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())
+    line = json.dumps(res, default=str)
+    print(line)
+    if args.out:
+        with open(args.out, "w") as f:
+            f.write(line + "\n")
+
+
+if __name__ == "__main__":
+    main()

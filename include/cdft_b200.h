@@ -82,6 +82,14 @@ typedef struct {
     int precision;                   /* CDFT_PREC_* */
 } cdft_system_desc;
 
+/* Called by cdft_converge / cdft_batch_converge every snapshot_every fixed-point
+ * evaluations with the profile of system `system` (index in the batch) after
+ * `evaluations` evaluations (the iterate the next evaluation receives), nc x N doubles in
+ * host memory valid during the call.  The counterpart of DFTProblem's save_callback /
+ * log_interval (src/methods/converge.jl:31-60,256-267).  It runs on the calling thread
+ * between kernel launches and must not call the library with the plans being converged. */
+typedef void (*cdft_snapshot_fn)(void* user, int system, int evaluations, const double* rho);
+
 /* The AASol fields used by aasol (src/utils/anderson.jl:193-207).  The
  * converge! keyword form maps onto it as __AASol does (converge.jl:3-9):
  * rtol = atol = tol, picard_maxit = maxit, picard_beta = beta,
@@ -100,6 +108,10 @@ typedef struct {
                                  ||r|| <= rtol ||r0|| + atol, the stopping test of an FP64 run (r0 of
                                  the initial profile); a system whose FP32 phase diverges is converged
                                  again in FP64 from its initial profile; <= 0: 1e-5 */
+    int snapshot_every;    /* > 0: call snapshot every this many evaluations (runs the grid engine,
+                              one CUDA-graph launch per interval); 0: never */
+    cdft_snapshot_fn snapshot;
+    void* snapshot_user;
 } cdft_solver_opts;
 
 /* execution engines of cdft_converge / cdft_batch_converge */

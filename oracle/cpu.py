@@ -48,6 +48,7 @@ class SolverOpts(ctypes.Structure):
         ("beta", ctypes.c_double), ("picard_maxit", ctypes.c_int), ("picard_beta", ctypes.c_double),
         ("picard_rtol", ctypes.c_double), ("picard_atol", ctypes.c_double), ("time_budget_s", ctypes.c_double),
         ("iters_per_launch", ctypes.c_int), ("engine", ctypes.c_int), ("mixed_switch_rtol", ctypes.c_double),
+        ("snapshot_every", ctypes.c_int), ("snapshot", ctypes.c_void_p), ("snapshot_user", ctypes.c_void_p),
     ]
 
 

@@ -77,3 +77,35 @@ def test_library_is_not_older_than_its_sources():
     spec.loader.exec_module(mod)
     assert len(mod.DEPS) >= 7
     assert mod.up_to_date(), "libcdft_b200.so is older than its sources: run cdft.jl_b200/build.py"
+
+
+def test_julia_shim_structs_mirror_the_header():
+    """CDFTB200.jl declares the C structs field by field (ccall passes them by value or
+    reference): same fields in the same order as include/cdft_b200.h."""
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    header = open(os.path.join(root, "include", "cdft_b200.h")).read()
+    shim = open(os.path.join(root, "cdft.jl_b200", "julia", "CDFTB200.jl")).read()
+
+    def c_fields(name):
+        end = header.index("} " + name + ";")
+        body = header[header.rindex("typedef struct {", 0, end) + len("typedef struct {"):end]
+        body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+        out = []
+        for decl in body.split(";"):
+            decl = re.sub(r"\[.*?\]", "", decl).replace("*", " ").strip()
+            if not decl:
+                continue
+            toks = [t for t in re.split(r"[\s,]+", decl) if t]
+            skip = 2 if toks[0] in ("const", "unsigned") else 1   # the type ("int icomp, jcomp" declares two)
+            out += toks[skip:]
+        return out
+
+    def jl_fields(name):
+        body = re.search(r"(?:mutable )?struct " + name + r"\n(.*?)\nend", shim, re.S).group(1)
+        return [ln.split("::")[0].strip() for ln in body.splitlines() if "::" in ln and not ln.strip().startswith("#")
+                and "=" not in ln.split("::")[0]]
+
+    for c, jl in (("cdft_system_desc", "CDFTSystemDesc"), ("cdft_solver_opts", "CDFTSolverOpts"),
+                  ("cdft_result", "CDFTResult"), ("cdft_assoc_pair", "CDFTAssocPair")):
+        assert jl_fields(jl) == c_fields(c), (c, jl_fields(jl), c_fields(c))

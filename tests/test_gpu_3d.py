@@ -204,3 +204,30 @@ def test_converge_256_mixed_matches_fp64():
     assert fb == pytest.approx(fa, rel=1e-9)
     s64.close()
     s32.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("N", [32, 64, 128])
+def test_tma_and_fused_passes_equal_plain_kernels(N, precision):
+    """The TMA tile kernels of the y/z passes and the fused x pass (inverse x-FFT, Phi,
+    forward x-FFT in one kernel) compute each line and each point with the arithmetic of
+    the per-stage kernels: dF/drho is identical to the last bit, and a converge takes the
+    same evaluations."""
+    import cdft_b200 as cd
+    sp, _ = _case(N=N, box_sigmas=8.0 if N == 32 else 16.0, nsol=2 if N == 32 else 27, precision=precision)
+    x = np.arange(N) / N
+    smooth = (np.sin(2 * np.pi * x)[None, None, :] * np.cos(4 * np.pi * x)[None, :, None]
+              + 0.5 * np.sin(6 * np.pi * x + 1.0)[:, None, None])
+    rho = cd.initialize_profiles(sp) * (1 + 0.2 * smooth[None])
+    out = {}
+    try:
+        for tma, fused in ((0, 0), (1, 0), (1, 1)):
+            cd.tuning("fft3d_tma", tma)
+            cd.tuning("fft3d_fused_phi", fused)
+            out[(tma, fused)] = cd.dFdrho_res(sp, rho)
+    finally:
+        cd.tuning("fft3d_tma", 1)
+        cd.tuning("fft3d_fused_phi", 1)
+    ref = out[(0, 0)]
+    for k, v in out.items():
+        assert np.array_equal(v, ref), (k, float(np.max(np.abs(v - ref)) / np.max(np.abs(ref))))

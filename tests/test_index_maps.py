@@ -3,9 +3,9 @@ computes them, against direct NumPy results (no GPU).
 
 - `pers_conv_dmma` (csrc/persistent.cuh): the exact circulant convolution of the persistent
   engine as a sum of 8x8 Toeplitz tap blocks times 8-column input slabs on the FP64
-  m8n8k4 tensor-core path.  The forward stage reads the periodically extended copy, the
-  adjoint reads dPhi/dn in place through a branch-free wrapped index; both index ranges are
-  checked against their buffers.
+  m8n8k4 tensor-core path, reading zero-padded taps and the periodically extended input at
+  bank-spread positions; the index ranges are checked against their buffers and the bank
+  pairs of every warp load counted.
 - `fft_lines` / `fft_reg` / the two-rows-in-one packing of `fft_x_r2c` and `fft_x_c2r`
   (csrc/fft3d.cuh): L = R1 R2 two-pass Cooley-Tukey with radix-2 register DFTs.
 """
@@ -16,63 +16,81 @@ PERS_R = 8
 FFT_SPLIT = {32: (4, 8), 64: (8, 8), 128: (8, 16), 256: (16, 16)}   # FftSplit<L>
 
 
-def pers_extn(N):
-    return 2 * N + 32 * (PERS_R + 2)
+PERS_TPAD = 16
 
 
 def pers_off(N):
-    return N + 32
+    return (N + 32 + 15) & ~15
 
 
-def dmma_conv(taps, x, periodic):
+def pers_extn(N):
+    return pers_off(N) + N + 32 * (PERS_R + 1) + 16
+
+
+def pers_pos(k):
+    return k + 4 * (k >> 4)
+
+
+def pers_extp(N):
+    return pers_extn(N) + 4 * ((pers_extn(N) + 15) >> 4)
+
+
+def dmma_conv(taps, x):
     """out[j] = sum_q taps[q] x[(j - q) mod N] as pers_conv_dmma forms it: per warp task
-    (8 output columns u0..u0+7 of 8 outputs each), for d < D two m8n8k4 products
-    A_d[a][c] B_d[c][n] with A_d[a][c] = t(8d + a - c) and B_d[c][n] = x[8(u0 + n - d) + c],
-    c < 4 and c >= 4 in two accumulators."""
+    (8 output columns u0..u0+7 of 8 outputs each), m8n8k4 products A_d B_d with
+    A_d[a][c] = t(8d + a - c) from the zero-padded taps and B_d[c][n] = x[8(u0 + n - d) + c]
+    from the extended input stored at bank-spread positions; tap blocks in pairs into four
+    accumulators.  Every read is checked against its buffer, and the B loads of a warp
+    must hit each 8-byte bank pair at most twice (2 shared-memory wavefronts)."""
     N = len(taps)
     U = (N + 7) // 8
     nut = (U + 7) // 8
     D = (N + 14) // 8
-    EXTN, OFF = pers_extn(N), pers_off(N)
-    ext = np.array([x[(k - OFF) % N] for k in range(EXTN)])
+    EXTN, EXTP, OFF, TS = pers_extn(N), pers_extp(N), pers_off(N), N + 2 * PERS_TPAD
+    ext = np.full(EXTP, np.nan)
+    for k in range(EXTN):
+        ext[pers_pos(k)] = x[(k - OFF) % N]
+    tp = np.zeros(TS)
+    tp[PERS_TPAD:PERS_TPAD + N] = taps
     out = np.zeros(N)
 
-    def t(q):
-        return taps[q] if 0 <= q < N else 0.0
+    def A(q):
+        assert 0 <= q + PERS_TPAD < TS, (N, q)
+        return tp[q + PERS_TPAD]
+
+    def B(xl):
+        assert 0 <= xl < EXTN, (N, xl)
+        v = ext[pers_pos(xl)]
+        assert np.isfinite(v)
+        return v
 
     for ut in range(nut):
         u0 = 8 * ut
-        C0 = np.zeros((8, 8))
-        C1 = np.zeros((8, 8))
-        # lane (r, k): A row r / B column r, A column k / B row k
-        i0 = {(r, k): (8 * (u0 + r) + k) % N for r in range(8) for k in range(4)}
-        for d in range(D):
-            A0 = np.zeros((8, 4))
-            A1 = np.zeros((8, 4))
-            B0 = np.zeros((4, 8))
-            B1 = np.zeros((4, 8))
-            for r in range(8):
-                for k in range(4):
-                    q0 = 8 * d + r - k
-                    A0[r, k] = t(q0)
-                    A1[r, k] = t(q0 - 4)
-                    if periodic:
-                        j0 = i0[(r, k)]
-                        j1 = j0 + 4 - (N if j0 + 4 >= N else 0)
-                        assert 0 <= j0 < N and 0 <= j1 < N, (N, d, r, k, j0, j1)
-                        B0[k, r] = x[j0]
-                        B1[k, r] = x[j1]
-                        j0 -= 8
-                        j0 += N if j0 < 0 else 0
-                        i0[(r, k)] = j0
-                    else:
-                        p = OFF + 8 * (u0 + r) + k - 8 * d
-                        assert 0 <= p and p + 4 < EXTN, (N, d, r, k, p)
-                        B0[k, r] = ext[p]
-                        B1[k, r] = ext[p + 4]
-            C0 += A0 @ B0
-            C1 += A1 @ B1
-        Dm = C0 + C1
+        acc = [np.zeros((8, 8)) for _ in range(4)]
+
+        def step(d, chains):
+            for half, ch in zip((0, 4), chains):
+                Am = np.zeros((8, 4))
+                Bm = np.zeros((4, 8))
+                banks = {}
+                for r in range(8):
+                    for k in range(4):
+                        Am[r, k] = A(8 * d + r - k - half)
+                        xl = OFF + 8 * (u0 + r) + k - 8 * d + half
+                        Bm[k, r] = B(xl)
+                        b = pers_pos(xl) % 16
+                        banks[b] = banks.get(b, 0) + 1
+                assert max(banks.values()) <= 2, (N, d, banks)
+                acc[ch] += Am @ Bm
+
+        d = 0
+        while d + 1 < D:
+            step(d, (0, 1))
+            step(d + 1, (2, 3))
+            d += 2
+        if d < D:
+            step(d, (0, 1))
+        Dm = (acc[0] + acc[1]) + (acc[2] + acc[3])
         for a in range(8):
             for n in range(8):
                 j = 8 * (u0 + n) + a
@@ -82,13 +100,12 @@ def dmma_conv(taps, x, periodic):
 
 
 @pytest.mark.parametrize("N", [8, 9, 15, 16, 17, 64, 100, 186, 257, 400])
-@pytest.mark.parametrize("periodic", [False, True])
-def test_dmma_circulant_index_map(N, periodic):
+def test_dmma_circulant_index_map(N):
     rng = np.random.default_rng(N)
     taps = rng.standard_normal(N)
     x = rng.standard_normal(N)
     ref = np.array([sum(taps[q] * x[(j - q) % N] for q in range(N)) for j in range(N)])
-    got = dmma_conv(taps, x, periodic)
+    got = dmma_conv(taps, x)
     np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
 
 
@@ -243,3 +260,66 @@ def test_taps_table_equals_inverse_dft(N, ktype):
     ref = np.real(np.fft.ifft(spec))
     got = taps_table(N, span, L, ktype, R)
     assert np.max(np.abs(got - ref)) <= 1e-14 * np.max(np.abs(ref))
+
+
+# ---------------------------------------------------------------------------
+# TMA tiles of the strided 3D passes (csrc/fft3d_tma.cuh, tensor maps of
+# make_spectrum_map in csrc/cdft_b200.cu)
+# ---------------------------------------------------------------------------
+def fft_lines_of(fp32, L):
+    return (16 if L * 4 <= 512 else 8) if fp32 else (16 if L * 8 <= 512 else 8)
+
+
+def tma_tile_coords(t, axis, L, LINES):
+    KX = L // 2 + 1
+    NT = (KX + LINES - 1) // LINES
+    kt, r = t % NT, t // NT
+    outer, field = r % L, r // L
+    return 2 * kt * LINES, (0 if axis == 1 else outer), (outer if axis == 1 else 0), field
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+@pytest.mark.parametrize("L", [32, 64, 128, 256])
+@pytest.mark.parametrize("axis", [1, 2])
+def test_tma_tiles_cover_each_spectrum_entry_once(fp32, L, axis):
+    es = 4 if fp32 else 8
+    LINES = fft_lines_of(fp32, L)
+    KX, KXP = L // 2 + 1, L // 2 + 2
+    nfields = 2
+    dims = (2 * KX, L, L, nfields)
+    strides = (2 * KXP * es, 2 * KXP * es * L, 2 * KXP * es * L * L)
+    box = (2 * LINES, L if axis == 1 else 1, 1 if axis == 1 else L, 1)
+    # tensor-map rules: 16-byte strides, box rows a multiple of 16 bytes, box dims <= 256
+    assert all(s % 16 == 0 for s in strides)
+    assert (box[0] * es) % 16 == 0 and max(box) <= 256
+    NT = (KX + LINES - 1) // LINES
+    cover = np.zeros((nfields, L, L, KX), dtype=np.int32)   # [field][z][y][kx]
+    for t in range(nfields * L * NT):
+        c0, c1, c2, c3 = tma_tile_coords(t, axis, L, LINES)
+        assert min(c0, c1, c2, c3) >= 0                         # no negative store coordinate
+        assert (c0 * es) % 16 == 0                              # innermost coordinate on 16 bytes
+        assert c1 + box[1] <= dims[1] and c2 + box[2] <= dims[2] and c3 < dims[3]
+        kx = np.arange(c0 // 2, c0 // 2 + LINES)
+        kx = kx[kx < KX]                                        # past 2 KX: zero-filled, store clipped
+        assert kx.size >= 1
+        if axis == 1:
+            cover[c3, c2, :, kx[0]:kx[-1] + 1] += 1
+        else:
+            cover[c3, :, c1, kx[0]:kx[-1] + 1] += 1
+    assert np.all(cover == 1)
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+@pytest.mark.parametrize("L", [32, 128, 256])
+def test_tma_shared_memory_fits(fp32, L):
+    """fft_tma_smem_*: the tile buffers and mbarriers of the three kernels fit the 227 KB of
+    one block, with the barriers 8-byte aligned and each tile buffer 128-byte aligned."""
+    cs = 8 if fp32 else 16
+    LINES = fft_lines_of(fp32, L)
+    tile = L * LINES * cs
+    assert tile % 128 == 0                     # every tile buffer starts on 128 bytes (tensor copies)
+    slack = 256                                # TMA_SMEM_SLACK: the base is rounded up to 128 bytes
+    for ntiles in (3, 5, 4):
+        off_bar = ntiles * tile + (L // 2) * cs
+        assert off_bar % 8 == 0
+        assert off_bar + 16 + 16 + slack <= 227 * 1024
