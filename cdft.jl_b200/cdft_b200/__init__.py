@@ -29,7 +29,7 @@ __all__ = [
     "DFTSystem", "AASol",
     "initialize_profiles", "converge", "batch_converge", "dFdrho_res", "F_res", "F_ideal",
     "free_energy", "surface_tension", "interfacial_tension", "adsorption", "integrate",
-    "F_res_grad", "grad_params", "dgamma_dtheta",
+    "F_res_grad", "grad_params", "dgamma_dtheta", "batch_integrals", "batch_properties", "grand_potential",
     "CDFTError", "launch_count", "tuning",
 ]
 
@@ -69,6 +69,27 @@ class Steele:
                     V[i] += pre * (0.4 * (sg / zz) ** 10 - (sg / zz) ** 4
                                    - sg ** 4 / (3 * self.delta[s] * (zz + 0.61 * self.delta[s]) ** 3))
         return V / T
+
+    def potential_dtheta(self, model, z, T):
+        """d(V_i / k_B T)/d theta_t on coordinates z, shape (3 nc, nc, N), theta = (sigma_k [A],
+        eps_k/k_B [K], m_k): V_i depends on its own component's parameters through
+        sigma_si = (sigma_s + sigma_i)/2 and eps_si = sqrt(eps_s eps_i) (steele.jl:36-41,49-81)."""
+        nc = len(model)
+        out = np.zeros((3 * nc, nc, z.size))
+        for s in range(len(self.surface)):
+            eps_si = np.sqrt(self.epsilon[s] * model.epsilon)
+            sig_si = (self.sigma[s] + model.sigma) / 2
+            d = self.delta[s]
+            for i in range(nc):
+                sg = sig_si[i]
+                pre = 2 * np.pi * self.rho[s] * eps_si[i] * d
+                for zz in ([z] if self.width == 0 else [z, self.width - z]):
+                    # V = pre A(sg) / T, A = 0.4 sg^12 z^-10 - sg^6 z^-4 - sg^6 / (3 d (z + 0.61 d)^3)
+                    A = 0.4 * sg ** 12 / zz ** 10 - sg ** 6 / zz ** 4 - sg ** 6 / (3 * d * (zz + 0.61 * d) ** 3)
+                    dA = 4.8 * sg ** 11 / zz ** 10 - 6 * sg ** 5 / zz ** 4 - 6 * sg ** 5 / (3 * d * (zz + 0.61 * d) ** 3)
+                    out[3 * i + 0, i] += pre * dA * 0.5e-10 / T          # per Angstrom of sigma_i
+                    out[3 * i + 1, i] += pre * A / T / (2 * model.epsilon[i])
+        return out
 
     def potential_radial(self, model, r, T, lb, ub):
         """V_ext / k_B T on a spherical or cylindrical grid (steele.jl:111-143): the planar
@@ -571,27 +592,58 @@ def F_res(system, rho):
     return out.value
 
 
+def batch_integrals(systems, rhos=None):
+    """The integrals of several systems on the device in one batch (cdft_batch_integrals):
+    per system a dict with F_res and F_ideal (k_B T), int_rho (per component) and int_one.
+    ``rhos`` None takes the profiles the plans hold (right after a converge)."""
+    n = len(systems)
+    nc = systems[0].nc
+    nq = 3 + nc
+    out = np.zeros(n * nq)
+    plans = (ctypes.c_void_p * n)(*[s._plan.value for s in systems])
+    if rhos is None:
+        ptrs = None
+    else:
+        for s, r in zip(systems, rhos):
+            _check_rho(s, r)
+        ptrs = (ctypes.c_void_p * n)(*[r.ctypes.data for r in rhos])
+    _lib.check(_LIB.cdft_batch_integrals(plans, n, ptrs, 0, _lib.dptr(out)))
+    res = []
+    for k in range(n):
+        q = out[k * nq:(k + 1) * nq]
+        res.append({"F_res": float(q[0]), "F_ideal": float(q[1]), "int_rho": q[2:2 + nc].copy(),
+                    "int_one": float(q[2 + nc])})
+    return res
+
+
+def _integrals(system, rho):
+    return batch_integrals([system], [rho])[0]
+
+
 def F_ideal(system, rho):
-    """F_ideal(system, ρ) (BasicIdeal.jl:10-38)."""
-    T = system.structure.conditions[1]
-    f = (N_A * rho * (np.log(rho) - 1.5 * np.log(T) - 1)).sum(axis=0)
-    return integrate(f, system.structure)   # (nc, grid...) summed over components
+    """F_ideal(system, ρ) (BasicIdeal.jl:10-38), on the device."""
+    return _integrals(system, rho)["F_ideal"]
 
 
 def free_energy(system, rho):
-    """free_energy(system, ρ) = F_ideal + F_res (src/utils/base.jl:8-10)."""
-    return F_ideal(system, rho) + F_res(system, rho)
+    """free_energy(system, ρ) = F_ideal + F_res (src/utils/base.jl:8-10), on the device."""
+    q = _integrals(system, rho)
+    return q["F_ideal"] + q["F_res"]
+
+
+def _omega_ex(system, q):
+    s = system.structure
+    p, T = s.conditions
+    mu = system.model.chemical_potential(s.rho_bulk, T)
+    F = q["F_ideal"] + q["F_res"]
+    return F * K_B * T - float(np.dot(mu, q["int_rho"])) + p * q["int_one"]
 
 
 def surface_tension(system, rho):
     """surface_tension(system, ρ) (surface_tension.jl:31-53), J/m^2; the
-    periodic two-interface seed gives twice the tension (callers divide by 2)."""
-    s = system.structure
-    p, T = s.conditions
-    F = free_energy(system, rho)
-    mu = system.model.chemical_potential(s.rho_bulk, T)
-    chem = sum(mu[i] * integrate(rho[i], s) for i in range(system.nc))
-    return F * K_B * T - chem + p * integrate(np.ones(s.grid_shape), s)
+    periodic two-interface seed gives twice the tension (callers divide by 2).
+    The integrals run on the device (cdft_batch_integrals)."""
+    return _omega_ex(system, _integrals(system, rho))
 
 
 def interfacial_tension(system, rho):
@@ -599,11 +651,23 @@ def interfacial_tension(system, rho):
     return surface_tension(system, rho)
 
 
+def _domain_volume(st):
+    return st.volume() if hasattr(st, "volume") else float(np.prod([ub - lb for (lb, ub) in st.bounds]))
+
+
 def adsorption(system, rho):
     """adsorption(system, ρ) (adsorption.jl:26-32), mol/m^3 of the domain."""
-    st = system.structure
-    V = st.volume() if hasattr(st, "volume") else np.prod([ub - lb for (lb, ub) in st.bounds])
-    return np.array([integrate(rho[i], st) / V for i in range(system.nc)])
+    return _integrals(system, rho)["int_rho"] / _domain_volume(system.structure)
+
+
+def batch_properties(systems, rhos=None):
+    """Excess grand potential (surface_tension's numerator, J/m^2 in 1D) and adsorption of
+    several systems from one batched device call."""
+    out = []
+    for sy, q in zip(systems, batch_integrals(systems, rhos)):
+        out.append({"omega_ex": _omega_ex(sy, q), "adsorption": q["int_rho"] / _domain_volume(sy.structure),
+                    "free_energy": q["F_ideal"] + q["F_res"]})
+    return out
 
 
 def F_res_grad(system, rho):
@@ -616,18 +680,40 @@ def F_res_grad(system, rho):
 
 
 def grad_params(system, rho, dmu_dtheta=None, dp_dtheta=None):
-    """d Omega_ex / d(sigma_k [A], eps_k/k_B [K], m_k) at a converged profile, shape
-    (nc, 3), J/m^2 per parameter unit; Omega_ex is surface_tension's numerator.
-    dmu_dtheta (nc, 3nc) and dp_dtheta (3nc) describe how the bulk state moves with
-    the parameters (None: held fixed)."""
+    """d Omega / d(sigma_k [A], eps_k/k_B [K], m_k) at a converged profile, shape (nc, 3),
+    J/m^2 per parameter unit.  Without an external field Omega is surface_tension's
+    numerator; with planar Steele walls it is the grand potential including the wall term
+    (grand_potential), the functional converge! makes stationary.  dmu_dtheta (nc, 3nc) and
+    dp_dtheta (3nc) describe how the bulk state moves with the parameters (None: held fixed)."""
     _check_rho(system, rho)
     nt = 3 * system.nc
     out = np.zeros(nt)
     mu = None if dmu_dtheta is None else np.ascontiguousarray(dmu_dtheta, dtype=float).reshape(system.nc, nt)
     dp = None if dp_dtheta is None else np.ascontiguousarray(dp_dtheta, dtype=float).reshape(nt)
-    _lib.check(_LIB.cdft_grad_params(system._plan, _lib.dptr(rho), None if mu is None else _lib.dptr(mu),
-                                     None if dp is None else _lib.dptr(dp), _lib.dptr(out)))
+    mu_p = None if mu is None else _lib.dptr(mu)
+    dp_p = None if dp is None else _lib.dptr(dp)
+    if system.vext is None:
+        _lib.check(_LIB.cdft_grad_params(system._plan, _lib.dptr(rho), mu_p, dp_p, _lib.dptr(out)))
+    else:
+        st = system.structure
+        if st.nd != 1 or st.coord != "cart" or not all(isinstance(f, Steele) for f in system.external_field):
+            raise NotImplementedError("parameter gradients with external fields: planar Steele walls")
+        z = st.coords(0)
+        T = st.conditions[1]
+        dv = np.ascontiguousarray(sum(f.potential_dtheta(system.model, z, T) for f in system.external_field))
+        _lib.check(_LIB.cdft_grad_params_ext(system._plan, _lib.dptr(rho), mu_p, dp_p, _lib.dptr(dv), _lib.dptr(out)))
     return out.reshape(system.nc, 3)
+
+
+def grand_potential(system, rho):
+    """The grand potential per unit area (1D) that converge! makes stationary, J/m^2:
+    F k_B T + k_B T sum_i int rho_i V_i - sum_i mu_i int rho_i + p int 1 (surface_tension's
+    numerator plus the external-field energy)."""
+    om = surface_tension(system, rho)
+    if system.vext is None:
+        return om
+    T = system.structure.conditions[1]
+    return om + K_B * T * sum(integrate(rho[i] * system.vext[i], system.structure) for i in range(system.nc))
 
 
 def dgamma_dtheta(system, rho):

@@ -33,11 +33,11 @@ LIB_PATH = os.environ.get("CDFT_B200_LIB") or os.path.join(os.path.dirname(os.pa
 EXPORTED = [
     "cdft_plan_create", "cdft_plan_destroy",
     "cdft_functional_derivative", "cdft_functional_derivative_dev",
-    "cdft_free_energy_res", "cdft_phi_pointwise", "cdft_free_energy_res_grad", "cdft_grad_params",
+    "cdft_free_energy_res", "cdft_phi_pointwise", "cdft_free_energy_res_grad", "cdft_grad_params", "cdft_grad_params_ext",
     "cdft_converge", "cdft_converge_dev",
     "cdft_batch_converge", "cdft_batch_converge_dev",
     "cdft_plan_set_stream", "cdft_batch_time_stage", "cdft_functional_derivative_noalloc",
-    "cdft_tuning_get", "cdft_tuning_set",
+    "cdft_tuning_get", "cdft_tuning_set", "cdft_batch_integrals",
     "cdft_launch_count", "cdft_last_error", "cdft_version",
 ]
 
@@ -129,6 +129,7 @@ def load(path=LIB_PATH):
     lib.cdft_phi_pointwise.argtypes = [P, dp, ctypes.c_int, dp, dp]
     lib.cdft_free_energy_res_grad.argtypes = [P, dp, dp]
     lib.cdft_grad_params.argtypes = [P, dp, dp, dp, dp]
+    lib.cdft_grad_params_ext.argtypes = [P, dp, dp, dp, dp, dp]
     lib.cdft_converge.argtypes = [P, dp, ctypes.POINTER(SolverOpts), ctypes.POINTER(Result)]
     lib.cdft_converge_dev.argtypes = [P, P, ctypes.POINTER(SolverOpts), ctypes.POINTER(Result)]
     lib.cdft_batch_converge.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.POINTER(dp),
@@ -138,6 +139,7 @@ def load(path=LIB_PATH):
     lib.cdft_plan_set_stream.argtypes = [P, P]
     lib.cdft_batch_time_stage.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
     lib.cdft_functional_derivative_noalloc.argtypes = [ctypes.POINTER(SystemDesc), P, P, P]
+    lib.cdft_batch_integrals.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.POINTER(P), ctypes.c_int, dp]
     lib.cdft_tuning_get.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]
     lib.cdft_tuning_set.argtypes = [ctypes.c_char_p, ctypes.c_int]
     lib.cdft_launch_count.argtypes = [ctypes.c_int]

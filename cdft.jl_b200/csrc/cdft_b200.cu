@@ -90,6 +90,7 @@ struct cdft_plan {
     void* d_dfield = nullptr;
     double* d_fval = nullptr;
     double* d_mats = nullptr;     // radial: dense weighted-density operators (both stages)
+    double* d_rw = nullptr;       // radial: quadrature weights on the device
     std::vector<double> rw;       // radial: quadrature weights of the integral (angular factor included)
     void* d_spec = nullptr;       // 3D: convolved-field spectra [comp][field][z][y][kx]
     void* d_R = nullptr;          // 3D: spectrum of rho / accumulated adjoint spectrum
@@ -396,6 +397,9 @@ int radial_build(cdft_plan* p)
                     for (int q = 0; q < N; ++q) A1[(size_t)m * N + q] = -A0[(size_t)q * N + m];
             }
         }
+    CU(cudaMalloc(&p->d_rw, (size_t)N * sizeof(double)));
+    CU(cudaMemcpyAsync(p->d_rw, p->rw.data(), (size_t)N * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    S.qw = p->d_rw;
     CU(cudaMalloc(&p->d_mats, mats.size() * sizeof(double)));
     CU(cudaMemcpyAsync(p->d_mats, mats.data(), mats.size() * sizeof(double), cudaMemcpyHostToDevice, p->stream));
     CU(cudaStreamSynchronize(p->stream));
@@ -424,6 +428,7 @@ int plan_build(cdft_plan* p)
     const double L = d.L, T = d.T;
     S.NA = kNA * L * L * L;
     p->dz[0] = (d.bounds[0][1] - d.bounds[0][0]) / N;
+    S.wscale = p->dz[0] / 3.0;
     for (int i = 0; i < nc; ++i) S.cprd[i] = d.mu_res_plus_ln_rhob[i];
     PhiParams& P = S.phi;
     P.nc = nc;
@@ -618,6 +623,7 @@ int plan_build3d(cdft_plan* p)
     const double Lr = d.L;
     S.NA = kNA * Lr * Lr * Lr;
     for (int k = 0; k < 3; ++k) p->dz[k] = (d.bounds[k][1] - d.bounds[k][0]) / L3;
+    S.wscale = (p->dz[0] / 3.0) * (p->dz[1] / 3.0) * (p->dz[2] / 3.0);
     for (int i = 0; i < nc; ++i) S.cprd[i] = d.mu_res_plus_ln_rhob[i];
     fill_phi_params(d, S);
     const size_t ne = (size_t)S.n_elem;
@@ -674,6 +680,7 @@ int plan_build3d(cdft_plan* p)
 
 void plan_free(cdft_plan* p)
 {
+    cudaFree(p->d_rw);
     cudaFree(p->d_mats);
     cudaFree(p->d_taps);
     cudaFree(p->d_taps32);
@@ -1313,7 +1320,16 @@ int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, boo
     std::vector<AAState> st(b->nsys), st1;
     std::vector<int> hist_off(b->nsys, 0);
     bool budget_hit = false, phase2 = false;
-    if (b->mixed) {
+    // 1D Cartesian mixed plans that run on the persistent engine converge in FP64 directly:
+    // there the FP32 circulant (FFMA) is no faster than the FP64 tensor-core one, and the
+    // FP32 phase only adds evaluations.  The FP32 phase pays on the 3D FFT path.
+    bool mixed_fp32 = b->mixed;
+    if (b->mixed && b->nd == 1 && b->coord == CDFT_COORD_CART && opts->engine != CDFT_ENGINE_GRID &&
+        opts->m <= PERS_MAX_M && !(opts->snapshot_every > 0 && opts->snapshot)) {
+        b->cur32 = 0;
+        mixed_fp32 = persistent_smem_need(b) > persistent_smem_limit(b);
+    }
+    if (mixed_fp32) {
         const double sw = opts->mixed_switch_rtol > 0 ? opts->mixed_switch_rtol : 1e-5;
         b->cur32 = 1;
         rc = run_phase(b, opts, std::max(opts->rtol, sw), opts->atol, hist_off, st, t0, &budget_hit);
@@ -1715,6 +1731,46 @@ int cdft_batch_time_stage(cdft_plan* const* plans, int nplans, int stage, int re
     return 0;
 }
 
+int cdft_batch_integrals(cdft_plan* const* plans, int nplans, double* const* rho, int rho_on_device, double* out)
+{
+    g_err_code = 0;
+    if (!plans || nplans <= 0 || !out) return set_error(CDFT_E_INVALID, "invalid argument");
+    std::vector<cdft_plan*> v(plans, plans + nplans);
+    for (int s = 0; s < nplans; ++s)
+        if (!v[s]) return set_error(CDFT_E_INVALID, "plan %d is NULL", s);
+    Batch* b = nullptr;
+    int rc = get_batch(v, &b);
+    if (rc) return rc;
+    b->stream = v[0]->stream;
+    CU(cudaSetDevice(v[0]->device));
+    rc = batch_upload_sys(b);
+    if (rc) return rc;
+    if (rho)
+        for (int s = 0; s < nplans; ++s) {
+            if (!rho[s]) return set_error(CDFT_E_INVALID, "rho %d is NULL", s);
+            CU(cudaMemcpyAsync(v[s]->sys.rho, rho[s], (size_t)v[s]->sys.n_elem * sizeof(double),
+                               rho_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->stream));
+        }
+    if ((rc = clear_kernel_error(b))) return rc;
+    rc = launch_eval_stages<double>(b, nullptr, false);   // weighted densities and Phi, FP64
+    if (rc) return rc;
+    const int nq = 3 + b->nc;
+    double* d_out = nullptr;
+    CU(cudaMalloc(&d_out, sizeof(double) * nq * nplans));
+    integrals_kernel<<<nplans, INTEG_THREADS, 0, b->stream>>>(b->d_sys, v[0]->desc.T, d_out);
+    g_launches += 1;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, sizeof(double) * nq * nplans, cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    cudaFree(d_out);
+    if (e != cudaSuccess) return set_error(CDFT_E_CUDA, "batch integrals: %s", cudaGetErrorString(e));
+    for (int s = 0; s < nplans; ++s) {   // F_res in k_B T per unit area (1D) or total (3D, radial)
+        const double L = v[s]->desc.L;
+        out[(size_t)s * nq] /= L * L * L;
+    }
+    return check_kernel_error(b);
+}
+
 long long cdft_launch_count(int reset)
 {
     const long long v = g_launches;
@@ -1897,14 +1953,18 @@ int cdft_free_energy_res_grad(cdft_plan* plan, const double* rho, double* dF)
     return 0;
 }
 
-int cdft_grad_params(cdft_plan* plan, const double* rho, const double* dmu_dtheta, const double* dp_dtheta,
-                     double* dOmega)
+}  // extern "C"
+
+namespace {
+
+int grad_params_impl(cdft_plan* plan, const double* rho, const double* dmu_dtheta, const double* dp_dtheta,
+                     const double* dvext_dtheta, double* dOmega)
 {
-    g_err_code = 0;
     if (!plan || !rho || !dOmega) return set_error(CDFT_E_INVALID, "NULL argument");
     const cdft_system_desc& d = plan->desc;
-    if (plan->d_vext)
-        return set_error(CDFT_E_UNSUPPORTED, "external fields depend on the parameters and are not differentiated");
+    if (plan->d_vext && !dvext_dtheta)
+        return set_error(CDFT_E_UNSUPPORTED,
+                         "the external field depends on the parameters: pass its derivative (cdft_grad_params_ext)");
     const int nc = d.nc, N = plan->N, np = 3 * nc;
     std::vector<double> dF(np);
     int rc = cdft_free_energy_res_grad(plan, rho, dF.data());
@@ -1929,9 +1989,35 @@ int cdft_grad_params(cdft_plan* plan, const double* rho, const double* dmu_dthet
         if (dmu_dtheta)
             for (int i = 0; i < nc; ++i) v -= dmu_dtheta[(size_t)i * np + t] * nint[i];
         if (dp_dtheta) v += dp_dtheta[t] * one;
+        if (dvext_dtheta)   // k_B T sum_i int rho_i dV_i/dtheta (V in units of k_B T)
+            for (int i = 0; i < nc; ++i) {
+                KSum acc;
+                const double* dv = dvext_dtheta + ((size_t)t * nc + i) * N;
+                for (int k = 1; k <= N; ++k) acc.add(coef(k, N) * rho[(size_t)i * N + k - 1] * dv[k - 1]);
+                v += kB * d.T * acc.value() * plan->dz[0] / 3.0;
+            }
         dOmega[t] = v;
     }
     return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cdft_grad_params(cdft_plan* plan, const double* rho, const double* dmu_dtheta, const double* dp_dtheta,
+                     double* dOmega)
+{
+    g_err_code = 0;
+    return grad_params_impl(plan, rho, dmu_dtheta, dp_dtheta, nullptr, dOmega);
+}
+
+int cdft_grad_params_ext(cdft_plan* plan, const double* rho, const double* dmu_dtheta, const double* dp_dtheta,
+                         const double* dvext_dtheta, double* dOmega)
+{
+    g_err_code = 0;
+    if (!dvext_dtheta) return set_error(CDFT_E_INVALID, "dvext_dtheta is NULL");
+    return grad_params_impl(plan, rho, dmu_dtheta, dp_dtheta, dvext_dtheta, dOmega);
 }
 
 }  // extern "C"

@@ -82,6 +82,8 @@ struct SysDev {
     double* out;                 // scratch output (functional derivative)
     void* adj;                   // 3D: adjoint sum sum_f ±omega_f * dPhi/dn_f per element (T), else nullptr
     const double* mats;          // radial grids: dense operators [(stage*nc + i)*nconv + f][j][q], else nullptr
+    const double* qw;            // radial grids: quadrature weights of the integral, else nullptr (Simpson)
+    double wscale;               // Cartesian grids: product over dimensions of dz / 3 (Simpson)
 };
 
 struct AAState {

@@ -436,7 +436,7 @@ __device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t 
                  : "memory");
 }
 
-#define FUSED_THREADS 256
+#define FUSED_THREADS 512   // Phi runs on two threads per point (hard sphere + association / chain + dispersion)
 #define FUSED_SMEM_MAX 232448   // dynamic shared memory of one block on sm_100
 
 template <typename T, int L, int NC, int LF>
@@ -541,20 +541,30 @@ fft_x_phi_fused(typename V2<T>::t* __restrict__ spec, size_t nspec, const SysDev
         F[(size_t)i * NF * FIELD + p] = T(S.NA * S.rho[(size_t)i * npts + row0 * L + p]);
     }
     __syncthreads();
-    // ---- Phi / dPhi/dn at every point of the block, in place ----
+    // ---- Phi / dPhi/dn at every point of the block, in place, two threads per point ----
+    // items w < FIELD: hard sphere + association (fields 1 .. 5: n2, n3, the vector n2);
+    // items FIELD + p: chain + dispersion (fields 0, 6, 7, 8).  The halves read and write
+    // disjoint fields (phi_grad's PART split), so no barrier sits between them.
     T* dfield = reinterpret_cast<T*>(S.dfield);
-    for (int p = threadIdx.x; p < FIELD; p += blockDim.x) {
+    for (int w = threadIdx.x; w < 2 * FIELD; w += blockDim.x) {
+        const bool first = w < FIELD;
+        const int p = first ? w : w - FIELD;
         T n[NC][NF], g[NC][NF];
 #pragma unroll
         for (int i = 0; i < NC; ++i)
 #pragma unroll
-            for (int a = 0; a < NF; ++a) n[i][a] = F[((size_t)i * NF + a) * FIELD + p];
-        phi_grad<T, NC, 3>(S.phi, n, g);
+            for (int a = 0; a < NF; ++a) {
+                const bool mine = (a >= 1 && a <= 5) == first;
+                n[i][a] = mine ? F[((size_t)i * NF + a) * FIELD + p] : T(1);
+            }
+        if (first) phi_grad<T, NC, 3, false, 1>(S.phi, n, g);
+        else phi_grad<T, NC, 3, false, 2>(S.phi, n, g);
 #pragma unroll
         for (int i = 0; i < NC; ++i) {
 #pragma unroll
-            for (int a = 1; a < NF; ++a) F[((size_t)i * NF + a) * FIELD + p] = g[i][a];
-            dfield[(size_t)i * NF * npts + row0 * L + p] = g[i][0];   // the rho field's dPhi/dn (EL step)
+            for (int a = 1; a < NF; ++a)
+                if ((a >= 1 && a <= 5) == first) F[((size_t)i * NF + a) * FIELD + p] = g[i][a];
+            if (!first) dfield[(size_t)i * NF * npts + row0 * L + p] = g[i][0];   // the rho field (EL step)
         }
     }
     __syncthreads();

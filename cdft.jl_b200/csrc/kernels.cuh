@@ -1069,3 +1069,78 @@ __global__ void to_float_kernel(const double* __restrict__ a, float* __restrict_
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i < n) b[i] = (float)a[i];
 }
+
+// ---------------------------------------------------------------------------
+// Integrals of a system at its current profile, one block per system: the free energies
+// and the amounts that surface_tension (surface_tension.jl:31-53), adsorption
+// (adsorption.jl:26-32) and free_energy (utils/base.jl:8-10) need.  out[(3 + nc) s + q]:
+//   q = 0        sum_j w_j Phi_j          (F_res L^3, k_B T)
+//   q = 1        sum_j w_j f_ideal_j      (F_ideal, k_B T; BasicIdeal.jl:34-38)
+//   q = 2 + i    sum_j w_j rho_ij         (int rho_i)
+//   q = 2 + nc   sum_j w_j                (int 1)
+// w_j: Simpson's 1, 4, 2, ..., 4, 1 per dimension times dz/3 (integrals.jl:17,28-41), or the
+// radial quadrature weights.  Each thread sums with Neumaier's compensation; the block's
+// partial pairs are combined by one thread in a fixed order (deterministic).
+// ---------------------------------------------------------------------------
+#define INTEG_THREADS 256
+struct NSum {
+    double s = 0.0, c = 0.0;
+    __device__ __forceinline__ void add(double x)
+    {
+        const double t = s + x;
+        c += (fabs(s) >= fabs(x)) ? ((s - t) + x) : ((x - t) + s);
+        s = t;
+    }
+};
+
+__device__ __forceinline__ double simpson_coef(int k, int n)   // k = 0 .. n-1
+{
+    return (k == 0 || k == n - 1) ? 1.0 : (((k + 1) & 1) == 0 ? 4.0 : 2.0);
+}
+
+__global__ void __launch_bounds__(INTEG_THREADS)
+integrals_kernel(const SysDev* __restrict__ sys, double T, double* __restrict__ out)
+{
+    const SysDev& S = sys[blockIdx.x];
+    const int nc = S.nc, nq = 3 + nc;
+    const double kNA = 6.02214076e23, lnT = log(T);
+    NSum acc[3 + CDFT_MAX_NC];
+    for (int j = threadIdx.x; j < S.N; j += INTEG_THREADS) {
+        double w;
+        if (S.qw) {
+            w = S.qw[j];
+        } else if (S.nd == 1) {
+            w = simpson_coef(j, S.N) * S.wscale;
+        } else {
+            const int L = S.ngrid[0];
+            const int x = j % L, y = (j / L) % L, z = j / (L * L);
+            w = simpson_coef(x, L) * simpson_coef(y, L) * simpson_coef(z, L) * S.wscale;
+        }
+        acc[0].add(w * S.fval[j]);
+        double fid = 0.0;
+        for (int i = 0; i < nc; ++i) {
+            const double r = S.rho[(size_t)i * S.N + j];
+            fid += kNA * r * (log(r) - 1.5 * lnT - 1.0);
+            acc[2 + i].add(w * r);
+        }
+        acc[1].add(w * fid);
+        acc[2 + nc].add(w);
+    }
+    __shared__ double ps[INTEG_THREADS][3 + CDFT_MAX_NC];
+    __shared__ double pc[INTEG_THREADS][3 + CDFT_MAX_NC];
+    for (int q = 0; q < nq; ++q) {
+        ps[threadIdx.x][q] = acc[q].s;
+        pc[threadIdx.x][q] = acc[q].c;
+    }
+    __syncthreads();
+    if (threadIdx.x < nq) {
+        const int q = threadIdx.x;
+        NSum tot;
+        double comp = 0.0;
+        for (int t = 0; t < INTEG_THREADS; ++t) {
+            tot.add(ps[t][q]);
+            comp += pc[t][q];
+        }
+        out[(size_t)blockIdx.x * nq + q] = tot.s + (tot.c + comp);
+    }
+}

@@ -19,8 +19,10 @@ struct TunedShapes {
     // block per tile with per-thread loads (0); both compute the same arithmetic
     int fft3d_tma = 1;
     // 3D grids: the inverse x pass of the 8 convolved fields, Phi and the forward x pass in one
-    // kernel (1) or three (0); both compute the same arithmetic
-    int fft3d_fused_phi = 1;
+    // kernel (1) or three (0); both compute the same arithmetic.  Measured at 128^3 and 256^3
+    // (FP64 and mixed): the three kernels are faster (the fused block holds 9 fields of its
+    // rows and runs one block per SM), so 0.
+    int fft3d_fused_phi = 0;
 };
 
 static TunedShapes g_tuned;

@@ -47,7 +47,9 @@ extern "C" {
 
 /* arithmetic of the convolutions and of Phi (DFTOptions precision, src/base/devices.jl:29-40) */
 #define CDFT_PREC_FP64 0
-#define CDFT_PREC_MIXED 1    /* FP32 convolutions and Phi; FP64 Anderson, norms, integrals */
+#define CDFT_PREC_MIXED 1    /* FP32 convolutions and Phi; FP64 Anderson, norms, integrals.  A 1D
+                                Cartesian system on the persistent engine converges in FP64 (the
+                                FP32 phase gains nothing there) */
 
 /* One Wertheim association pair, as packed by pack_assoc_params
  * (src/models/DFT/assoc.jl:18-56): site A on component icomp bonds with
@@ -155,6 +157,18 @@ int cdft_functional_derivative_dev(cdft_plan* plan, const double* d_rho, double*
  * compensated FP64 summation). */
 int cdft_free_energy_res(cdft_plan* plan, const double* rho, double* F);
 
+/* The integrals of several systems at given profiles, on the device in one batch:
+ * out[(3 + nc) s + q] for system s, with q = 0 F_res (as cdft_free_energy_res), q = 1
+ * F_ideal (BasicIdeal.jl:10-38, k_B T), q = 2 + i int rho_i, q = 2 + nc int 1 -- the
+ * Simpson rule of src/utils/integrals.jl:17-41 (or the radial quadrature), compensated
+ * FP64 summation.  From them: free_energy = F_ideal + F_res (utils/base.jl:8-10),
+ * surface_tension's numerator F k_B T - sum mu_i int rho_i + p int 1
+ * (surface_tension.jl:31-53) and adsorption int rho_i / V (adsorption.jl:26-32).
+ * rho[s]: the profile of system s in host (rho_on_device = 0) or device memory; rho = NULL
+ * takes the profiles the plans hold (e.g. right after a converge).  The systems must
+ * share nc, dimension, coordinates and precision (as a batch). */
+int cdft_batch_integrals(cdft_plan* const* plans, int nplans, double* const* rho, int rho_on_device, double* out);
+
 /* Pointwise fused Phi and dPhi/dn_alpha at npts points: n and dphi are
  * (npts, NF, nc) column-major (point fastest), fval is (npts).  Replaces
  * the Enzyme kernels δf_fwd_kernel!/δf_rev_kernel! (models.jl:355-411) that
@@ -180,9 +194,20 @@ int cdft_free_energy_res_grad(cdft_plan* plan, const double* rho, double* dF);
  * dmu_dtheta (nc x 3nc, row i = d mu_i / d theta in J/mol) and dp_dtheta (3nc, Pa) are
  * the caller's derivatives of the bulk state the structure was built on (e.g. along
  * phase coexistence); NULL means held fixed.  Plans with an external field are refused
- * (CDFT_E_UNSUPPORTED): V_ext depends on the parameters and is not differentiated. */
+ * (CDFT_E_UNSUPPORTED): V_ext depends on the parameters; cdft_grad_params_ext takes its
+ * derivative. */
 int cdft_grad_params(cdft_plan* plan, const double* rho, const double* dmu_dtheta, const double* dp_dtheta,
                      double* dOmega);
+
+/* cdft_grad_params for plans with an external field (1D Cartesian): the derivative of the
+ * grand potential Omega = F k_B T + k_B T sum_i int rho_i V_i - sum_i mu_i int rho_i + p int 1
+ * (the functional whose stationary point converge! finds; surface_tension.jl:31-53 reports
+ * it without the wall term), which at a converged profile gains
+ * k_B T sum_i int rho_i dV_i/dtheta.  dvext_dtheta[(t*nc + i)*N + k] = d(V_i/k_B T)/d theta_t at
+ * grid point k (e.g. the Steele wall's, steele.jl:49-81, through sigma_sf = (sigma_s +
+ * sigma_i)/2 and eps_sf = sqrt(eps_s eps_i)).  No counterpart in the reference. */
+int cdft_grad_params_ext(cdft_plan* plan, const double* rho, const double* dmu_dtheta, const double* dp_dtheta,
+                         const double* dvext_dtheta, double* dOmega);
 
 /* Converge rho in place.  Replaces converge!(prob::DFTProblem, method::AASol, ρ),
  * src/methods/converge.jl:220-254, running aasol (src/utils/anderson.jl:301-443)

@@ -92,12 +92,15 @@ def _lle_system(model, N, box_sigmas=60.0, T=298.15, p=1e5):
     return cd.DFTSystem(model, st)
 
 
-def test_dgamma_dtheta_water_octane_matches_fd():
+@pytest.mark.parametrize("N", [256, 4096])
+def test_dgamma_dtheta_water_octane_matches_fd(N):
     """d gamma/dtheta (adjoint at the converged profile + coexistence sensitivity) vs
-    central differences of gamma through bulk LLE, converge and surface tension."""
+    central differences of gamma through bulk LLE, converge and surface tension; 4096
+    points over 60 sigma is the differentiation configuration itself.  The difference step
+    is 1e-5 relative: with converge's 1e-12 tolerance (about 1e-10 relative in gamma) a 1e-6
+    step would leave ~5e-5 of noise in the quotient."""
     import cdft_b200 as cd
     pm, _ = S.models(["water", "octane"])
-    N = 256
     kw = dict(beta=0.01, tol=1e-12, anderson_m=5, maxit=20000)
     sys0 = _lle_system(pm, N)
     rho0 = cd.initialize_profiles(sys0)
@@ -120,5 +123,51 @@ def test_dgamma_dtheta_water_octane_matches_fd():
             vals.append(cd.surface_tension(st, r) / 2)
             st.close()
         fd[t] = (vals[0] - vals[1]) / (2 * h)
+    err = np.abs(grad - fd) / np.max(np.abs(fd))
+    assert float(np.max(err)) < 1e-5, (grad, fd)
+
+
+def test_dgrand_potential_dtheta_slit_pore_matches_fd():
+    """Methane in a graphite slit (two Steele walls): d Omega/d theta of the grand potential
+    including the wall energy (the functional converge! makes stationary), with the walls'
+    own dependence on sigma_i and eps_i, against central differences (step 1e-6 relative)
+    through converge at fixed bulk density (mu and p follow the parameters)."""
+    import cdft_b200 as cd
+    pm, _ = S.models(["methane"])
+    T, H, p0, N = 150.0, 3e-9, 1e5, 150
+    rb = pm.stable_density(p0, T, [1.0])
+    s = pm.sigma[0]
+    bounds = [0.7 * s, H - 0.7 * s]
+    kw = dict(beta=0.1, tol=1e-12, anderson_m=5, maxit=20000)
+
+    def build(model):
+        st = cd.Uniform1DCart((model.pressure([rb], T), T), [rb], bounds, N)
+        return cd.DFTSystem(model, st, cd.Steele(["graphite"], H))
+
+    sys0 = build(pm)
+    rho0 = cd.initialize_profiles(sys0)
+    assert cd.converge(sys0, rho0, **kw).errcode == 0
+    theta0 = pm.theta()
+    dmu = np.zeros((1, 3))
+    dp = np.zeros(3)
+    fd = np.zeros(3)
+    for t in range(3):
+        h = 1e-6 * abs(theta0[t])
+        vals, mus, ps = [], [], []
+        for sgn in (1.0, -1.0):
+            th = theta0.copy()
+            th[t] += sgn * h
+            mdl = pm.with_theta(th)
+            mus.append(mdl.chemical_potential([rb], T)[0])
+            ps.append(mdl.pressure([rb], T))
+            st = build(mdl)
+            r = rho0.copy()
+            assert cd.converge(st, r, **kw).errcode in (0, -1)
+            vals.append(cd.grand_potential(st, r))
+            st.close()
+        fd[t] = (vals[0] - vals[1]) / (2 * h)
+        dmu[0, t] = (mus[0] - mus[1]) / (2 * h)
+        dp[t] = (ps[0] - ps[1]) / (2 * h)
+    grad = cd.grad_params(sys0, rho0, dmu, dp).ravel()
     err = np.abs(grad - fd) / np.max(np.abs(fd))
     assert float(np.max(err)) < 1e-5, (grad, fd)

@@ -237,3 +237,47 @@ def test_mixed_dfdrho_close_to_fp64():
     d32 = cd.dFdrho_res(s32, rho)
     for i in range(2):
         assert _rel(d32[i], d64[i]) < 2e-5, _rel(d32[i], d64[i])
+
+
+@pytest.mark.parametrize("case", ["wall", "lle", "sphr", "3d"])
+def test_device_integrals_match_host_quadrature(case):
+    """cdft_batch_integrals (F_res, F_ideal, int rho, int 1 on the device, compensated sums)
+    against the host Simpson / radial quadrature of the same profile and the oracle's
+    surface_tension numerator and adsorption."""
+    import cdft_b200 as cd
+    rng = np.random.default_rng(11)
+    so = None
+    if case == "wall":
+        sp, so = S.methane_wall(N=201)
+        rho = cd.initialize_profiles(sp)
+    elif case == "lle":
+        sp, so = S.water_octane_lle(N=256)
+        rho = S.random_smooth_profile(sp, rng)
+    elif case == "sphr":
+        from oracle import pcsaft_bulk as pb
+        pm, om = S.models(["methane"])
+        rb = pb.density(om, 1e7, 150.0, [1.0])
+        sp = cd.DFTSystem(pm, cd.Uniform1DSphr((1e7, 150.0), [rb], [0.0, 10 * om.sigma[0]], 121),
+                          cd.HardCore(1.5 * om.sigma[0]))
+        rho = cd.initialize_profiles(sp)
+    else:
+        from oracle import pcsaft_bulk as pb
+        pm, om = S.models(["argon"])
+        rb = 0.021e30 / pb.N_A
+        box = 8.0 * om.sigma[0]
+        sp = cd.DFTSystem(pm, cd.Uniform3DCart((1e5, 100.0), [rb], [0.0, box], 32), None)
+        x = np.arange(32) / 32
+        rho = cd.initialize_profiles(sp) * (1 + 0.1 * np.sin(2 * np.pi * x))[None, None, None, :]
+        rho = np.ascontiguousarray(rho)
+    q = cd.batch_integrals([sp], [rho])[0]
+    st = sp.structure
+    T = st.conditions[1]
+    fid = (cd.N_A * rho * (np.log(rho) - 1.5 * np.log(T) - 1)).sum(axis=0)
+    assert q["F_ideal"] == pytest.approx(cd.integrate(fid, st), rel=1e-12)
+    for i in range(sp.nc):
+        assert q["int_rho"][i] == pytest.approx(cd.integrate(rho[i], st), rel=1e-12)
+    assert q["int_one"] == pytest.approx(cd.integrate(np.ones(st.grid_shape), st), rel=1e-12)
+    assert q["F_res"] == pytest.approx(cd.F_res(sp, rho), rel=1e-12)
+    if so is not None:
+        assert cd.surface_tension(sp, rho) == pytest.approx(so.surface_tension(rho), rel=1e-10)
+        assert cd.adsorption(sp, rho) == pytest.approx(so.adsorption(rho), rel=1e-12)

@@ -115,3 +115,20 @@ def test_radial_steele_equals_planar_wall_at_wall_distance(coord, lb_L):
     clamped = zw <= 0.5 * sig_f
     assert clamped.any()
     np.testing.assert_allclose(V[0, clamped], planar(0.5 * sig_f), rtol=1e-12)
+
+
+@pytest.mark.parametrize("width", [0.0, 3.2e-9])
+def test_steele_parameter_derivative_matches_central_differences(width):
+    """Steele.potential_dtheta (the wall's dependence on the fluid's sigma_i and eps_i,
+    steele.jl:36-41,49-81) against central differences of the potential."""
+    import cdft_b200 as cd
+    pm, _ = S.models(["methane"])
+    z = np.linspace(2e-10, 3e-9, 50)
+    wall = cd.Steele(["graphite"], width)
+    d = wall.potential_dtheta(pm, z, 150.0)
+    th = pm.theta()
+    for t in range(3):
+        h = 1e-6 * abs(th[t])
+        e = np.where(np.arange(3) == t, h, 0.0)
+        fd = (wall.potential(pm.with_theta(th + e), z, 150.0) - wall.potential(pm.with_theta(th - e), z, 150.0)) / (2 * h)
+        assert np.max(np.abs(fd - d[t])) <= 1e-8 * max(np.max(np.abs(fd)), 1e-300) + (0.0 if t < 2 else 0.0)
