@@ -365,7 +365,7 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and plain is not None:
         line["plain_fp64_gpu_path"] = plain
     if rank == 0 and args.with3d:
-        line["solutes3d"] = {str(N): solutes3d(N) for N in args.grid3d}
+        line["solutes3d"] = {str(N): solutes3d(N, plain=args.plain) for N in args.grid3d}
     if args.cpu_baseline and rank == 0:
         line["cpu_baseline"] = cpu_baseline(specs, budget_s=args.cpu_budget)
     if dist:
@@ -478,7 +478,7 @@ def solutes3d_run(N, precision, reps=2):
     return out, rho, omega, fluid
 
 
-def solutes3d(N=128, reps=2):
+def solutes3d(N=128, reps=2, plain=True):
     """3D configuration: PC-SAFT argon, 100 K, rho_b = 0.021 A^-3, periodic cubic box of
     edge 16 sigma on N^3 points, 27 hard spherical solutes of radius 1.5 sigma at
     non-overlapping positions (numpy default_rng(0), centre gaps >= 3 sigma + 2 cells),
@@ -487,7 +487,7 @@ def solutes3d(N=128, reps=2):
     the FP64 ones (relative errors; rho over the fluid, V_ext = 0)."""
     r64, rho64, om64, fluid = solutes3d_run(N, "fp64", reps)
     r32, rho32, om32, _ = solutes3d_run(N, "mixed", reps)
-    return {
+    out = {
         "workload": f"solutes3d: argon 100 K, {N}^3 periodic box edge 16 sigma, 27 hard solutes r=1.5 sigma",
         "solver": SOLVER_3D, "fp64": r64, "mixed": r32,
         "mixed_vs_fp64": {
@@ -497,6 +497,16 @@ def solutes3d(N=128, reps=2):
             "speedup_per_iteration": round(r64["ms_per_iteration"] / r32["ms_per_iteration"], 3),
         },
     }
+    if plain:
+        p = plain_fp64_gpu_3d(N)
+        out["plain_fp64_gpu_path"] = p
+        out["speedup_vs_plain_fp64_gpu"] = {
+            "fp64_per_iteration": round(p["ms_per_iteration"] / r64["ms_per_iteration"], 3),
+            "mixed_per_iteration": round(p["ms_per_iteration"] / r32["ms_per_iteration"], 3),
+            "fp64_converge": round(1e3 * p["seconds"] / r64["ms_per_converge"], 3),
+            "mixed_converge": round(1e3 * p["seconds"] / r32["ms_per_converge"], 3),
+        }
+    return out
 
 
 def run_3d_only(args):
@@ -513,6 +523,240 @@ def run_3d_only(args):
             "dtype": "f64" if args.precision == "fp64" else "f32 FFT+Phi / f64 solver",
             "data": "synthetic: seeded solute positions",
             "config": {"workload": f"solutes3d {N}^3", "solver": SOLVER_3D}, "solutes3d": r}
+
+
+# ---------------------------------------------------------------------------
+# The plain FP64 GPU path of the 3D configuration, built with the reference's structure on
+# cuFFT (torch.fft) and PyTorch: every convolution copies its input into a complex buffer,
+# runs a forward and an inverse C2C FFT and keeps the real part (convolve!,
+# src/utils/integrals.jl:88-96) -- rho is transformed again for every field; Phi's gradient
+# comes from automatic differentiation of the pointwise f_res (models.jl:131-186; reverse
+# mode, one pass, where the reference's default runs one forward pass per field); aasol
+# keeps its vectors on the device and solves the small least-squares problem and the QR
+# downdate on the host (anderson.jl:386-416,552-583), one device-host round trip per step.
+# The comparison arm for "plain FP64 GPU path" of the 3D configuration.
+# ---------------------------------------------------------------------------
+def plain3d_params(sy):
+    """The scalars and arrays of a one-component 3D system that the plain path needs."""
+    st = sy.structure
+    lb, ub = st.bounds[0]
+    return dict(N=st.ngrid[0], box=ub - lb, L=sy.L, d=float(sy.size[0] / sy.L), m=float(sy.model.m[0]),
+                s=float(sy.model.sigma_ij[0, 0] / sy.L), eps=float(sy.model.eps_ij[0, 0]), T=st.conditions[1],
+                vext=np.ascontiguousarray(sy.vext[0]), cprd=float(sy.chempot_res[0] + np.log(st.rho_bulk[0])))
+
+
+def plain3d_functional(prm, device="cuda"):
+    """G(x) = clamp(mu_res + ln rho_b - dF/drho[exp x] - V_ext) of the plain path (GFix!,
+    converge.jl:108-153), on torch tensors of shape (N, N, N), grid order (z, y, x)."""
+    import torch
+    from cdft_b200.thermo import _A, _B
+    N, L, d, m = prm["N"], prm["L"], prm["d"], prm["m"]
+    s3 = prm["s"] ** 3
+    eT = prm["eps"] / prm["T"]
+    NA = 6.02214076e23 * L ** 3
+    dev = device
+    w1 = torch.tensor(np.fft.fftfreq(N) * N / prm["box"] * L, dtype=torch.float64, device=dev)
+    KZ, KY, KX = torch.meshgrid(w1, w1, w1, indexing="ij")
+    wb = torch.sqrt(KX * KX + KY * KY + KZ * KZ)
+    zero = wb == 0
+    safe = torch.where(zero, torch.ones_like(wb), wb)
+    two_pi = 2 * np.pi
+
+    def k_dz(R):
+        return (torch.where(zero, torch.full_like(wb, 2 * R), 2 * torch.sin(safe * R) / safe) / two_pi).to(torch.complex128)
+
+    def k_z2dz(R):
+        return (torch.where(zero, torch.full_like(wb, 4 * np.pi * R ** 3 / 3),
+                            4 * np.pi / safe ** 3 * (torch.sin(safe * R) - R * safe * torch.cos(safe * R)))
+                / two_pi ** 3).to(torch.complex128)
+
+    def k_vec(R):
+        core = 4 * np.pi / safe ** 3 * (torch.sin(safe * R) - R * safe * torch.cos(safe * R))
+        return [torch.complex(torch.zeros_like(wb), torch.where(zero, torch.full_like(wb, 4 * np.pi * R), od * core))
+                / two_pi ** 3 for od in (KX, KY, KZ)]
+
+    R = lambda w: two_pi * w * d
+    psi = 1.3862
+    K = [k_dz(R(0.5)), k_z2dz(R(0.5))] + k_vec(R(0.5)) + [k_z2dz(R(1.0)), k_dz(R(1.0)), k_z2dz(R(psi))]
+    sign = [1, 1, -1, -1, -1, 1, 1, 1]   # vector fields enter the adjoint with -= (fields.jl:50-61)
+    A = torch.tensor(np.asarray(_A), dtype=torch.float64, device=dev)
+    B = torch.tensor(np.asarray(_B), dtype=torch.float64, device=dev)
+    wbs = torch.tensor([(j + 1.0) * (j + 3.0) / (j + 2.0) for j in range(16)], dtype=torch.float64, device=dev)
+    vext = torch.from_numpy(prm["vext"]).to(dev)
+    cprd = prm["cprd"]
+
+    def conv(f, k):   # convolve!: C2C forward and inverse FFT, real part
+        return torch.fft.ifftn(torch.fft.fftn(f.to(torch.complex128)) * k).real
+
+    def f_res(n):
+        n0 = n[1] * m / d
+        n1 = 0.5 * n[1] * m
+        n2 = np.pi * n[1] * m * d
+        nv1 = [n[2 + k] * m / d for k in (1, 2, 3)]
+        nv2 = [-2 * np.pi * n[2 + k] * m for k in (1, 2, 3)]
+        n3 = n[2] * m
+        nv1v2 = nv1[0] * nv2[0] + nv1[1] * nv2[1] + nv1[2] * nv2[2]
+        nv2sq = nv2[0] * nv2[0] + nv2[1] * nv2[1] + nv2[2] * nv2[2]
+        dn = 1 - n3
+        log1dn = torch.log(torch.abs(dn))
+        small = torch.abs(n3) < 0.05
+        n3s = torch.where(small, torch.full_like(n3, 0.5), n3)   # closed form only where it is used
+        closed = log1dn / (12 * np.pi * n3s * n3s) + 1 / (12 * np.pi * n3s * dn * dn)
+        ser = torch.zeros_like(n3) + wbs[15]
+        for j in range(14, -1, -1):
+            ser = ser * n3 + wbs[j]
+        bkt = torch.where(small, ser / (12 * np.pi), closed)
+        res = -n0 * log1dn + (n1 * n2 - nv1v2) / dn + (n2 * n2 * n2 / 3 - n2 * nv2sq) * bkt
+        z3 = m * n[6] / 8   # chain (PCSAFT.jl:123-144); (m - 1) = 0 for argon
+        z2 = m * n[6] / d / 8
+        inv1 = 1 / (1 - z3)
+        ydd = inv1 + 1.5 * d * z2 * inv1 * inv1 + 0.5 * d * d * z2 * z2 * inv1 ** 3
+        res = res - n[0] * (m - 1) * torch.log(torch.abs(ydd * (n[7] / (2 * d)) / n[0]))
+        rz = n[8] * (3 / (4 * psi ** 3 * np.pi)) / d ** 3
+        eta = m * rz * d ** 3 * np.pi / 6
+        cij = rz * rz * m * m * s3
+        s1, s2 = cij * eT, cij * eT * eT
+        e2 = eta * eta
+        C1 = 1 + m * (8 * eta - 2 * e2) / (1 - eta) ** 4 + (1 - m) * (20 * eta - 27 * e2 + 12 * eta * e2 - 2 * e2 * e2) / (
+            (1 - eta) ** 2 * (2 - eta) ** 2)
+        c1 = (m - 1) / m
+        c2 = c1 * (m - 2) / m
+        I1 = torch.zeros_like(eta)
+        I2 = torch.zeros_like(eta)
+        for k in range(6, -1, -1):
+            I1 = I1 * eta + (A[k, 0] + c1 * A[k, 1] + c2 * A[k, 2])
+            I2 = I2 * eta + (B[k, 0] + c1 * B[k, 1] + c2 * B[k, 2])
+        return res - 2 * np.pi * I1 * s1 - np.pi * m * I2 * s2 / C1
+
+    def gfix(lnx):   # GFix!: rho = exp(x); ln G = mu + ln rho_b - dF/drho - V_ext, clamp (converge.jl:108-153)
+        rho = torch.exp(lnx)
+        n = [(rho * NA).requires_grad_(True)] + [(conv(rho, k) * NA).requires_grad_(True) for k in K]
+        phi = f_res(n).sum()
+        g = torch.autograd.grad(phi, n)
+        out = g[0].detach()
+        for gf, k, sg in zip(g[1:], K, sign):
+            out = out + sg * conv(gf.detach(), k)
+        return torch.clamp(cprd - out - vext, -100.0, 100.0)
+
+    return gfix
+
+
+def plain_aasol(gfix, x0, m=10, beta=0.1, tol=1e-10, anderson_start=0.1, maxit=2000):
+    """aasol (anderson.jl:301-443; picard_maxit = maxit, picard_beta = beta, Picard
+    tolerances anderson_start) with the vectors on the device -- the history Q and DG as
+    m rows of n contiguous values, the columns of the reference's column-major matrices --
+    and the small triangular solve and the downdate's Householder QR (LAPACK through
+    numpy, downdate_aaqr!, anderson.jl:552-583) on the host.  Returns (x, evaluations, ok)."""
+    import torch
+    import scipy.linalg
+    shape = x0.shape
+    n = x0.numel()
+
+    def G(x):
+        return ((1 - beta) * x + beta * gfix(x.view(shape)).reshape(-1))
+
+    sol = x0.reshape(-1).clone()
+    gx = G(sol)
+    res = gx - sol
+    resnorm = float(torch.linalg.norm(res))
+    up, tolv, ptol = 1e4 * resnorm, tol * resnorm + tol, anderson_start * resnorm + anderson_start
+    evals, k = 1, 0
+    toosoon = resnorm <= tolv
+    if not toosoon:   # Picard warm-up
+        sol = gx.clone()
+        for _ in range(maxit - 1):
+            gx = G(sol)
+            evals += 1
+            res = gx - sol
+            resnorm = float(torch.linalg.norm(res))
+            if resnorm <= ptol or resnorm >= up:
+                break
+            sol = gx.clone()
+        toosoon = resnorm <= tolv
+    Qt = torch.zeros((m, n), dtype=torch.float64, device=x0.device)
+    DGt = torch.zeros((m, n), dtype=torch.float64, device=x0.device)
+    Rm = np.zeros((m, m))
+
+    def point(gx, sol, res):
+        g = G(sol)
+        r = g - sol
+        return g, g - gx, r - res, r, float(torch.linalg.norm(r))
+
+    dg = df = None
+    if not toosoon:
+        sol = gx.clone()
+        k = 1
+        gx, dg, df, res, resnorm = point(gx, sol, res)
+        evals += 1
+    while k < 2 * maxit and resnorm > tolv and not toosoon and resnorm < up:
+        kk = k + 1
+        if kk > m + 1:   # BuildDG!
+            DGt = torch.roll(DGt, -1, dims=0)
+            DGt[m - 1] = dg
+        else:
+            DGt[kk - 2] = dg
+        kq0 = k - 1
+        if kq0 == 0:
+            nv = float(torch.linalg.norm(df))
+            Rm[0, 0] = nv
+            Qt[0] = df / nv
+        else:
+            if kq0 > m - 1:
+                Qx, Rd = np.linalg.qr(Rm[:, 1:m])
+                Rm[:] = 0.0
+                Rm[:m - 1, :m - 1] = Rd
+                Qt[:m - 1] = torch.from_numpy(np.ascontiguousarray(Qx.T)).to(Qt.device) @ Qt
+                Qt[m - 1] = 0.0
+            kq = min(kq0, m - 1)
+            Qk = Qt[:kq]
+            h1 = Qk @ df   # CGS2 (Orthogonalize!, anderson.jl:525-540)
+            v = df - h1 @ Qk
+            h2 = Qk @ v
+            v = v - h2 @ Qk
+            nv = float(torch.linalg.norm(v))
+            Rm[:kq, kq] = (h1 + h2).cpu().numpy()
+            Rm[kq, kq] = nv
+            Qt[kq] = v / nv
+        mk = min(m, k)
+        tres = (Qt[:mk] @ res).cpu().numpy()
+        theta = scipy.linalg.solve_triangular(Rm[:mk, :mk], tres, lower=False)
+        sol = gx - torch.from_numpy(theta).to(gx.device) @ DGt[:mk]
+        k += 1
+        gx, dg, df, res, resnorm = point(gx, sol, res)
+        evals += 1
+    return sol.view(shape), evals, bool(resnorm <= tolv)
+
+
+def plain_fp64_gpu_3d(N):
+    """The reference-structured FP64 GPU path converging the 3D configuration: Anderson
+    iterations per second (fixed-point evaluations over the CUDA-synchronised wall time of
+    the whole solve) and its converged excess grand potential beside ours."""
+    import torch
+    import cdft_b200 as cd
+    sy = _solutes3d_system(N, "fp64")
+    prm = plain3d_params(sy)
+    gfix = plain3d_functional(prm, "cuda")
+    x0 = torch.log(torch.from_numpy(cd.initialize_profiles(sy)[0]).cuda())
+    gfix(x0)   # warm-up (cuFFT plans, allocator)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    x, evals, ok = plain_aasol(gfix, x0, m=SOLVER_3D["anderson_m"], beta=SOLVER_3D["beta"],
+                               tol=SOLVER_3D["tol"], maxit=SOLVER_3D["maxit"])
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t
+    rho = torch.exp(x).cpu().numpy()[None]
+    om_plain = float(cd.surface_tension(sy, rho))
+    rho_ours = cd.initialize_profiles(sy)
+    cd.converge(sy, rho_ours, method=cd.AASol.for_system(None, **SOLVER_3D))
+    om_ours = float(cd.surface_tension(sy, rho_ours))
+    sy.close()
+    return {"iterations_per_s": round(evals / dt, 3), "ms_per_iteration": round(1e3 * dt / evals, 3),
+            "evaluations": evals, "converged": ok, "seconds": round(dt, 3),
+            "omega_ex_rel_diff_vs_ours": abs(om_plain / om_ours - 1),
+            "rho_max_rel_diff_vs_ours": float(np.max(np.abs(rho / rho_ours - 1))),
+            "how": ("reference structure on cuFFT + PyTorch: a C2C FFT pair per convolution (rho transformed "
+                    "again for every field), autograd dPhi/dn, aasol with device vectors and a host-side "
+                    "triangular solve / downdate QR; whole solve timed")}
 
 
 def plain_fp64_gpu(specs):

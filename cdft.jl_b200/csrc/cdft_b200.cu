@@ -1755,10 +1755,15 @@ int cdft_batch_integrals(cdft_plan* const* plans, int nplans, double* const* rho
     rc = launch_eval_stages<double>(b, nullptr, false);   // weighted densities and Phi, FP64
     if (rc) return rc;
     const int nq = 3 + b->nc;
+    int maxn = 1;
+    for (int s = 0; s < nplans; ++s) maxn = std::max(maxn, v[s]->sys.N);
+    const int nchunk = (maxn + INTEG_CHUNK - 1) / INTEG_CHUNK;
     double* d_out = nullptr;
-    CU(cudaMalloc(&d_out, sizeof(double) * nq * nplans));
-    integrals_kernel<<<nplans, INTEG_THREADS, 0, b->stream>>>(b->d_sys, v[0]->desc.T, d_out);
-    g_launches += 1;
+    CU(cudaMalloc(&d_out, sizeof(double) * nq * nplans * (1 + 2 * (size_t)nchunk)));
+    double* d_part = d_out + (size_t)nq * nplans;
+    integrals_kernel<<<dim3(nchunk, nplans), INTEG_THREADS, 0, b->stream>>>(b->d_sys, v[0]->desc.T, d_part, nchunk);
+    integrals_reduce_kernel<<<nplans, 32, 0, b->stream>>>(d_part, nchunk, nq, d_out);
+    g_launches += 2;
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, sizeof(double) * nq * nplans, cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);

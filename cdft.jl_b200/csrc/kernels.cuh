@@ -1079,10 +1079,13 @@ __global__ void to_float_kernel(const double* __restrict__ a, float* __restrict_
 //   q = 2 + i    sum_j w_j rho_ij         (int rho_i)
 //   q = 2 + nc   sum_j w_j                (int 1)
 // w_j: Simpson's 1, 4, 2, ..., 4, 1 per dimension times dz/3 (integrals.jl:17,28-41), or the
-// radial quadrature weights.  Each thread sums with Neumaier's compensation; the block's
-// partial pairs are combined by one thread in a fixed order (deterministic).
+// radial quadrature weights.  Grid (chunks, systems): a block sums INTEG_CHUNK consecutive
+// points of one system, each thread with Neumaier's compensation, and writes the block's
+// (sum, compensation) pair per amount; integrals_reduce_kernel then combines the chunks of
+// a system in chunk order.  The order of every addition is fixed (deterministic).
 // ---------------------------------------------------------------------------
 #define INTEG_THREADS 256
+#define INTEG_CHUNK (INTEG_THREADS * 32)
 struct NSum {
     double s = 0.0, c = 0.0;
     __device__ __forceinline__ void add(double x)
@@ -1098,14 +1101,17 @@ __device__ __forceinline__ double simpson_coef(int k, int n)   // k = 0 .. n-1
     return (k == 0 || k == n - 1) ? 1.0 : (((k + 1) & 1) == 0 ? 4.0 : 2.0);
 }
 
+// part[((s * nchunk + chunk) * nq + q) * 2 + {0, 1}] = (sum, compensation)
 __global__ void __launch_bounds__(INTEG_THREADS)
-integrals_kernel(const SysDev* __restrict__ sys, double T, double* __restrict__ out)
+integrals_kernel(const SysDev* __restrict__ sys, double T, double* __restrict__ part, int nchunk)
 {
-    const SysDev& S = sys[blockIdx.x];
+    const SysDev& S = sys[blockIdx.y];
     const int nc = S.nc, nq = 3 + nc;
     const double kNA = 6.02214076e23, lnT = log(T);
     NSum acc[3 + CDFT_MAX_NC];
-    for (int j = threadIdx.x; j < S.N; j += INTEG_THREADS) {
+    const int j0 = blockIdx.x * INTEG_CHUNK;
+    const int j1 = min(S.N, j0 + INTEG_CHUNK);
+    for (int j = j0 + threadIdx.x; j < j1; j += INTEG_THREADS) {
         double w;
         if (S.qw) {
             w = S.qw[j];
@@ -1141,6 +1147,23 @@ integrals_kernel(const SysDev* __restrict__ sys, double T, double* __restrict__ 
             tot.add(ps[t][q]);
             comp += pc[t][q];
         }
-        out[(size_t)blockIdx.x * nq + q] = tot.s + (tot.c + comp);
+        double* o = part + (((size_t)blockIdx.y * nchunk + blockIdx.x) * nq + q) * 2;
+        o[0] = tot.s;
+        o[1] = tot.c + comp;
     }
+}
+
+// One block per system: out[s * nq + q] from the chunk pairs, in chunk order.
+__global__ void integrals_reduce_kernel(const double* __restrict__ part, int nchunk, int nq, double* __restrict__ out)
+{
+    const int q = threadIdx.x;
+    if (q >= nq) return;
+    NSum tot;
+    double comp = 0.0;
+    for (int c = 0; c < nchunk; ++c) {
+        const double* o = part + (((size_t)blockIdx.x * nchunk + c) * nq + q) * 2;
+        tot.add(o[0]);
+        comp += o[1];
+    }
+    out[(size_t)blockIdx.x * nq + q] = tot.s + (tot.c + comp);
 }
