@@ -331,11 +331,12 @@ class DFTSystem:
                 d.eps[i * nc + j] = model.eps_ij[i, j]
         d.L = self.L
         d.T = T
-        if len(model.assoc) > 1:
-            raise NotImplementedError("one association pair per system is supported")
-        d.n_assoc = len(model.assoc)
-        for i, (eab, kab) in model.assoc.items():
-            d.assoc[0] = _lib.AssocPair(i, i, 1, 1, eab, kab)
+        pairs = model.assoc_pairs()
+        if len(pairs) > _lib.MAX_ASSOC:
+            raise NotImplementedError(f"at most {_lib.MAX_ASSOC} association pairs per system")
+        d.n_assoc = len(pairs)
+        for q, (i, a, j, b, eab, kab) in enumerate(pairs):
+            d.assoc[q] = _lib.AssocPair(i, j, a, b, 1, 1, eab, kab)
         self._vext_buf = None
         if self.vext is not None:
             self._vext_buf = np.ascontiguousarray(self.vext, dtype=np.float64)

@@ -10,7 +10,8 @@ import os
 import numpy as np
 
 MAX_NC = 4
-MAX_ASSOC = 1
+MAX_ASSOC = 8
+MAX_SITES = 8
 MAX_M = 16
 
 OK = 0
@@ -45,6 +46,7 @@ EXPORTED = [
 class AssocPair(ctypes.Structure):
     _fields_ = [
         ("icomp", ctypes.c_int), ("jcomp", ctypes.c_int),
+        ("isite", ctypes.c_int), ("jsite", ctypes.c_int),
         ("n_ia", ctypes.c_int), ("n_jb", ctypes.c_int),
         ("eps_ab", ctypes.c_double), ("kappa_ab", ctypes.c_double),
     ]

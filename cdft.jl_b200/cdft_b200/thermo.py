@@ -39,7 +39,7 @@ class PCSAFT:
     and 2B association ``assoc = {component_index: (eps_AB_K, kappa_AB)}``.
     """
 
-    def __init__(self, components, m, sigma, epsilon, kij=None, assoc=None):
+    def __init__(self, components, m, sigma, epsilon, kij=None, assoc=None, assoc_cross=None):
         self.components = list(components)
         self.m = np.asarray(m, dtype=float)
         self.sigma = np.asarray(sigma, dtype=float) * 1e-10
@@ -50,6 +50,12 @@ class PCSAFT:
         self.sigma_ij = (self.sigma[:, None] + self.sigma[None, :]) / 2
         self.eps_ij = np.sqrt(np.outer(self.epsilon, self.epsilon)) * (1 - k)
         self.assoc = dict(assoc or {})
+        # cross-association {(i, j): (eps_AB_K, kappa_AB)}: site A of i with B of j and A of j
+        # with B of i (two of the reference's pairs, assoc.jl:18-56)
+        self.assoc_cross = {tuple(sorted(k)): tuple(v) for k, v in dict(assoc_cross or {}).items()}
+        for (i, j) in self.assoc_cross:
+            if i == j or i not in self.assoc or j not in self.assoc:
+                raise ValueError("cross-association needs two distinct self-associating components")
 
     def __len__(self):
         return len(self.m)
@@ -65,7 +71,17 @@ class PCSAFT:
     def with_theta(self, theta):
         """Copy of the model with parameters theta (layout of theta())."""
         t = np.asarray(theta, dtype=float).reshape(-1, 3)
-        return PCSAFT(self.components, t[:, 2], t[:, 0], t[:, 1], kij=self.kij, assoc=self.assoc)
+        return PCSAFT(self.components, t[:, 2], t[:, 0], t[:, 1], kij=self.kij, assoc=self.assoc,
+                      assoc_cross=self.assoc_cross)
+
+    def assoc_pairs(self):
+        """Site pairs (icomp, isite, jcomp, jsite, eps_AB, kappa_AB) in pack_assoc_params'
+        order (assoc.jl:18-56): each associating component has sites A (0) and B (1) of the
+        2B scheme; a self pair bonds A_i-B_i, a cross entry A_i-B_j and A_j-B_i."""
+        pairs = [(i, 0, i, 1, e, k) for i, (e, k) in sorted(self.assoc.items())]
+        for (i, j), (e, k) in sorted(self.assoc_cross.items()):
+            pairs += [(i, 0, j, 1, e, k), (j, 0, i, 1, e, k)]
+        return pairs
 
     def length_scale(self):
         return float(self.sigma_ij.max())
@@ -100,13 +116,39 @@ class PCSAFT:
         m2e2s3 = (xx * (self.eps_ij / T) ** 2).sum()
         adisp = -2 * np.pi * tot * I1 * m2es3 - np.pi * tot * mb * C1 * I2 * m2e2s3
         aas = 0.0
-        for i, (eab, kab) in self.assoc.items():
-            # self-associating 2B: X_A = X_B = X, X = 1/(1 + rho_i X Delta)
-            D = self.sigma_ij[i, i] ** 3 * gij(d[i] / 2) * kab * (np.exp(eab / T) - 1)
-            q = rn[i] * D
-            X = 2 / (1 + np.sqrt(1 + 4 * q))
-            aas = aas + x[i] * 2 * (np.log(X) - X / 2 + 0.5)
+        if self.assoc and not self.assoc_cross:
+            for i, (eab, kab) in self.assoc.items():
+                # self-associating 2B: X_A = X_B = X, X = 1/(1 + rho_i X Delta)
+                D = self.sigma_ij[i, i] ** 3 * gij(d[i] / 2) * kab * (np.exp(eab / T) - 1)
+                q = rn[i] * D
+                X = 2 / (1 + np.sqrt(1 + 4 * q))
+                aas = aas + x[i] * 2 * (np.log(X) - X / 2 + 0.5)
+        elif self.assoc:
+            aas = self._assoc_general(rn, x, d, gij, T)
         return tot * (ahc + adisp + aas)
+
+    def _assoc_general(self, rn, x, d, gij, T):
+        """Wertheim with several pairs: X_s = 1/(1 + sum_t rho_c(t) Delta_st X_t) by damped
+        substitution and Newton (complex-step safe), a = sum_i x_i sum_a (ln X - X/2 + 1/2)."""
+        pairs = self.assoc_pairs()
+        sites = sorted({(p[0], p[1]) for p in pairs} | {(p[2], p[3]) for p in pairs})
+        gi = {k: q for q, k in enumerate(sites)}
+        ns = len(sites)
+        dt = complex if np.iscomplexobj(rn) else float
+        K = np.zeros((ns, ns), dtype=dt)   # K[s, t] = rho_c(t) Delta_st
+        for (i, a, j, b, e, k) in pairs:
+            dij = d[i] * d[j] / (d[i] + d[j])
+            D = self.sigma_ij[i, j] ** 3 * gij(dij) * k * (np.exp(e / T) - 1)
+            K[gi[(i, a)], gi[(j, b)]] += rn[j] * D
+            K[gi[(j, b)], gi[(i, a)]] += rn[i] * D
+        X = np.full(ns, 0.9, dtype=dt)
+        for _ in range(5 * ns):
+            X = 0.5 * (X + 1 / (1 + K @ X))
+        for _ in range(12):
+            C = K @ X
+            J = np.diag(1 + C) + X[:, None] * K
+            X = X - np.linalg.solve(J, X * (1 + C) - 1)
+        return sum(x[c] * (np.log(X[q]) - X[q] / 2 + 0.5) for q, (c, _) in enumerate(sites))
 
     def mu_res(self, rho, T):
         """mu_res / kT of every component at molar densities ``rho``."""

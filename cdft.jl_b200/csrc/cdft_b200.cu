@@ -15,6 +15,7 @@
 #include <mutex>
 #include <string>
 #include <vector>
+#include <algorithm>
 
 #include "persistent.cuh"
 #include "fft3d.cuh"
@@ -190,13 +191,34 @@ int validate_desc(const cdft_system_desc* d)
     if (d->ngrid[0] < 2) return set_error(CDFT_E_INVALID, "ngrid[0]=%d < 2", d->ngrid[0]);
     if (!(d->bounds[0][1] > d->bounds[0][0])) return set_error(CDFT_E_INVALID, "bounds must satisfy ub > lb");
     if (!(d->L > 0) || !(d->T > 0)) return set_error(CDFT_E_INVALID, "L and T must be positive");
-    if (d->n_assoc < 0 || d->n_assoc > CDFT_MAX_ASSOC) return set_error(CDFT_E_UNSUPPORTED, "n_assoc=%d (one pair supported)", d->n_assoc);
+    if (d->n_assoc < 0 || d->n_assoc > CDFT_MAX_ASSOC)
+        return set_error(CDFT_E_UNSUPPORTED, "n_assoc=%d out of [0,%d]", d->n_assoc, CDFT_MAX_ASSOC);
     for (int i = 0; i < d->nc; ++i)
         if (!(d->hsd[i] > 0) || !(d->m[i] > 0)) return set_error(CDFT_E_INVALID, "component %d: hsd and m must be positive", i);
-    if (d->n_assoc == 1) {
-        const cdft_assoc_pair& a = d->assoc[0];
-        if (a.icomp < 0 || a.icomp >= d->nc || a.jcomp < 0 || a.jcomp >= d->nc)
-            return set_error(CDFT_E_INVALID, "association pair component out of range");
+    {
+        int keys[2 * CDFT_MAX_ASSOC], mult[2 * CDFT_MAX_ASSOC], nk = 0;
+        for (int p = 0; p < d->n_assoc; ++p) {
+            const cdft_assoc_pair& a = d->assoc[p];
+            if (a.icomp < 0 || a.icomp >= d->nc || a.jcomp < 0 || a.jcomp >= d->nc)
+                return set_error(CDFT_E_INVALID, "association pair %d: component out of range", p);
+            if (a.isite < 0 || a.isite >= 64 || a.jsite < 0 || a.jsite >= 64 || a.n_ia < 1 || a.n_jb < 1)
+                return set_error(CDFT_E_INVALID, "association pair %d: site index or multiplicity out of range", p);
+            if (!(a.kappa_ab >= 0) || !std::isfinite(a.eps_ab))
+                return set_error(CDFT_E_INVALID, "association pair %d: eps_ab and kappa_ab", p);
+            const int ka = a.icomp * 64 + a.isite, kb = a.jcomp * 64 + a.jsite;
+            const int ma = a.n_ia, mb = a.n_jb;
+            for (int e = 0; e < 2; ++e) {
+                const int key = e ? kb : ka, mu = e ? mb : ma;
+                int q = 0;
+                while (q < nk && keys[q] != key) ++q;
+                if (q == nk) { keys[nk] = key; mult[nk++] = mu; }
+                else if (mult[q] != mu)
+                    return set_error(CDFT_E_INVALID, "association site (%d, %d): two multiplicities", key / 64, key % 64);
+            }
+        }
+        if (nk > CDFT_MAX_SITES) return set_error(CDFT_E_UNSUPPORTED, "%d association sites (at most %d)", nk, CDFT_MAX_SITES);
+        if (d->n_assoc > 1 && d->nc < 2)
+            return set_error(CDFT_E_UNSUPPORTED, "several association pairs are supported for mixtures (nc >= 2)");
     }
     if (d->precision != CDFT_PREC_FP64 && d->precision != CDFT_PREC_MIXED)
         return set_error(CDFT_E_INVALID, "precision=%d", d->precision);
@@ -407,6 +429,61 @@ int radial_build(cdft_plan* p)
     return 0;
 }
 
+// Association tables of PhiParams from the descriptor's pairs (pack_assoc_params,
+// assoc.jl:18-56): one pair fills the analytic path's fields, several the general
+// solve's site and pair tables (sites numbered by (component, site) in ascending order).
+static void fill_assoc_params(PhiParams& P, const cdft_system_desc& d)
+{
+    const int nc = d.nc;
+    const double L = d.L, T = d.T;
+    P.has_assoc = d.n_assoc;
+    P.a_ns = 0;
+    auto K_of = [&](const cdft_assoc_pair& a) {
+        const double sg = d.sigma[a.icomp * nc + a.jcomp] / L;
+        return sg * sg * sg * (exp(a.eps_ab / T) - 1.0) * a.kappa_ab;
+    };
+    auto dij_of = [&](const cdft_assoc_pair& a) {
+        const double di = P.d[a.icomp], dj = P.d[a.jcomp];
+        return di * dj / (di + dj);
+    };
+    if (d.n_assoc == 1) {
+        const cdft_assoc_pair& a = d.assoc[0];
+        P.a_ic = a.icomp;
+        P.a_jc = a.jcomp;
+        P.a_nia = a.n_ia;
+        P.a_njb = a.n_jb;
+        P.a_dij = dij_of(a);
+        P.a_K = K_of(a);
+    } else if (d.n_assoc > 1) {
+        int keys[2 * CDFT_MAX_ASSOC], nk = 0;   // key = component * 64 + site
+        for (int p = 0; p < d.n_assoc; ++p) {
+            const int ka = d.assoc[p].icomp * 64 + d.assoc[p].isite, kb = d.assoc[p].jcomp * 64 + d.assoc[p].jsite;
+            for (int key : {ka, kb}) {
+                bool seen = false;
+                for (int q = 0; q < nk; ++q) seen |= keys[q] == key;
+                if (!seen) keys[nk++] = key;
+            }
+        }
+        std::sort(keys, keys + nk);
+        P.a_ns = nk;
+        auto site_of = [&](int key) { return int(std::lower_bound(keys, keys + nk, key) - keys); };
+        for (int p = 0; p < d.n_assoc; ++p) {
+            const cdft_assoc_pair& a = d.assoc[p];
+            const int sa = site_of(a.icomp * 64 + a.isite), sb = site_of(a.jcomp * 64 + a.jsite);
+            P.g_pa[p] = sa;
+            P.g_pb[p] = sb;
+            P.g_sc[sa] = a.icomp;
+            P.g_sc[sb] = a.jcomp;
+            P.g_sm[sa] = a.n_ia;
+            P.g_sm[sb] = a.n_jb;
+            P.g_nia[p] = a.n_ia;
+            P.g_njb[p] = a.n_jb;
+            P.g_dij[p] = dij_of(a);
+            P.g_K[p] = K_of(a);
+        }
+    }
+}
+
 int plan_build(cdft_plan* p)
 {
     if (p->desc.nd == 3) return plan_build3d(p);
@@ -446,18 +523,7 @@ int plan_build(cdft_plan* p)
             P.c1[i * CDFT_MAX_NC + j] = c1;
             P.c2[i * CDFT_MAX_NC + j] = c1 * e / T;
         }
-    P.has_assoc = d.n_assoc;
-    if (d.n_assoc) {
-        const cdft_assoc_pair& a = d.assoc[0];
-        P.a_ic = a.icomp;
-        P.a_jc = a.jcomp;
-        P.a_nia = a.n_ia;
-        P.a_njb = a.n_jb;
-        const double di = P.d[a.icomp], dj = P.d[a.jcomp];
-        P.a_dij = di * dj / (di + dj);
-        const double s = d.sigma[a.icomp * nc + a.jcomp] / L;
-        P.a_K = s * s * s * (exp(a.eps_ab / T) - 1.0) * a.kappa_ab;
-    }
+    fill_assoc_params(P, d);
 
     const size_t ne = (size_t)S.n_elem;
     const size_t ntap = (size_t)S.nconv * nc * N;
@@ -525,18 +591,7 @@ void fill_phi_params(const cdft_system_desc& d, SysDev& S)
             P.c1[i * CDFT_MAX_NC + j] = c1;
             P.c2[i * CDFT_MAX_NC + j] = c1 * e / T;
         }
-    P.has_assoc = d.n_assoc;
-    if (d.n_assoc) {
-        const cdft_assoc_pair& a = d.assoc[0];
-        P.a_ic = a.icomp;
-        P.a_jc = a.jcomp;
-        P.a_nia = a.n_ia;
-        P.a_njb = a.n_jb;
-        const double di = P.d[a.icomp], dj = P.d[a.jcomp];
-        P.a_dij = di * dj / (di + dj);
-        const double sg = d.sigma[a.icomp * nc + a.jcomp] / L;
-        P.a_K = sg * sg * sg * (exp(a.eps_ab / T) - 1.0) * a.kappa_ab;
-    }
+    fill_assoc_params(P, d);
 }
 
 // omega_hat of SWeightedDensity (weighted_densities.jl:48-69) at reduced |omega|
@@ -1823,6 +1878,8 @@ int cdft_free_energy_res_grad(cdft_plan* plan, const double* rho, double* dF)
     const cdft_system_desc& d = plan->desc;
     if (d.nd != 1 || d.coord != CDFT_COORD_CART)
         return set_error(CDFT_E_UNSUPPORTED, "the parameter gradient is implemented for 1D Cartesian grids");
+    if (d.n_assoc > 1)
+        return set_error(CDFT_E_UNSUPPORTED, "the parameter gradient covers one association pair");
     const int nc = d.nc, N = plan->N;
     const double L = d.L, T = d.T;
     // the chain below assumes PC-SAFT's diameter d_i = sigma_i (1 - 0.12 exp(-3 eps_i / T)) and the
@@ -2123,18 +2180,7 @@ extern "C" int cdft_functional_derivative_noalloc(const cdft_system_desc* desc, 
             P.c1[i * CDFT_MAX_NC + j] = c1;
             P.c2[i * CDFT_MAX_NC + j] = c1 * e / T;
         }
-    P.has_assoc = d.n_assoc;
-    if (d.n_assoc) {
-        const cdft_assoc_pair& a = d.assoc[0];
-        P.a_ic = a.icomp;
-        P.a_jc = a.jcomp;
-        P.a_nia = a.n_ia;
-        P.a_njb = a.n_jb;
-        const double di = P.d[a.icomp], dj = P.d[a.jcomp];
-        P.a_dij = di * dj / (di + dj);
-        const double sg = d.sigma[a.icomp * nc + a.jcomp] / L;
-        P.a_K = sg * sg * sg * (exp(a.eps_ab / T) - 1.0) * a.kappa_ab;
-    }
+    fill_assoc_params(P, d);
 
     // task and chunk lists on the host stack (bounded by the size limits)
     ConvTask tasks[1024];

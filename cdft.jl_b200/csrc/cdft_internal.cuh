@@ -49,8 +49,15 @@ struct PhiParams {
     double d[CDFT_MAX_NC];                       // reduced hard-sphere diameters d_i / L
     double c1[CDFT_MAX_NC * CDFT_MAX_NC];        // m_i m_j (sigma_ij/L)^3 eps_ij/T
     double c2[CDFT_MAX_NC * CDFT_MAX_NC];        // c1 * eps_ij/T
-    int has_assoc, a_ic, a_jc;
+    int has_assoc, a_ic, a_jc;                   // has_assoc: number of pairs (1: analytic, >1: general)
     double a_nia, a_njb, a_dij, a_K;             // d_ij (reduced) and (sigma_ij/L)^3 (exp(eps/T)-1) kappa
+    // several pairs (assoc.jl:771-828): sites s < a_ns of component g_sc[s], multiplicity g_sm[s];
+    // pair p bonds site g_pa[p] (multiplicity g_nia[p]) with g_pb[p] (g_njb[p])
+    int a_ns;
+    int g_sc[CDFT_MAX_SITES];
+    double g_sm[CDFT_MAX_SITES];
+    int g_pa[CDFT_MAX_ASSOC], g_pb[CDFT_MAX_ASSOC];
+    double g_nia[CDFT_MAX_ASSOC], g_njb[CDFT_MAX_ASSOC], g_dij[CDFT_MAX_ASSOC], g_K[CDFT_MAX_ASSOC];
 };
 
 struct SysDev {

@@ -5,6 +5,7 @@
 //   f_hc   Sauer-Gross chain          PCSAFT.jl:123-144
 //   f_disp weighted dispersion        PCSAFT.jl:150-211
 //   f_assoc one-pair analytic Wertheim  src/models/DFT/assoc.jl:159-168,702-769
+//   f_assoc with several pairs          assoc.jl:251-413,771-828 (solve), :830-960 (IFT gradient)
 // The reference differentiates f_res with Enzyme (models.jl:355-411, NF*nc
 // forward passes by default).  Here the gradient is a hand-written reverse
 // sweep computed in the same pass as Phi: one evaluation per point gives all
@@ -52,6 +53,115 @@ __device__ __forceinline__ void wb_bracket(double n3, double D, double Lg, doubl
     B = Lg / (c12 * n3 * n3) + 1.0 / (c12 * n3 * D * D);
     dB = -invD / (c12 * n3 * n3) - 2.0 * Lg / (c12 * n3 * n3 * n3)
          - 1.0 / (c12 * n3 * n3 * D * D) + 2.0 / (c12 * n3 * D * D * D);
+}
+
+// Wertheim association with several pairs at one point (assoc.jl:771-828), FP64.
+// Inputs: u_c = n0_c xi_c per component, I = 1/(1 - n3), the mixture n2 and xi of g_hs.
+// X_s by _assoc_solve (:405-413): X0 = 0.9, 5 NS blended substitutions
+// X_s <- (X_s + 1/(1 + C_s(X)))/2 (:251-285), then 5 NS Newton steps on F_s = X_s (1 + C_s) - 1,
+// J_st = (1 + C_s) delta_st + X_s dC_s/dX_t, solved by Gaussian elimination without pivoting;
+// a candidate outside (0, 1) falls back to the plain substitution (:294-385).  Returns
+// f = sum_s u_c(s) n_s (ln X_s - X_s/2 + 1/2) and its gradient in (u, I, n2, xi): the
+// implicit-function derivative at the final X (:830-960, reverse: J^T lambda = df/dX).
+// Not inlined, so the plain functional keeps its own register allocation.
+__device__ __noinline__ double assoc_general(const PhiParams& P, const double* u, double I, double n2m, double xim,
+                                             double* gu, double& gI, double& gn2, double& gxi)
+{
+    const int ns = P.a_ns, np = P.has_assoc;
+    double D[CDFT_MAX_ASSOC], ca[CDFT_MAX_ASSOC], cb[CDFT_MAX_ASSOC];
+    for (int p = 0; p < np; ++p) {
+        const double dij = P.g_dij[p];
+        const double ghs = I + 0.5 * dij * xim * n2m * I * I + dij * dij * n2m * n2m * xim * (I * I * I) / 18.0;
+        D[p] = ghs * P.g_K[p];
+        ca[p] = P.g_njb[p] * u[P.g_sc[P.g_pb[p]]] * D[p];   // coefficient of X_pb in C_pa
+        cb[p] = P.g_nia[p] * u[P.g_sc[P.g_pa[p]]] * D[p];   // coefficient of X_pa in C_pb
+    }
+    double X[CDFT_MAX_SITES], C[CDFT_MAX_SITES];
+    for (int s = 0; s < ns; ++s) X[s] = 0.9;
+    auto fill_C = [&]() {
+        for (int s = 0; s < ns; ++s) C[s] = 0.0;
+        for (int p = 0; p < np; ++p) {
+            C[P.g_pa[p]] += ca[p] * X[P.g_pb[p]];
+            C[P.g_pb[p]] += cb[p] * X[P.g_pa[p]];
+        }
+    };
+    double J[CDFT_MAX_SITES][CDFT_MAX_SITES + 1];
+    auto fill_J = [&]() {   // J | F
+        for (int s = 0; s < ns; ++s) {
+            for (int t = 0; t < ns; ++t) J[s][t] = (s == t) ? 1.0 + C[s] : 0.0;
+            J[s][ns] = X[s] * (1.0 + C[s]) - 1.0;
+        }
+        for (int p = 0; p < np; ++p) {
+            J[P.g_pa[p]][P.g_pb[p]] += X[P.g_pa[p]] * ca[p];
+            J[P.g_pb[p]][P.g_pa[p]] += X[P.g_pb[p]] * cb[p];
+        }
+    };
+    for (int it = 0; it < 5 * ns; ++it) {
+        fill_C();
+        for (int s = 0; s < ns; ++s) X[s] = 0.5 * (X[s] + 1.0 / (1.0 + C[s]));
+    }
+    double dX[CDFT_MAX_SITES];
+    for (int it = 0; it < 5 * ns; ++it) {
+        fill_C();
+        fill_J();
+        for (int k = 0; k < ns; ++k)
+            for (int i = k + 1; i < ns; ++i) {
+                const double f = J[i][k] / J[k][k];
+                for (int j = k + 1; j <= ns; ++j) J[i][j] -= f * J[k][j];
+            }
+        for (int k = ns - 1; k >= 0; --k) {
+            double r = J[k][ns];
+            for (int j = k + 1; j < ns; ++j) r -= J[k][j] * dX[j];
+            dX[k] = r / J[k][k];
+        }
+        for (int s = 0; s < ns; ++s) {
+            const double cand = X[s] - dX[s];
+            X[s] = (cand > 0.0 && cand < 1.0) ? cand : 1.0 / (1.0 + C[s]);
+        }
+    }
+    // value and the adjoint at the final X
+    fill_C();
+    fill_J();
+    double f = 0.0, lam[CDFT_MAX_SITES];
+    for (int c = 0; c < CDFT_MAX_NC; ++c) gu[c] = 0.0;
+    for (int s = 0; s < ns; ++s) {
+        const double h = logabs64(X[s]) - 0.5 * X[s] + 0.5;
+        const double us = u[P.g_sc[s]];
+        f += us * P.g_sm[s] * h;
+        gu[P.g_sc[s]] += P.g_sm[s] * h;
+        lam[s] = us * P.g_sm[s] * (1.0 / X[s] - 0.5);   // df/dX_s, overwritten by lambda
+    }
+    // J^T lambda = df/dX: elimination on the transpose, no pivoting
+    double A[CDFT_MAX_SITES][CDFT_MAX_SITES];
+    for (int s = 0; s < ns; ++s)
+        for (int t = 0; t < ns; ++t) A[s][t] = J[t][s];
+    for (int k = 0; k < ns; ++k)
+        for (int i = k + 1; i < ns; ++i) {
+            const double q = A[i][k] / A[k][k];
+            for (int j = k + 1; j < ns; ++j) A[i][j] -= q * A[k][j];
+            lam[i] -= q * lam[k];
+        }
+    for (int k = ns - 1; k >= 0; --k) {
+        double r = lam[k];
+        for (int j = k + 1; j < ns; ++j) r -= A[k][j] * lam[j];
+        lam[k] = r / A[k][k];
+    }
+    // df/dtheta = explicit - lambda^T dF/dtheta, theta = (u_c, D_p)
+    gI = gn2 = gxi = 0.0;
+    for (int p = 0; p < np; ++p) {
+        const int sa = P.g_pa[p], sb = P.g_pb[p];
+        const int ca_c = P.g_sc[sb], cb_c = P.g_sc[sa];
+        // F_sa gets X_sa * ca[p] * X_sb, F_sb gets X_sb * cb[p] * X_sa
+        const double wa = lam[sa] * X[sa] * X[sb], wb = lam[sb] * X[sb] * X[sa];
+        gu[ca_c] -= wa * P.g_njb[p] * D[p];
+        gu[cb_c] -= wb * P.g_nia[p] * D[p];
+        const double gD = -(wa * P.g_njb[p] * u[ca_c] + wb * P.g_nia[p] * u[cb_c]);
+        const double gg = gD * P.g_K[p], dij = P.g_dij[p];
+        gI += gg * (1.0 + dij * xim * n2m * I + dij * dij * n2m * n2m * xim * I * I / 6.0);
+        gn2 += gg * (0.5 * dij * xim * I * I + dij * dij * n2m * xim * I * I * I / 9.0);
+        gxi += gg * (0.5 * dij * n2m * I * I + dij * dij * n2m * n2m * I * I * I / 18.0);
+    }
+    return f;
 }
 
 // Layout of the parameter gradient of Phi (phi_grad with PG = true): the entries of
@@ -330,7 +440,7 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
     }   // chain and dispersion
 
     // ---------------- association, one pair (assoc.jl:702-769), FP64 ----------------
-    if (PART != 2 && P.has_assoc) {
+    if (PART != 2 && P.has_assoc == 1) {
         const double PI = 3.14159265358979323846, TWO_PI = 2.0 * PI;
         double n2m = 0, n3m = 0, nv2m[ND];
 #pragma unroll
@@ -459,6 +569,71 @@ __device__ __forceinline__ T phi_grad(const PhiParams& P, const T (&n)[NC][6 + N
                 for (int i = 0; i < NC; ++i)
                     if (i == c) gp[PI_::D + i] += gu[s] * du;
             }
+        }
+    }
+    // ---------------- association, several pairs (assoc.jl:771-828), FP64 ----------------
+    // Compiled for mixtures only (plans with one component and several pairs are refused):
+    // the call keeps its own registers, but the caller must save its live values around it,
+    // which would cost the one-component kernels spills they do not need.
+    if constexpr (NC >= 2) if (PART != 2 && P.has_assoc > 1) {
+        const double PI = 3.14159265358979323846, TWO_PI = 2.0 * PI;
+        double n2m = 0, n3m = 0, nv2m[ND];
+#pragma unroll
+        for (int k = 0; k < ND; ++k) nv2m[k] = 0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            n2m += PI * double(n[i][F2]) * P.m[i] * P.d[i];
+            n3m += double(n[i][F3]) * P.m[i];
+#pragma unroll
+            for (int k = 0; k < ND; ++k) nv2m[k] -= TWO_PI * double(n[i][FV + k]) * P.m[i];
+        }
+        if (n2m == 0.0) {   // exact zero (FP32 weighted densities): xi = 1, as in the one-pair path
+#pragma unroll
+            for (int k = 0; k < ND; ++k) nv2m[k] = 0.0;
+        }
+        const double d2m = (n2m == 0.0) ? 1.0 : n2m;
+        double nv2sqm = 0;
+#pragma unroll
+        for (int k = 0; k < ND; ++k) nv2sqm += nv2m[k] * nv2m[k];
+        const double xim = 1.0 - nv2sqm / (d2m * d2m);
+        const double I = 1.0 / (1.0 - n3m);
+        double u[CDFT_MAX_NC], n0c[NC], n2c[NC], sqc[NC], xic[NC];
+        bool zc[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const double f2 = double(n[c][F2]);
+            n0c[c] = f2 / P.d[c];
+            n2c[c] = PI * f2 * P.d[c];
+            zc[c] = (n2c[c] == 0.0);
+            double sq = 0;
+#pragma unroll
+            for (int k = 0; k < ND; ++k) { const double t = -TWO_PI * double(n[c][FV + k]); sq += t * t; }
+            sqc[c] = zc[c] ? 0.0 : sq;
+            if (zc[c]) n2c[c] = 1.0;
+            xic[c] = 1.0 - sqc[c] / (n2c[c] * n2c[c]);
+            u[c] = n0c[c] * xic[c];
+        }
+        double gu[CDFT_MAX_NC], gI, gn2, gxi;
+        phi += T(assoc_general(P, u, I, n2m, xim, gu, gI, gn2, gxi));
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const double g_n0 = gu[c] * xic[c];
+            const double g_xi = gu[c] * n0c[c];
+            const double g_n2 = g_xi * 2.0 * sqc[c] / (n2c[c] * n2c[c] * n2c[c]);
+            g[c][F2] += T(g_n0 / P.d[c] + g_n2 * PI * P.d[c]);
+#pragma unroll
+            for (int k = 0; k < ND; ++k)
+                if (!zc[c]) g[c][FV + k] += T(g_xi * (-2.0 * TWO_PI * TWO_PI * double(n[c][FV + k]) / (n2c[c] * n2c[c])));
+        }
+        const double g_n2m = gn2 + gxi * 2.0 * nv2sqm / (d2m * d2m * d2m);
+        const double g_n3m = gI * I * I;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            g[i][F2] += T(g_n2m * PI * P.m[i] * P.d[i]);
+            g[i][F3] += T(g_n3m * P.m[i]);
+#pragma unroll
+            for (int k = 0; k < ND; ++k)
+                g[i][FV + k] += T(gxi * (-2.0 * nv2m[k] / (d2m * d2m)) * (-TWO_PI * P.m[i]));
         }
     }
     return phi;

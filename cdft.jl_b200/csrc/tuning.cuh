@@ -12,9 +12,10 @@
 struct TunedShapes {
     // persistent engine: a system of at most this many elements (N * nc) runs the Anderson
     // vector slots on one warp (no block barriers); larger systems use the whole block.
-    // Measured on the 64-point isotherm (N = 100..400, m = 5): the whole block is faster at
-    // every size (Anderson section 5.6 vs 10.7 us per evaluation on average), so 0.
-    int pers_warp_aa_max_elem = 0;
+    // Measured on the 64-point isotherm (N = 100..400, m = 5, three-pass Anderson update):
+    // 11.26 ms per batch with 0, 10.74 with 256, 10.67 with 512, 10.66 with 1024, so 1024
+    // (every isotherm system takes the warp path).
+    int pers_warp_aa_max_elem = 1024;
     // 3D grids: the strided y and z FFT passes as persistent TMA tile kernels (1) or as one
     // block per tile with per-thread loads (0); both compute the same arithmetic
     int fft3d_tma = 1;

@@ -17,7 +17,7 @@ using CUDA
 
 const LIB = get(ENV, "CDFT_B200_LIB", joinpath(@__DIR__, "..", "cdft_b200", "libcdft_b200.so"))
 const MAX_NC = 4
-const MAX_ASSOC = 1
+const MAX_ASSOC = 8
 
 """
     B200Device(; mixed = false)
@@ -37,6 +37,8 @@ export B200Device
 struct CDFTAssocPair
     icomp::Cint
     jcomp::Cint
+    isite::Cint
+    jsite::Cint
     n_ia::Cint
     n_jb::Cint
     eps_ab::Cdouble
@@ -123,15 +125,20 @@ function system_desc(system::DFTSystem{<:PCSAFTModel}, vext::Union{Nothing,Array
     end
     ng = ntuple(d -> d <= nd ? Cint(st.ngrid[d]) : Cint(1), 3)
     nassoc = Clapeyron.assoc_pair_length(model)
-    nassoc <= MAX_ASSOC || error("one association pair per system is supported")
-    pairs = if nassoc == 1
+    nassoc <= MAX_ASSOC || error("at most $MAX_ASSOC association pairs per system")
+    empty = CDFTAssocPair(0, 0, 0, 0, 0, 0, 0.0, 0.0)
+    pairs = if nassoc >= 1
         (icomp, jcomp, isite, jsite, epsa, kap, _, _, nsflat, nscum, _) =
             cDFT.pack_assoc_params(model, sp.size ./ cDFT.length_scale(model))
-        ia = nscum[icomp[1]] + isite[1]
-        jb = nscum[jcomp[1]] + jsite[1]
-        (CDFTAssocPair(icomp[1] - 1, jcomp[1] - 1, nsflat[ia], nsflat[jb], epsa[1], kap[1]),)
+        ntuple(MAX_ASSOC) do p
+            p > nassoc && return empty
+            ia = nscum[icomp[p]] + isite[p]
+            jb = nscum[jcomp[p]] + jsite[p]
+            CDFTAssocPair(icomp[p] - 1, jcomp[p] - 1, isite[p] - 1, jsite[p] - 1,
+                          nsflat[ia], nsflat[jb], epsa[p], kap[p])
+        end
     else
-        (CDFTAssocPair(0, 0, 0, 0, 0.0, 0.0),)
+        ntuple(_ -> empty, MAX_ASSOC)
     end
     coord = st isa cDFT.DFTStructByCoord{cDFT.Cartesian} ? 0 :
             st isa cDFT.DFTStructByCoord{cDFT.Spherical} ? 1 :

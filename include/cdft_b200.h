@@ -29,7 +29,9 @@ extern "C" {
 #endif
 
 #define CDFT_MAX_NC 4        /* components per system */
-#define CDFT_MAX_ASSOC 1     /* association pairs per system (one-pair analytic path) */
+#define CDFT_MAX_ASSOC 8     /* association pairs per system: one pair takes the analytic path
+                                (assoc.jl:702-769), two or more the general solve (:771-828) */
+#define CDFT_MAX_SITES 8     /* distinct association sites over all components */
 #define CDFT_MAX_M 16        /* Anderson history depth */
 
 /* error codes */
@@ -52,10 +54,12 @@ extern "C" {
                                 FP32 phase gains nothing there) */
 
 /* One Wertheim association pair, as packed by pack_assoc_params
- * (src/models/DFT/assoc.jl:18-56): site A on component icomp bonds with
- * site B on component jcomp. */
+ * (src/models/DFT/assoc.jl:18-56): site isite of component icomp bonds with
+ * site jsite of component jcomp.  (icomp, isite) names one site: pairs that
+ * share it refer to the same fraction X of non-bonded sites. */
 typedef struct {
     int icomp, jcomp;          /* 0-based */
+    int isite, jsite;          /* 0-based site index within the component */
     int n_ia, n_jb;            /* site multiplicities */
     double eps_ab;             /* epsilon_assoc / k_B, K */
     double kappa_ab;           /* bonding volume (dimensionless) */
@@ -77,7 +81,7 @@ typedef struct {
     double eps[CDFT_MAX_NC * CDFT_MAX_NC];   /* eps_ij / k_B, K, row-major nc x nc */
     double L;                        /* length scale, m (length_scale(model) = max sigma) */
     double T;                        /* temperature, K */
-    int n_assoc;                     /* 0 or 1 */
+    int n_assoc;                     /* 0 .. CDFT_MAX_ASSOC */
     cdft_assoc_pair assoc[CDFT_MAX_ASSOC];
     double mu_res_plus_ln_rhob[CDFT_MAX_NC]; /* species.chempot_res + log(bulk_density), converge.jl:121 */
     const double* vext;              /* external potential / k_B T, (ngrid..., nc); NULL = none */

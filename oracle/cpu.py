@@ -22,12 +22,12 @@ HEADER = os.path.join(HERE, "..", "include", "cdft_b200.h")
 # and runs on the host cores of the GPU machines as well
 FLAGS = ["-O3", "-std=c++17", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared"]
 
-MAX_NC, MAX_ASSOC = 4, 1
+MAX_NC, MAX_ASSOC = 4, 8
 
 
 class AssocPair(ctypes.Structure):
-    _fields_ = [("icomp", ctypes.c_int), ("jcomp", ctypes.c_int), ("n_ia", ctypes.c_int), ("n_jb", ctypes.c_int),
-                ("eps_ab", ctypes.c_double), ("kappa_ab", ctypes.c_double)]
+    _fields_ = [("icomp", ctypes.c_int), ("jcomp", ctypes.c_int), ("isite", ctypes.c_int), ("jsite", ctypes.c_int),
+                ("n_ia", ctypes.c_int), ("n_jb", ctypes.c_int), ("eps_ab", ctypes.c_double), ("kappa_ab", ctypes.c_double)]
 
 
 class SystemDesc(ctypes.Structure):
@@ -90,6 +90,11 @@ def load():
     return _LIB
 
 
+def fn_pairs(so):
+    from .functional import assoc_site_pairs
+    return assoc_site_pairs(so.model)
+
+
 def desc_of(so):
     """cdft_system_desc of an oracle functional.DFTSystem (1D Cartesian); keeps the
     V_ext array alive on the returned object."""
@@ -110,10 +115,12 @@ def desc_of(so):
             d.eps[i * nc + j] = so.eps_ij[i, j]
     d.L = so.L
     d.T = st.T
+    if len(fn_pairs(so)) > 1:
+        raise NotImplementedError("the C++ restatement covers the one-pair association path")
     d.n_assoc = len(so.model.assoc)
     if so.model.assoc:
         ic, jc, eab, kab = so.model.assoc[0]
-        d.assoc[0] = AssocPair(ic, jc, 1, 1, eab, kab)
+        d.assoc[0] = AssocPair(ic, jc, 0, 1, 1, 1, eab, kab)
     vext = None if so.vext is None else np.ascontiguousarray(so.vext, dtype=np.float64)
     d.vext = vext.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if vext is not None else None
     d._keep = vext

@@ -11,7 +11,9 @@ A NumPy FP64 restatement of the reference's converge! path:
 * evaluate/integrate -- weighted_densities.jl:118-164 and :345-385, dispatcher
   src/fields/fields.jl:26-61 (rho field copied / overwrites, vector fields ``-=``)
 * Phi = f_hs + f_hc + f_disp + f_assoc -- FMT.jl:17-46, PCSAFT.jl:110-211,
-  assoc.jl:159-168,702-769 (analytic one-pair association)
+  assoc.jl:159-168,702-769 (analytic one-pair association) and :771-828 with
+  _assoc_solve :405-413 (several pairs: 5 NS blended substitutions, 5 NS safeguarded
+  Newton steps)
 * dPhi/dn -- the reference differentiates with Enzyme forward mode
   (models.jl:377-389); here: complex-step forward derivatives, one per
   (field, component) direction, exact to rounding for these analytic expressions
@@ -113,8 +115,7 @@ class DFTSystem:
         # get_species: mu_res/RT at the bulk density of phase 1 (PCSAFT.jl:65-72)
         self.mu_res = pb.mu_res(model, structure.rho_bulk, T)
         self.chem_pot_res_dens = self.mu_res + np.log(structure.rho_bulk)  # converge.jl:121
-        if len(model.assoc) > 1:
-            raise NotImplementedError("only the one-pair analytic association path is restated")
+        self.assoc_pairs = assoc_site_pairs(model)
         self.fields = self._field_list()
         self.kernels = self._build_kernels()
         self.vext = self._build_vext()
@@ -401,6 +402,81 @@ def _wb_bracket(n3, dn, log1dn, closed_only=False):
     return np.where(small, ser / (12 * np.pi), closed)
 
 
+def assoc_site_pairs(model):
+    """Association site pairs as pack_assoc_params lays them out (assoc.jl:18-56):
+    (icomp, isite, jcomp, jsite, eps_AB, kappa_AB, n_ia, n_jb).  Every associating
+    component carries the two sites of the 2B scheme, A (0) and B (1), one of each; a
+    model entry (i, j, eps, kappa) bonds A_i with B_j and, for i != j, A_j with B_i."""
+    pairs = []
+    for (i, j, eAB, kAB) in model.assoc:
+        pairs.append((i, 0, j, 1, eAB, kAB, 1.0, 1.0))
+        if i != j:
+            pairs.append((j, 0, i, 1, eAB, kAB, 1.0, 1.0))
+    return pairs
+
+
+def _assoc_general(pairs, comp, deltas):
+    """f_assoc with several pairs (assoc.jl:771-828): X_s of every site by _assoc_solve
+    (:405-413) -- X0 = 0.9, 5 NS blended substitutions X <- (X + 1/(1 + C(X)))/2
+    (:251-285), then 5 NS Newton steps on F = X (1 + C) - 1 whose candidate is kept where
+    it lies in (0, 1) and replaced by the plain substitution elsewhere (:294-385) -- then
+    sum_s u_c(s) n_s (ln X_s - X_s/2 + 1/2) with u_c = n0_c xi_c.  Complex-step safe: the
+    derivative of the converged iteration is the implicit-function one the reference
+    registers for Enzyme (:830-960)."""
+    sites = []
+    for (ic, ia, jc, jb, *_rest) in pairs:
+        for key in ((ic, ia), (jc, jb)):
+            if key not in sites:
+                sites.append(key)
+    sites.sort()
+    NS = len(sites)
+    gi = {k: q for q, k in enumerate(sites)}
+    u = [n0 * xi for (n0, xi) in comp]
+    # (site s, partner t, coefficient of X_t in C_s, component of t)
+    terms = []
+    for p, (ic, ia, jc, jb, _e, _k, nia, njb) in enumerate(pairs):
+        sa, sb = gi[(ic, ia)], gi[(jc, jb)]
+        terms.append((sa, sb, njb * u[jc] * deltas[p]))
+        terms.append((sb, sa, nia * u[ic] * deltas[p]))
+    mult = {}
+    for (ic, ia, jc, jb, _e, _k, nia, njb) in pairs:
+        mult[(ic, ia)] = nia
+        mult[(jc, jb)] = njb
+    shape = np.broadcast(*[t[2] for t in terms]).shape
+    dt = complex if any(np.iscomplexobj(t[2]) for t in terms) else float
+    X = [np.full(shape, 0.9, dtype=dt) for _ in range(NS)]
+
+    def C_of(X):
+        C = [np.zeros(shape, dtype=dt) for _ in range(NS)]
+        for (s, t, kst) in terms:
+            C[s] = C[s] + kst * X[t]
+        return C
+
+    for _ in range(5 * NS):
+        C = C_of(X)
+        X = [0.5 * (X[s] + 1.0 / (1.0 + C[s])) for s in range(NS)]
+    for _ in range(5 * NS):
+        C = C_of(X)
+        ss = [1.0 / (1.0 + C[s]) for s in range(NS)]
+        F = np.stack([X[s] * (1.0 + C[s]) - 1.0 for s in range(NS)], axis=-1)
+        J = np.zeros(shape + (NS, NS), dtype=dt)
+        for s in range(NS):
+            J[..., s, s] = 1.0 + C[s]
+        for (s, t, kst) in terms:
+            J[..., s, t] = J[..., s, t] + X[s] * kst
+        dX = np.linalg.solve(J, F[..., None])[..., 0]
+        Xn = []
+        for s in range(NS):
+            cand = X[s] - dX[..., s]
+            ok = (np.real(cand) > 0) & (np.real(cand) < 1)
+            Xn.append(np.where(ok, cand, ss[s]))
+        X = Xn
+    res = 0.0
+    for q, (c, a) in enumerate(sites):
+        res = res + u[c] * mult[(c, a)] * (_logabs(X[q]) - 0.5 * X[q] + 0.5)
+    return res
+
+
 def f_res(n, sys):
     """Pointwise PC-SAFT residual free-energy density (PCSAFT.jl:110-117).
 
@@ -470,10 +546,10 @@ def f_res(n, sys):
         I1 = I1 * etad + (pb.PCSAFT_A[k, 0] + c1 * pb.PCSAFT_A[k, 1] + c2 * pb.PCSAFT_A[k, 2])
         I2 = I2 * etad + (pb.PCSAFT_B[k, 0] + c1 * pb.PCSAFT_B[k, 1] + c2 * pb.PCSAFT_B[k, 2])
     res_disp = -2 * (pi * I1 * s1) - pi * mbar * I2 * s2 / C1
-    # --- f_assoc, one pair (assoc.jl:702-769) ---
+    # --- f_assoc (assoc.jl:702-828) ---
     res_assoc = 0.0
-    if sys.model.assoc:
-        ic, jc, eAB, kAB = sys.model.assoc[0]
+    pairs = getattr(sys, "assoc_pairs", None) or assoc_site_pairs(sys.model)
+    if pairs:
         n2m = 0.0
         n3m = 0.0
         for i in range(nc):
@@ -486,10 +562,12 @@ def f_res(n, sys):
                 v = v - 2 * pi * n[i, FV + k] * m[i]
             nv2sqm = nv2sqm + v * v
         xim = 1.0 - nv2sqm / (n2m * n2m)
-        dij = d[ic] * d[jc] / (d[ic] + d[jc])
         inv1n3 = 1.0 / (1.0 - n3m)
-        ghs = inv1n3 + 0.5 * dij * xim * n2m * inv1n3 ** 2 + dij * dij * n2m * n2m * xim * inv1n3 ** 3 / 18
-        delta = ghs * sys.sigma_red[ic, jc] ** 3 * (np.exp(eAB / T) - 1) * kAB
+
+        def delta_of(ic, jc, eAB, kAB):   # _assoc_delta, assoc.jl:159-168
+            dij = d[ic] * d[jc] / (d[ic] + d[jc])
+            ghs = inv1n3 + 0.5 * dij * xim * n2m * inv1n3 ** 2 + dij * dij * n2m * n2m * xim * inv1n3 ** 3 / 18
+            return ghs * sys.sigma_red[ic, jc] ** 3 * (np.exp(eAB / T) - 1) * kAB
 
         def comp_terms(c):
             n0c = n[c, F2] / d[c]
@@ -500,13 +578,19 @@ def f_res(n, sys):
                 sq = sq + v * v
             return n0c, 1.0 - sq / (n2c * n2c)
 
-        n0i, xii = comp_terms(ic)
-        n0j, xij = comp_terms(jc)
-        kia = n0i * xii * delta
-        kjb = n0j * xij * delta
-        b = 1.0 - kia + kjb
-        Xa = 2 / (b + np.sqrt(b * b + 4 * kia))
-        Xb = 1.0 / (1.0 + kia * Xa)
-        res_assoc = (n0i * xii * (_logabs(Xa) - 0.5 * Xa + 0.5)
-                     + n0j * xij * (_logabs(Xb) - 0.5 * Xb + 0.5))
+        if len(pairs) == 1:   # analytic one-pair solution, assoc.jl:702-769
+            ic, _, jc, _, eAB, kAB, nia, njb = pairs[0]
+            delta = delta_of(ic, jc, eAB, kAB)
+            n0i, xii = comp_terms(ic)
+            n0j, xij = comp_terms(jc)
+            kia = nia * n0i * xii * delta
+            kjb = njb * n0j * xij * delta
+            b = 1.0 - kia + kjb
+            Xa = 2 / (b + np.sqrt(b * b + 4 * kia))
+            Xb = 1.0 / (1.0 + kia * Xa)
+            res_assoc = (n0i * xii * nia * (_logabs(Xa) - 0.5 * Xa + 0.5)
+                         + n0j * xij * njb * (_logabs(Xb) - 0.5 * Xb + 0.5))
+        else:
+            res_assoc = _assoc_general(pairs, [comp_terms(c) for c in range(nc)],
+                                       [delta_of(p[0], p[2], p[4], p[5]) for p in pairs])
     return res_hs + res_hc + res_disp + res_assoc

@@ -17,7 +17,21 @@ PARAMS = {
     "octane": dict(m=3.8176, sigma=3.8373, eps=242.78),
     "water": dict(m=1.0656, sigma=3.0007, eps=366.51, assoc=(2500.7, 0.034868)),
     "argon": dict(m=1.0, sigma=3.4, eps=120.0),
+    "ethanol": dict(m=2.3827, sigma=3.1771, eps=198.24, assoc=(2653.4, 0.032384)),
 }
+
+
+def cross_assoc(P):
+    """Cross-association between every two self-associating components by the Elliott
+    rule: eps_ij = (eps_i + eps_j)/2, kappa_ij sigma_ij^3 = sqrt(kappa_i sigma_i^3 kappa_j sigma_j^3)."""
+    out = {}
+    for i, a in enumerate(P):
+        for j, b in enumerate(P):
+            if j > i and "assoc" in a and "assoc" in b:
+                sij = 0.5 * (a["sigma"] + b["sigma"])
+                k = np.sqrt(a["assoc"][1] * b["assoc"][1]) * (np.sqrt(a["sigma"] * b["sigma"]) / sij) ** 3
+                out[(i, j)] = (0.5 * (a["assoc"][0] + b["assoc"][0]), float(k))
+    return out
 
 
 def models(names):
@@ -29,7 +43,12 @@ def models(names):
     e = [p["eps"] for p in P]
     assoc_pkg = {i: p["assoc"] for i, p in enumerate(P) if "assoc" in p}
     assoc_or = [(i, i, p["assoc"][0], p["assoc"][1]) for i, p in enumerate(P) if "assoc" in p]
-    return cd.PCSAFT(names, m, s, e, assoc=assoc_pkg), pb.PCSAFTModel(names, m, s, e, assoc=assoc_or)
+    cross = cross_assoc(P)
+    assoc_or += [(i, j, e_, k_) for (i, j), (e_, k_) in cross.items()]
+    om = pb.PCSAFTModel(names, m, s, e, assoc=assoc_or)
+    if cross:
+        return cd.PCSAFT(names, m, s, e, assoc=assoc_pkg, assoc_cross=cross), om
+    return cd.PCSAFT(names, m, s, e, assoc=assoc_pkg), om
 
 
 def pair(names, conditions, rho_bulk, bounds, N, kind="uniform", rho_bulk2=None, walls=(), precision="fp64"):
@@ -94,6 +113,17 @@ def water_octane_lle(N=256, box_sigmas=60.0, T=298.15, p=1e5):
     s = om.sigma[0]
     half = box_sigmas * s / 2
     return pair(["water", "octane"], (p, T), list(r1), (-half, half), N, kind="twophase", rho_bulk2=list(r2))
+
+
+def water_ethanol_wall(N=150, x=(0.5, 0.5), p=1e5, T=298.15, width=0.0, precision="fp64"):
+    """Liquid water + ethanol (self- and cross-association: 4 site pairs, the general
+    association path, as the reference's test/test_models.jl:171-188 case) next to a
+    graphite Steele wall on [0.5 sigma_w, 4.5 sigma_w]."""
+    _, om = models(["water", "ethanol"])
+    x = np.asarray(x, dtype=float)
+    rb = x * pb.density(om, p, T, x, "liquid")
+    s = om.sigma[0]
+    return pair(["water", "ethanol"], (p, T), list(rb), (0.5 * s, 4.5 * s), N, walls=(width,), precision=precision)
 
 
 def random_smooth_profile(sysp, rng, amp=0.3):

@@ -6,7 +6,7 @@ compressed ``.npz`` files next to this script.  The ``-m gpu`` tests
 (``tests/test_gpu_configs.py``) build the same systems from the stored inputs and
 compare the CUDA path with these outputs.
 
-    python tests/golden/make_fixtures.py [--only c1,c2,c3,c4,c5] [--jobs 8]
+    python tests/golden/make_fixtures.py [--only c1,c2,c3,c4,c5,a9] [--jobs 8]
 
 Configurations (synthetic state points, explicit PC-SAFT parameters):
 
@@ -26,6 +26,12 @@ Configurations (synthetic state points, explicit PC-SAFT parameters):
   27 hard spherical solutes (radius 1.5 sigma, numpy default_rng(0)); beta 0.1,
   m 10, tol 1e-11 (the FFT path's FP64 residual floor on this box sits near
   1e-12 ||r0||).  The converged profile is stored on every 4th point per axis.
+
+* a9 -- water + ethanol liquid (x = 0.5/0.5, 298.15 K, 1e5 Pa) next to one graphite
+  Steele wall, 150 points on [0.5 sigma_water, 4.5 sigma_water]: self- and
+  cross-association, 4 site pairs, the general association solve (assoc.jl:771-828);
+  beta 0.01, m 5, tol 1e-12.  Not one of the five benchmark configurations: the parity
+  case of the general association path.
 
 Every configuration is converged twice: with the oracle's default White-Bear
 bracket (a 16-term Taylor series for |n3| < 0.05, elsewhere the reference's closed
@@ -50,8 +56,10 @@ PARAMS = {
     "octane": (3.8176, 3.8373, 242.78),
     "water": (1.0656, 3.0007, 366.51),
     "argon": (1.0, 3.4, 120.0),
+    "ethanol": (2.3827, 3.1771, 198.24),
 }
 WATER_ASSOC = (2500.7, 0.034868)
+ASSOC = {"water": WATER_ASSOC, "ethanol": (2653.4, 0.032384)}
 
 ISO_T = 150.0
 ISO_WIDTHS = np.linspace(2e-9, 8e-9, 8)
@@ -64,7 +72,14 @@ def oracle_model(names):
     m = [PARAMS[n][0] for n in names]
     s = [PARAMS[n][1] for n in names]
     e = [PARAMS[n][2] for n in names]
-    assoc = [(i, i, WATER_ASSOC[0], WATER_ASSOC[1]) for i, n in enumerate(names) if n == "water"]
+    assoc = [(i, i, ASSOC[n][0], ASSOC[n][1]) for i, n in enumerate(names) if n in ASSOC]
+    # cross-association between two associating components by the Elliott rule
+    for i, a in enumerate(names):
+        for j, b in enumerate(names):
+            if j > i and a in ASSOC and b in ASSOC:
+                sij = 0.5 * (s[i] + s[j])
+                k = np.sqrt(ASSOC[a][1] * ASSOC[b][1]) * (np.sqrt(s[i] * s[j]) / sij) ** 3
+                assoc.append((i, j, 0.5 * (ASSOC[a][0] + ASSOC[b][0]), float(k)))
     return pb.PCSAFTModel(list(names), m, s, e, assoc=assoc)
 
 
@@ -210,6 +225,23 @@ def case_c4():
         closed_rho_rel_diff=float(np.max(np.abs(rc / rho - 1))), closed_gamma_rel_diff=abs(gc / g - 1), seconds=dt)
 
 
+def case_a9():
+    from oracle import functional as fn, pcsaft_bulk as pb
+    om = oracle_model(["water", "ethanol"])
+    p, T = 1e5, 298.15
+    x = np.array([0.5, 0.5])
+    rb = x * pb.density(om, p, T, x, "liquid")
+    s = om.sigma[0]
+    so = fn.DFTSystem(om, fn.Structure((p, T), rb, [(0.5 * s, 4.5 * s)], (150,)), [fn.SteeleWall.graphite(0.0)])
+    kw = dict(beta=0.01, tol=1e-12, anderson_m=5, maxit=10000)
+    rho, out, dt = _converge(so, kw)
+    rc, outc, _ = _converge(so, kw, closed=True)
+    return "a9_water_ethanol_wall_150", dict(
+        p=p, T=T, x=x, rho_bulk=rb, N=150, rho=rho, errcode=out.errcode, evaluations=len(out.history),
+        adsorption=so.adsorption(rho), omega_ex=_excess_omega(so, rho),
+        closed_errcode=outc.errcode, closed_rho_rel_diff=float(np.max(np.abs(rc / rho - 1))), seconds=dt)
+
+
 def solute_centres(n, radius, box, min_gap, seed=0):
     """n non-overlapping centres in [0, box)^3 by rejection sampling with
     numpy.random.default_rng(seed); minimum-image centre distances >= 2 radius + min_gap."""
@@ -281,7 +313,7 @@ def _run(task):
     if name == "c3":
         res = case_c3_point(arg)
     else:
-        res = {"c1": case_c1, "c2": case_c2, "c4": case_c4, "c5": case_c5}[name]()
+        res = {"c1": case_c1, "c2": case_c2, "c4": case_c4, "c5": case_c5, "a9": case_a9}[name]()
     print(f"{name}{'' if arg is None else arg} done in {time.perf_counter() - t:.1f} s", flush=True)
     return name, res
 
@@ -294,12 +326,12 @@ def save(name, data):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", default="c1,c2,c3,c4,c5")
+    ap.add_argument("--only", default="c1,c2,c3,c4,c5,a9")
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 1)
     args = ap.parse_args()
     want = args.only.split(",")
     # the long single cases first, then the 64 isotherm points fill the other workers
-    tasks = [(c, None) for c in ("c5", "c4", "c2", "c1") if c in want]
+    tasks = [(c, None) for c in ("c5", "c4", "c2", "c1", "a9") if c in want]
     if "c3" in want:
         tasks += [("c3", k) for k in range(len(isotherm_specs()))]
     c3 = []

@@ -67,6 +67,11 @@ int main(void) {{
     assert offs == [_lib.SystemDesc.vext.offset, _lib.SystemDesc.precision.offset,
                     _lib.SystemDesc.mu_res_plus_ln_rhob.offset, _lib.SolverOpts.engine.offset,
                     _lib.Result.history_len.offset]
+    # the oracle's C++ restatement takes the same structs through its own ctypes mirror
+    from oracle import cpu
+    assert sizes == [ctypes.sizeof(cpu.SystemDesc), ctypes.sizeof(cpu.SolverOpts), ctypes.sizeof(cpu.Result),
+                     ctypes.sizeof(cpu.AssocPair)]
+    assert offs[:2] == [cpu.SystemDesc.vext.offset, cpu.SystemDesc.precision.offset]
 
 
 def test_library_is_not_older_than_its_sources():

@@ -101,3 +101,17 @@ def test_white_bear_series_departure_recorded():
     for f in (f1, f2):
         assert np.isfinite(float(f["closed_rho_rel_diff"]))
     assert f3["closed_rho_rel_diff"].shape == (64,)
+
+
+def test_a9_fixture_is_oracle_fixed_point():
+    """Water + ethanol at a graphite wall: the general association path (4 site pairs)."""
+    from oracle import functional as fn
+    f = _load("a9_water_ethanol_wall_150")
+    om = mf.oracle_model(["water", "ethanol"])
+    s = om.sigma[0]
+    so = fn.DFTSystem(om, fn.Structure((float(f["p"]), float(f["T"])), list(f["rho_bulk"]), [(0.5 * s, 4.5 * s)],
+                                       (int(f["N"]),)), [fn.SteeleWall.graphite()])
+    assert len(so.assoc_pairs) == 4
+    assert int(f["errcode"]) == 0
+    assert _fixed_point_residual(so, f["rho"], 0.01) < 1e-12
+    np.testing.assert_allclose(so.adsorption(f["rho"]), f["adsorption"], rtol=1e-13)

@@ -65,20 +65,21 @@ def test_F_res_grad_matches_oracle_fd(case):
     assert float(np.max(err)) < 1e-6, (g, fd)
 
 
-def test_grad_params_refuses_external_fields_and_3d():
-    """V_ext (Steele walls, solutes) depends on the parameters and is not differentiated:
-    cdft_grad_params refuses such plans; the 3D engine has no parameter gradient."""
+def test_grad_params_scope():
+    """Planar Steele walls are differentiated (their dV/dtheta enters the gradient); the
+    3D engine has no parameter gradient and hard solutes no dV/dtheta: both are refused."""
     import cdft_b200 as cd
     from cdft_b200._lib import CDFTError
     sp, _ = S.methane_wall(N=101)
     rho = cd.initialize_profiles(sp)
     cd.F_res_grad(sp, rho)   # F_res itself carries no external field
-    with pytest.raises(CDFTError):
-        cd.grad_params(sp, rho)
+    g = cd.grad_params(sp, rho)
+    assert g.shape == (1, 3) and np.all(np.isfinite(g))
     pm, _ = S.models(["argon"])
     s3 = cd.DFTSystem(pm, cd.Uniform3DCart((1e5, 100.0), [0.021e30 / cd.N_A], [0.0, 8 * 3.4e-10], 32))
     with pytest.raises(CDFTError):
         cd.F_res_grad(s3, cd.initialize_profiles(s3))
+    s3.close()
 
 
 def _lle_system(model, N, box_sigmas=60.0, T=298.15, p=1e5):

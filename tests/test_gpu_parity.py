@@ -281,3 +281,22 @@ def test_device_integrals_match_host_quadrature(case):
     if so is not None:
         assert cd.surface_tension(sp, rho) == pytest.approx(so.surface_tension(rho), rel=1e-10)
         assert cd.adsorption(sp, rho) == pytest.approx(so.adsorption(rho), rel=1e-12)
+
+
+def test_persistent_anderson_warp_and_block_paths_agree():
+    """The persistent engine's Anderson section on one warp (systems up to
+    pers_warp_aa_max_elem elements) and on the whole block reduce in different orders:
+    both reach the oracle's fixed point."""
+    import cdft_b200 as cd
+    sp, so = S.methane_wall(N=201)
+    ro, out = so.converge(cd.initialize_profiles(sp), beta=0.1, tol=1e-13, anderson_m=5)
+    old = cd.tuning("pers_warp_aa_max_elem")
+    try:
+        for thr in (0, 1 << 20):
+            cd.tuning("pers_warp_aa_max_elem", thr)
+            rho = cd.initialize_profiles(sp)
+            res = cd.converge(sp, rho, beta=0.1, tol=1e-13, anderson_m=5, engine="persistent")
+            assert res.errcode == 0
+            assert float(np.max(np.abs(rho / ro - 1))) < 1e-9, thr
+    finally:
+        cd.tuning("pers_warp_aa_max_elem", old)
