@@ -37,6 +37,10 @@ PRESSURES = np.logspace(3, 7, 8)
 N_OF_WIDTH = [int(round(100 + 300 * k / 7)) for k in range(8)]
 SOLVER = dict(beta=0.1, tol=1e-10, anderson_m=5, maxit=10000)
 METHANE = dict(m=[1.0], sigma=[3.7039], epsilon=[150.03])
+# DRAM bytes (read + write) per launch of the dominant kernel, from one ncu capture of the
+# same command (dram__bytes_read.sum + dram__bytes_write.sum; the summaries and commands are
+# in profiles/): the isotherm's persistent_kernel, one launch per step.
+ISO_TRAFFIC_BYTES = 2.126336e6 + 2.9184e4
 FP64_PEAK_NOMINAL_TFLOPS = 37.0   # HGX B200 FP64 / FP64 tensor (datasheet); no measured FP64 peak exists for this pool
 
 
@@ -73,8 +77,9 @@ def build_systems(specs, precision):
     model = cd.PCSAFT(["methane"], **METHANE)
     s = model.sigma[0]
     systems, rho0 = [], []
-    for H, p, N in specs:
-        rb = model.stable_density(p, T_ISO, [1.0])
+    # the stable bulk root of every state point, solved on the device in one launch
+    rbs = cd.bulk_density(model, [p for _, p, _ in specs], T_ISO, [1.0], "stable")
+    for (H, p, N), rb in zip(specs, rbs):
         st = cd.Uniform1DCart((p, T_ISO), [rb], [0.7 * s, H - 0.7 * s], N)
         sy = cd.DFTSystem(model, st, cd.Steele(["graphite"], H), cd.DFTOptions(precision))
         systems.append(sy)
@@ -337,8 +342,9 @@ def run_ours(args, rank, world, local_rank):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
             "e2e_with_setup": {
                 "value": round(n / (ms_setup * 1e-3), 3), "unit": "state points/s", "ms_per_step": round(ms_setup, 2),
-                "how": ("64 x (DFTSystem: host bulk thermodynamics + plan creation with its device kernel "
-                        "tables; initialize_profiles) + batched converge with host arrays, host wall clock")},
+                "how": ("bulk densities of the 64 state points in one device launch, 64 x (DFTSystem: bulk "
+                        "mu_res on the host, plan creation with its device kernel tables; initialize_profiles) "
+                        "+ batched converge with host arrays, host wall clock")},
             "gpu_launches": run["launches"],
             "roofline": {
                 "kernel": ("persistent_kernel (whole batched converge, 1 launch per step; circulant "
@@ -350,7 +356,8 @@ def run_ours(args, rank, world, local_rank):
                 "peak_source": "nominal HGX B200 FP64 tensor (of nominal: MEASURED_PEAKS.json has no FP64 figure)",
                 "unit": "TFLOP/s",
                 "frac": round(achieved / FP64_PEAK_NOMINAL_TFLOPS, 4),
-                "traffic": None,
+                "traffic": ISO_TRAFFIC_BYTES if args.engine != "grid" else None,
+                "traffic_unit": "bytes per launch (ncu, profiles/isotherm64_fp64_persistent_kernel.md)",
                 "algorithmic_flops_per_launch": step_flops,
                 "stage_conv1d": {"ms_per_launch": round(ms_conv.value, 5), "tflops": round(conv_tflops, 3),
                                  "algorithmic_flops_per_launch": flops_conv},

@@ -28,7 +28,7 @@ __all__ = [
     "Uniform1DCyl", "TwoPhase1DCart", "DFTOptions",
     "DFTSystem", "AASol",
     "initialize_profiles", "converge", "batch_converge", "dFdrho_res", "F_res", "F_ideal",
-    "free_energy", "surface_tension", "interfacial_tension", "adsorption", "integrate",
+    "free_energy", "surface_tension", "interfacial_tension", "adsorption", "integrate", "ddft_rhs", "ddft_problem", "bulk_density",
     "F_res_grad", "grad_params", "dgamma_dtheta", "batch_integrals", "batch_properties", "grand_potential",
     "CDFTError", "launch_count", "tuning",
 ]
@@ -531,6 +531,67 @@ def dFdrho_res(system, rho):
     return out
 
 
+def bulk_density(model, p, T, x=None, phase="stable"):
+    """Molar densities (mol/m^3) at pressures ``p`` (scalar or array, Pa), temperature T and
+    mole fractions ``x`` (one composition, or one row per pressure), solved on the device in
+    one launch (cdft_bulk_density): "stable" (the lower-Gibbs-energy root, as
+    PCSAFT.stable_density and Clapeyron's volume(model, p, T, x)), "liquid" (densest root)
+    or "vapour" (most dilute).  Models with cross-association are refused (use
+    PCSAFT.stable_density)."""
+    p = np.atleast_1d(np.asarray(p, dtype=np.float64))
+    n = p.size
+    nc = len(model)
+    x = np.ones(nc) if x is None else np.asarray(x, dtype=np.float64)
+    x = np.ascontiguousarray(np.broadcast_to(x.reshape(-1, nc), (n, nc)))
+    d = _lib.SystemDesc()
+    d.nc = nc
+    size = model.d(T)
+    for i in range(nc):
+        d.m[i] = model.m[i]
+        d.hsd[i] = size[i]
+        for j in range(nc):
+            d.sigma[i * nc + j] = model.sigma_ij[i, j]
+            d.eps[i * nc + j] = model.eps_ij[i, j]
+    d.L = model.length_scale()
+    d.T = T
+    pairs = model.assoc_pairs()
+    d.n_assoc = len(pairs)
+    for q, (i, a, j, b, eab, kab) in enumerate(pairs):
+        d.assoc[q] = _lib.AssocPair(i, j, a, b, 1, 1, eab, kab)
+    rho = np.empty(n)
+    status = np.zeros(n, dtype=np.int32)
+    code = {"stable": 0, "liquid": 1, "vapour": 2}[phase]
+    _lib.check(_LIB.cdft_bulk_density(ctypes.byref(d), n, _lib.dptr(p), _lib.dptr(x), code, _lib.dptr(rho),
+                                      status.ctypes.data_as(ctypes.c_void_p)))
+    if np.any(status != 0):
+        raise ValueError(f"no density root at pressures {p[status != 0]}")
+    return rho
+
+
+def ddft_rhs(system, eta):
+    """The right-hand side of dynamic DFT in eta = ln rho, the function ddft_rhs_log! that
+    SciMLBase.ODEProblem(system, ρ, tspan) integrates (ext/SciMLBasecDFTExt.jl:10-61):
+    lap(eta) + lap(mu) + grad eta . (grad eta + grad mu), mu = dF/drho_res + V_ext, rho =
+    exp(clamp(eta, -50, 30)), spectral derivatives in reduced lengths; shape (nc, grid...)."""
+    eta = np.ascontiguousarray(eta, dtype=np.float64)
+    _check_rho(system, eta)
+    out = np.empty_like(eta)
+    _lib.check(_LIB.cdft_ddft_rhs(system._plan, _lib.dptr(eta), _lib.dptr(out)))
+    return out
+
+
+def ddft_problem(system, rho, tspan):
+    """SciMLBase.ODEProblem(system, ρ, tspan) (ext/SciMLBasecDFTExt.jl:10-61) as the triple
+    (f, u0, tspan): f(u, t) -> du/dt with u = ln rho, u0 = log(rho); any ODE integrator
+    (scipy.integrate.solve_ivp on the raveled state, say) takes it from here."""
+    shape = np.shape(rho)
+
+    def f(u, t=None):
+        return ddft_rhs(system, np.reshape(u, shape)).reshape(np.shape(u))
+
+    return f, np.log(np.asarray(rho, dtype=np.float64)), tuple(tspan)
+
+
 def phi_pointwise(system, n):
     """Fused Phi and dPhi/dn at points; n has shape (nc, NF, npts)."""
     n = np.ascontiguousarray(n, dtype=np.float64)
@@ -706,15 +767,49 @@ def grad_params(system, rho, dmu_dtheta=None, dp_dtheta=None):
     return out.reshape(system.nc, 3)
 
 
-def grand_potential(system, rho):
+def grand_potential(system, rho, quadrature="simpson"):
     """The grand potential per unit area (1D) that converge! makes stationary, J/m^2:
-    F k_B T + k_B T sum_i int rho_i V_i - sum_i mu_i int rho_i + p int 1 (surface_tension's
-    numerator plus the external-field energy)."""
-    om = surface_tension(system, rho)
-    if system.vext is None:
-        return om
+    F k_B T + R T sum_i int rho_i V_i - sum_i mu_i int rho_i + p int 1 (surface_tension's
+    numerator plus the external-field energy; rho in mol/m^3, V in k_B T).
+    quadrature "simpson": the weights of surface_tension (integrals.jl:28-41); "uniform":
+    the weights dz of the discrete functional whose gradient the pointwise Euler-Lagrange
+    equation is -- the converged profile is its exact stationary point, and grad_params is
+    its exact parameter derivative."""
     T = system.structure.conditions[1]
-    return om + K_B * T * sum(integrate(rho[i] * system.vext[i], system.structure) for i in range(system.nc))
+    if quadrature == "simpson":
+        om = surface_tension(system, rho)
+        if system.vext is None:
+            return om
+        return om + N_A * K_B * T * sum(integrate(rho[i] * system.vext[i], system.structure)
+                                        for i in range(system.nc))
+    if quadrature != "uniform":
+        raise ValueError("quadrature is 'simpson' or 'uniform'")
+    st = system.structure
+    if st.nd != 1 or st.coord != "cart":
+        raise NotImplementedError("the uniform quadrature is defined for 1D Cartesian grids")
+    lb, ub = st.bounds[0]
+    dz = (ub - lb) / st.ngrid[0]
+    p, _ = st.conditions
+    mu = system.model.chemical_potential(st.rho_bulk, T)
+    # F_res by the device (Simpson) is not what is needed here: the uniform sum of Phi
+    n_pts = st.ngrid[0]
+    f_res = _uniform_F_res(system, rho)
+    f_id = sum(float(np.sum(N_A * rho[i] * (np.log(rho[i]) - 1.5 * np.log(T) - 1))) for i in range(system.nc)) * dz
+    om = (f_res + f_id) * K_B * T - sum(mu[i] * float(np.sum(rho[i])) * dz for i in range(system.nc)) + p * n_pts * dz
+    if system.vext is not None:
+        om += N_A * K_B * T * sum(float(np.sum(rho[i] * system.vext[i])) for i in range(system.nc)) * dz
+    return om
+
+
+def _uniform_F_res(system, rho):
+    """F_res (k_B T per m^2) summed with uniform weights dz: Phi at every point from the
+    device (cdft_phi_pointwise on the plan's own weighted densities)."""
+    _check_rho(system, rho)
+    f = np.empty(system.structure.ngrid[0])
+    _lib.check(_LIB.cdft_phi_field(system._plan, _lib.dptr(rho), _lib.dptr(f)))
+    st = system.structure
+    lb, ub = st.bounds[0]
+    return float(np.sum(f)) * (ub - lb) / st.ngrid[0] / system.L ** 3
 
 
 def dgamma_dtheta(system, rho):

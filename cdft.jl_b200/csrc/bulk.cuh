@@ -1,0 +1,215 @@
+// Bulk PC-SAFT at fixed temperature and composition on the device: the density roots
+// behind a system's bulk state (get_species / volume(model, p, T, x), PCSAFT.jl:65-72;
+// adsorption(model, surface, p, T) builds one per state point, adsorption.jl:48-65).
+//
+// Residual Helmholtz energy per molecule (Gross & Sadowski, Ind. Eng. Chem. Res. 40 (2001)
+// 1244; 2B self-association: Ind. Eng. Chem. Res. 41 (2002) 5510) in forward-mode dual
+// numbers in the number density, so the compressibility Z = 1 + rho d(a_res)/d(rho) and the
+// pressure p = rho k_B T Z come out exactly.  Roots of p(eta) = p_target as the host
+// molar_density finds them: the sign changes of p - p_target on 40 log-spaced packing
+// fractions in [1e-12, 10^-1.3] and 70 linear ones in [0.051, 0.74], the densest bracket
+// for the liquid, the most dilute for the vapour, refined to 1e-15 relative (Illinois
+// false position).  The stable phase is the root of lower Gibbs energy per molecule,
+// a_res + Z + ln rho (the terms common to both roots dropped).
+#pragma once
+
+struct Dual {
+    double v, d;
+};
+__device__ __forceinline__ Dual dc(double v) { return Dual{v, 0.0}; }
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return Dual{a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return Dual{a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return Dual{a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b)
+{
+    const double q = a.v / b.v;
+    return Dual{q, (a.d - q * b.d) / b.v};
+}
+__device__ __forceinline__ Dual operator*(double s, Dual a) { return Dual{s * a.v, s * a.d}; }
+__device__ __forceinline__ Dual operator+(double s, Dual a) { return Dual{s + a.v, a.d}; }
+__device__ __forceinline__ Dual operator-(double s, Dual a) { return Dual{s - a.v, -a.d}; }
+__device__ __forceinline__ Dual operator+(Dual a, double s) { return Dual{a.v + s, a.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, double s) { return Dual{a.v - s, a.d}; }
+__device__ __forceinline__ Dual dlog(Dual a) { return Dual{log(a.v), a.d / a.v}; }
+__device__ __forceinline__ Dual dsqrt(Dual a)
+{
+    const double r = sqrt(a.v);
+    return Dual{r, 0.5 * a.d / r};
+}
+
+struct BulkModel {
+    int nc;
+    double T;
+    double m[CDFT_MAX_NC], d[CDFT_MAX_NC];        // segments, hard-sphere diameters (m)
+    double s3[CDFT_MAX_NC * CDFT_MAX_NC];         // sigma_ij^3 (m^3)
+    double eT[CDFT_MAX_NC * CDFT_MAX_NC];         // eps_ij / T
+    double aK[CDFT_MAX_NC];                       // 2B self-association: sigma_ii^3 kappa (exp(eps_AB/T) - 1), 0 = none
+};
+
+__constant__ double kBulkA[7][3] = {
+    {0.9105631445, -0.3084016918, -0.0906148351}, {0.6361281449, 0.1860531159, 0.4527842806},
+    {2.6861347891, -2.5030047259, 0.5962700728}, {-26.547362491, 21.419793629, -1.7241829131},
+    {97.759208784, -65.25588533, -4.1302112531}, {-159.59154087, 83.318680481, 13.77663187},
+    {91.297774084, -33.74692293, -8.6728470368}};
+__constant__ double kBulkB[7][3] = {
+    {0.7240946941, -0.5755498075, 0.0976883116}, {2.2382791861, 0.6995095521, -0.2557574982},
+    {-4.0025849485, 3.892567339, -9.155856153}, {-21.003576815, -17.215471648, 20.642075974},
+    {26.855641363, 192.67226447, -38.804430052}, {206.55133841, -161.82646165, 93.626774077},
+    {-355.60235612, -165.20769346, -29.666905585}};
+
+// a_res per molecule (k_B T) at number density rho (1/m^3) and mole fractions x, with its
+// derivative in rho
+__device__ Dual bulk_ares(const BulkModel& M, const double* x, Dual rho)
+{
+    const double PI = 3.14159265358979323846;
+    const int nc = M.nc;
+    Dual z[4];
+    for (int k = 0; k < 4; ++k) {
+        double c = 0.0;
+        for (int i = 0; i < nc; ++i) {
+            double dk = 1.0;
+            for (int q = 0; q < k; ++q) dk *= M.d[i];
+            c += x[i] * M.m[i] * dk;
+        }
+        z[k] = (PI / 6.0 * c) * rho;
+    }
+    const Dual e = z[3], ome = 1.0 - e;
+    const Dual lno = dlog(ome);
+    const Dual ahs = (3.0 * (z[1] * z[2] / ome) + z[2] * z[2] * z[2] / (e * ome * ome) +
+                      (z[2] * z[2] * z[2] / (e * e) - z[0]) * lno) / z[0];
+    auto gij = [&](double dd) {   // g_hs at contact, dd = d_i d_j / (d_i + d_j)
+        return dc(1.0) / ome + (3.0 * dd) * (z[2] / (ome * ome)) + (2.0 * dd * dd) * (z[2] * z[2] / (ome * ome * ome));
+    };
+    double mb = 0.0;
+    for (int i = 0; i < nc; ++i) mb += x[i] * M.m[i];
+    Dual ahc = mb * ahs;
+    for (int i = 0; i < nc; ++i)
+        if (M.m[i] != 1.0) ahc = ahc - (x[i] * (M.m[i] - 1.0)) * dlog(gij(0.5 * M.d[i]));
+    const double c1 = (mb - 1.0) / mb, c2 = (mb - 1.0) * (mb - 2.0) / (mb * mb);
+    Dual I1 = dc(0.0), I2 = dc(0.0);
+    for (int k = 6; k >= 0; --k) {
+        I1 = I1 * e + dc(kBulkA[k][0] + c1 * kBulkA[k][1] + c2 * kBulkA[k][2]);
+        I2 = I2 * e + dc(kBulkB[k][0] + c1 * kBulkB[k][1] + c2 * kBulkB[k][2]);
+    }
+    const Dual e2 = e * e;
+    const Dual C1 = dc(1.0) / (1.0 + mb * (8.0 * e - 2.0 * e2) / (ome * ome * ome * ome) +
+                           (1.0 - mb) * (20.0 * e - 27.0 * e2 + 12.0 * e2 * e - 2.0 * e2 * e2) /
+                               ((ome * (2.0 - e)) * (ome * (2.0 - e))));
+    double m2es3 = 0.0, m2e2s3 = 0.0;
+    for (int i = 0; i < nc; ++i)
+        for (int j = 0; j < nc; ++j) {
+            const double t = x[i] * x[j] * M.m[i] * M.m[j] * M.s3[i * CDFT_MAX_NC + j];
+            const double et = M.eT[i * CDFT_MAX_NC + j];
+            m2es3 += t * et;
+            m2e2s3 += t * et * et;
+        }
+    const Dual adisp = (-2.0 * PI * m2es3) * (rho * I1) - (PI * mb * m2e2s3) * (rho * C1 * I2);
+    Dual aas = dc(0.0);
+    for (int i = 0; i < nc; ++i)
+        if (M.aK[i] != 0.0) {
+            const Dual D = M.aK[i] * gij(0.5 * M.d[i]);
+            const Dual q = (x[i] * D) * rho;
+            const Dual X = dc(2.0) / (1.0 + dsqrt(1.0 + 4.0 * q));
+            aas = aas + (2.0 * x[i]) * (dlog(X) - 0.5 * X + 0.5);
+        }
+    return ahc + adisp + aas;
+}
+
+// pressure (Pa) and Gibbs term a_res + Z + ln rho at number density rho
+__device__ __forceinline__ double bulk_pressure(const BulkModel& M, const double* x, double rho, double* g = nullptr)
+{
+    const double kB = 1.380649e-23;
+    const Dual a = bulk_ares(M, x, Dual{rho, 1.0});
+    const double Z = 1.0 + rho * a.d;
+    if (g) *g = a.v + Z + log(rho);
+    return rho * kB * M.T * Z;
+}
+
+#define BULK_GRID 110
+__device__ __forceinline__ double bulk_grid_eta(int k)
+{
+    if (k < 40) return pow(10.0, -12.0 + k * (10.7 / 39.0));   // numpy.logspace(-12, -1.3, 40)
+    return 0.051 + (k - 40) * (0.689 / 69.0);                   // numpy.linspace(0.051, 0.74, 70)
+}
+
+// root of p(eta / scale) = p0 in the bracket [a, b] (f(a), f(b) of opposite signs)
+__device__ double bulk_refine(const BulkModel& M, const double* x, double scale, double p0, double a, double b,
+                              double fa, double fb)
+{
+    int side = 0;
+    for (int it = 0; it < 400; ++it) {
+        if (fabs(b - a) <= 1e-15 * fabs(b) + 1e-300) break;
+        double c = (a * fb - b * fa) / (fb - fa);
+        if (!(c > fmin(a, b) && c < fmax(a, b))) c = 0.5 * (a + b);
+        const double fc = bulk_pressure(M, x, c / scale) - p0;
+        if (fc == 0.0) return c;
+        if ((fc > 0) == (fb > 0)) {
+            b = c;
+            fb = fc;
+            if (side == -1) fa *= 0.5;   // Illinois: halve the retained end
+            side = -1;
+        } else {
+            a = c;
+            fa = fc;
+            if (side == 1) fb *= 0.5;
+            side = 1;
+        }
+    }
+    return 0.5 * (a + b);
+}
+
+// one warp per state point: rho[s] (mol/m^3) of the requested phase; status[s] = 0 ok, 1 no root
+__global__ void bulk_density_kernel(BulkModel M, int n, const double* __restrict__ p, const double* __restrict__ xin,
+                                    int phase, double* __restrict__ rho_out, int* __restrict__ status)
+{
+    const double NAVO = 6.02214076e23;
+    const int s = blockIdx.x;
+    if (s >= n) return;
+    const int lane = threadIdx.x;
+    __shared__ double fgrid[BULK_GRID];
+    double x[CDFT_MAX_NC];
+    double sx = 0.0;
+    for (int i = 0; i < M.nc; ++i) sx += xin[(size_t)s * M.nc + i];
+    double scale = 0.0;
+    for (int i = 0; i < M.nc; ++i) {
+        x[i] = xin[(size_t)s * M.nc + i] / sx;
+        scale += x[i] * M.m[i] * M.d[i] * M.d[i] * M.d[i];
+    }
+    const double PI = 3.14159265358979323846;
+    scale *= PI / 6.0;   // eta per (molecule / m^3)
+    const double p0 = p[s];
+    for (int k = lane; k < BULK_GRID; k += 32) fgrid[k] = bulk_pressure(M, x, bulk_grid_eta(k) / scale) - p0;
+    __syncwarp();
+    if (lane != 0) return;
+    auto sgn = [](double v) { return v > 0 ? 1 : (v < 0 ? -1 : 0); };
+    int first = -1, last = -1;
+    for (int k = 0; k + 1 < BULK_GRID; ++k)
+        if (sgn(fgrid[k]) != sgn(fgrid[k + 1])) {
+            if (first < 0) first = k;
+            last = k;
+        }
+    if (first < 0) {
+        rho_out[s] = __longlong_as_double(0x7ff8000000000000LL);
+        status[s] = 1;
+        return;
+    }
+    auto root = [&](int k) {
+        const double e = bulk_refine(M, x, scale, p0, bulk_grid_eta(k), bulk_grid_eta(k + 1), fgrid[k], fgrid[k + 1]);
+        return e / scale;   // molecules / m^3
+    };
+    double r;
+    if (phase == 1) r = root(last);
+    else if (phase == 2) r = root(first);
+    else {
+        const double rl = root(last), rv = root(first);
+        if (fabs(rl / rv - 1.0) < 1e-10) r = rl;
+        else {
+            double gl, gv;
+            bulk_pressure(M, x, rl, &gl);
+            bulk_pressure(M, x, rv, &gv);
+            r = (gl <= gv) ? rl : rv;
+        }
+    }
+    rho_out[s] = r / NAVO;
+    status[s] = 0;
+}

@@ -21,6 +21,7 @@
 #include "fft3d.cuh"
 #include "fft3d_tma.cuh"
 #include "tuning.cuh"
+#include "bulk.cuh"
 
 namespace {
 
@@ -101,6 +102,8 @@ struct cdft_plan {
     int tma_ready = 0;
     int L3 = 0, k2max = 0;        // 3D: points per dimension, max |k|^2 index
     double w0 = 0.0;              // 3D: reduced frequency per index
+    double* d_ddft = nullptr;     // DDFT: [tg, tl] per axis, then eta and deta scratch
+    size_t ddft_eta = 0;          // DDFT: offset of the eta scratch in d_ddft
     Batch* self = nullptr;        // batch of this plan alone
 };
 
@@ -750,6 +753,7 @@ void plan_free(cdft_plan* p)
     cudaFree(p->d_R);
     cudaFree(p->d_adj);
     cudaFree(p->d_ktab);
+    cudaFree(p->d_ddft);
     if (p->own_stream) cudaStreamDestroy(p->own_stream);
 }
 
@@ -1553,6 +1557,106 @@ struct KSum {
     double value() const { return s + c; }
 };
 
+// DDFT taps of one axis: the real inverse DFT of the one-axis maps of ddft_rhs_log!
+// (ext/SciMLBasecDFTExt.jl:17-19), 2 pi i k and -(2 pi)^2 k^2 with k = m / B, m the fftfreq
+// integers and B the reduced box length.  Angles by exact integer reduction of m q mod n;
+// the points where sin or cos is exactly 0 or +-1 are set exactly (the Nyquist bin of the
+// gradient then drops out, as the real part of the reference's inverse transform drops it).
+void ddft_axis_taps(int n, double B, double* tg, double* tl)
+{
+    const double two_pi = 6.283185307179586476925286766559;
+    for (int q = 0; q < n; ++q) {
+        KSum sg, sl;
+        for (int idx = 0; idx < n; ++idx) {
+            const long long m = idx < (n + 1) / 2 ? idx : idx - n;
+            long long r = (m * q) % n;
+            if (r < 0) r += n;
+            double sn, cs;
+            if (r == 0) { sn = 0.0; cs = 1.0; }
+            else if (2 * r == n) { sn = 0.0; cs = -1.0; }
+            else if (4 * r == n) { sn = 1.0; cs = 0.0; }
+            else if (4 * r == 3 * (long long)n) { sn = -1.0; cs = 0.0; }
+            else {
+                const double th = two_pi * double(r) / double(n);
+                sn = std::sin(th);
+                cs = std::cos(th);
+            }
+            sg.add(double(m) * sn);
+            sl.add(double(m) * double(m) * cs);
+        }
+        tg[q] = -(two_pi / (double(n) * B)) * sg.value();
+        tl[q] = -(two_pi * two_pi / (double(n) * B * B)) * sl.value();
+    }
+}
+
+int ddft_rhs(cdft_plan* p, const double* eta, double* deta, bool is_dev)
+{
+    if (!p || !eta || !deta) return set_error(CDFT_E_INVALID, "NULL argument");
+    const cdft_system_desc& d = p->desc;
+    if (d.coord != CDFT_COORD_CART)
+        return set_error(CDFT_E_UNSUPPORTED, "the DDFT right-hand side is defined on Cartesian grids");
+    const int nd = d.nd;
+    int len[3] = {1, 1, 1};
+    for (int k = 0; k < nd; ++k) len[k] = d.ngrid[k];
+    int maxlen = 0;
+    for (int k = 0; k < nd; ++k) maxlen = std::max(maxlen, len[k]);
+    const size_t smem = 2 * (size_t)maxlen * sizeof(double);
+    if (smem > 200 * 1024) return set_error(CDFT_E_UNSUPPORTED, "DDFT axis of %d points (at most 12800)", maxlen);
+    CU(cudaSetDevice(p->device));
+    const size_t ne = (size_t)p->sys.n_elem;
+    if (!p->d_ddft) {
+        size_t ntap = 0;
+        for (int k = 0; k < nd; ++k) ntap += 2 * (size_t)len[k];
+        std::vector<double> taps(ntap);
+        size_t off = 0;
+        for (int k = 0; k < nd; ++k) {
+            const double B = (d.bounds[k][1] - d.bounds[k][0]) / d.L;
+            ddft_axis_taps(len[k], B, taps.data() + off, taps.data() + off + len[k]);
+            off += 2 * (size_t)len[k];
+        }
+        CU(cudaMalloc(&p->d_ddft, (ntap + 2 * ne) * sizeof(double)));
+        CU(cudaMemcpy(p->d_ddft, taps.data(), ntap * sizeof(double), cudaMemcpyHostToDevice));
+        p->ddft_eta = ntap;
+        CU(cudaFuncSetAttribute(ddft_axis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    }
+    double* d_eta = p->d_ddft + p->ddft_eta;
+    double* d_out = is_dev ? deta : d_eta + ne;
+    Batch* b = nullptr;
+    int rc = self_batch(p, &b);
+    if (rc) return rc;
+    CU(cudaMemcpyAsync(d_eta, eta, ne * sizeof(double), is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                       p->stream));
+    ddft_prep_kernel<<<std::min<size_t>((ne + 255) / 256, 4096), 256, 0, p->stream>>>(d_eta, p->sys.rho, ne);
+    CHECK_LAUNCH();
+    if ((rc = clear_kernel_error(b))) return rc;
+    rc = p->sys.mixed ? launch_eval_stages<float>(b, nullptr, true) : launch_eval_stages<double>(b, nullptr, true);
+    if (rc) return rc;
+    if (p->sys.mixed)
+        dfdrho_out_kernel<float><<<b->nechunks, ELEM_THREADS, 0, p->stream>>>(b->d_echunks, b->d_sys);
+    else
+        dfdrho_out_kernel<double><<<b->nechunks, ELEM_THREADS, 0, p->stream>>>(b->d_echunks, b->d_sys);
+    CHECK_LAUNCH();
+    // mu = dF/drho_res + V_ext is in sys.out; the axes in x, y, z order, grid [comp][z][y][x]
+    size_t off = 0;
+    long long stride = 1;
+    for (int k = 0; k < nd; ++k) {
+        const long long inner = stride;
+        const long long nlines = (long long)(ne / len[k]);
+        dim3 grid((unsigned)nlines, (unsigned)((len[k] + DDFT_THREADS - 1) / DDFT_THREADS));
+        ddft_axis_kernel<<<grid, DDFT_THREADS, 2 * (size_t)len[k] * sizeof(double), p->stream>>>(
+            d_eta, p->sys.out, d_out, p->d_ddft + off, p->d_ddft + off + len[k], len[k], stride, inner, nlines,
+            k == 0 ? 1 : 0);
+        CHECK_LAUNCH();
+        off += 2 * (size_t)len[k];
+        stride *= len[k];
+    }
+    g_launches += 2 + nd;
+    if (!is_dev) CU(cudaMemcpyAsync(deta, d_out, ne * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    CU(cudaStreamSynchronize(p->stream));
+    return check_kernel_error(b);
+}
+
+
 }  // namespace
 
 // ===========================================================================
@@ -1623,6 +1727,87 @@ int cdft_functional_derivative_dev(cdft_plan* plan, const double* d_rho, double*
 {
     g_err_code = 0;
     return functional_derivative(plan, d_rho, d_dFdrho, true);
+}
+
+int cdft_bulk_density(const cdft_system_desc* desc, int n, const double* p, const double* x, int phase,
+                      double* rho, int* status)
+{
+    g_err_code = 0;
+    if (!desc || n < 0 || (n > 0 && (!p || !x || !rho || !status))) return set_error(CDFT_E_INVALID, "invalid argument");
+    if (phase < 0 || phase > 2) return set_error(CDFT_E_INVALID, "phase=%d (0 stable, 1 liquid, 2 vapour)", phase);
+    const cdft_system_desc& d = *desc;
+    if (d.nc < 1 || d.nc > CDFT_MAX_NC || !(d.T > 0)) return set_error(CDFT_E_INVALID, "nc and T");
+    if (n == 0) return 0;
+    BulkModel M{};
+    M.nc = d.nc;
+    M.T = d.T;
+    for (int i = 0; i < d.nc; ++i) {
+        if (!(d.m[i] > 0) || !(d.hsd[i] > 0)) return set_error(CDFT_E_INVALID, "component %d: m and hsd", i);
+        M.m[i] = d.m[i];
+        M.d[i] = d.hsd[i];
+        for (int j = 0; j < d.nc; ++j) {
+            const double sg = d.sigma[i * d.nc + j];
+            M.s3[i * CDFT_MAX_NC + j] = sg * sg * sg;
+            M.eT[i * CDFT_MAX_NC + j] = d.eps[i * d.nc + j] / d.T;
+        }
+    }
+    for (int q = 0; q < d.n_assoc; ++q) {   // the closed form covers 2B self-association
+        const cdft_assoc_pair& a = d.assoc[q];
+        if (a.icomp != a.jcomp || a.isite == a.jsite || a.n_ia != 1 || a.n_jb != 1 || a.icomp < 0 || a.icomp >= d.nc ||
+            M.aK[a.icomp] != 0.0)
+            return set_error(CDFT_E_UNSUPPORTED, "device bulk densities cover 2B self-association only");
+        const double sg = d.sigma[a.icomp * d.nc + a.icomp];
+        M.aK[a.icomp] = sg * sg * sg * a.kappa_ab * (exp(a.eps_ab / d.T) - 1.0);
+    }
+    double* dbuf = nullptr;
+    const size_t nb = (size_t)n * (2 + d.nc) * sizeof(double) + (size_t)n * sizeof(int);
+    CU(cudaMalloc(&dbuf, nb));
+    double* dp = dbuf;
+    double* dx = dp + n;
+    double* dr = dx + (size_t)n * d.nc;
+    int* ds = reinterpret_cast<int*>(dr + n);
+    cudaError_t e = cudaMemcpy(dp, p, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dx, x, (size_t)n * d.nc * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        bulk_density_kernel<<<n, 32>>>(M, n, dp, dx, phase, dr, ds);
+        e = cudaGetLastError();
+        g_launches += 1;
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(rho, dr, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(status, ds, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(dbuf);
+    if (e != cudaSuccess) return set_error(CDFT_E_CUDA, "bulk densities: %s", cudaGetErrorString(e));
+    return 0;
+}
+
+int cdft_ddft_rhs(cdft_plan* plan, const double* eta, double* deta)
+{
+    g_err_code = 0;
+    return ddft_rhs(plan, eta, deta, false);
+}
+
+int cdft_ddft_rhs_dev(cdft_plan* plan, const double* d_eta, double* d_deta)
+{
+    g_err_code = 0;
+    return ddft_rhs(plan, d_eta, d_deta, true);
+}
+
+int cdft_phi_field(cdft_plan* plan, const double* rho, double* fval)
+{
+    g_err_code = 0;
+    if (!plan || !rho || !fval) return set_error(CDFT_E_INVALID, "NULL argument");
+    CU(cudaSetDevice(plan->device));
+    Batch* b = nullptr;
+    int rc = self_batch(plan, &b);
+    if (rc) return rc;
+    CU(cudaMemcpyAsync(plan->sys.rho, rho, (size_t)plan->sys.n_elem * sizeof(double), cudaMemcpyHostToDevice,
+                       plan->stream));
+    if ((rc = clear_kernel_error(b))) return rc;
+    rc = launch_eval_stages<double>(b, nullptr, false);
+    if (rc) return rc;
+    CU(cudaMemcpyAsync(fval, plan->sys.fval, sizeof(double) * plan->N, cudaMemcpyDeviceToHost, plan->stream));
+    CU(cudaStreamSynchronize(plan->stream));
+    return check_kernel_error(b);
 }
 
 int cdft_free_energy_res(cdft_plan* plan, const double* rho, double* F)
@@ -1871,9 +2056,19 @@ int cdft_tuning_set(const char* name, int value)
 // ---------------------------------------------------------------------------
 // Parameter gradient of F_res and of the excess grand potential (1D)
 // ---------------------------------------------------------------------------
+// uniform = false: the Simpson weights of F_res (integrals.jl:28-41); true: the uniform
+// weights dz of the discrete functional whose gradient the pointwise Euler-Lagrange equation
+// of converge! is (what cdft_grad_params differentiates)
+static int fres_grad_impl(cdft_plan* plan, const double* rho, double* dF, bool uniform);
+
 int cdft_free_energy_res_grad(cdft_plan* plan, const double* rho, double* dF)
 {
     g_err_code = 0;
+    return fres_grad_impl(plan, rho, dF, false);
+}
+
+static int fres_grad_impl(cdft_plan* plan, const double* rho, double* dF, bool uniform)
+{
     if (!plan || !rho || !dF) return set_error(CDFT_E_INVALID, "NULL argument");
     const cdft_system_desc& d = plan->desc;
     if (d.nd != 1 || d.coord != CDFT_COORD_CART)
@@ -1950,8 +2145,11 @@ int cdft_free_energy_res_grad(cdft_plan* plan, const double* rho, double* dF)
     cudaFree(d_kt);
     cudaFree(d_scale);
     if (rc) return rc;
-    // Simpson integrals (as cdft_free_energy_res): G[q] = dF_res / dP_q, Gd[i] = dF_res / dd_i via the kernels
-    auto coef = [](int k, int n) { return (k == 1 || k == n) ? 1.0 : ((k % 2 == 0) ? 4.0 : 2.0); };
+    // Simpson (as cdft_free_energy_res) or uniform integrals: G[q] = dF_res / dP_q, Gd[i] = dF_res / dd_i
+    // via the kernels
+    auto coef = [uniform](int k, int n) {
+        return uniform ? 3.0 : ((k == 1 || k == n) ? 1.0 : ((k % 2 == 0) ? 4.0 : 2.0));
+    };
     const double w = (plan->dz[0] / 3.0) / (L * L * L);
     std::vector<double> G(NP), Gd(nc);
     for (int q = 0; q < NP; ++q) {
@@ -2029,34 +2227,34 @@ int grad_params_impl(cdft_plan* plan, const double* rho, const double* dmu_dthet
                          "the external field depends on the parameters: pass its derivative (cdft_grad_params_ext)");
     const int nc = d.nc, N = plan->N, np = 3 * nc;
     std::vector<double> dF(np);
-    int rc = cdft_free_energy_res_grad(plan, rho, dF.data());
+    g_err_code = 0;
+    int rc = fres_grad_impl(plan, rho, dF.data(), true);
     if (rc) return rc;
-    // Simpson integrals of rho_i (mol/m^2) and of 1 (m), as surface_tension's
-    auto coef = [](int k, int n) { return (k == 1 || k == n) ? 1.0 : ((k % 2 == 0) ? 4.0 : 2.0); };
+    // The envelope theorem needs the quadrature in which the converged profile is stationary:
+    // the pointwise Euler-Lagrange equation is the gradient of the functional summed with
+    // uniform weights dz (the adjoint of the periodic convolution), so every integral below
+    // uses them.  surface_tension's Simpson weights differ from it where the profile is not
+    // resolved on the grid (sharp adsorbed layers); for resolved profiles the two agree.
+    const double dz = plan->dz[0];
     std::vector<double> nint(nc);
-    double one = 0.0;
     for (int i = 0; i < nc; ++i) {
         KSum acc;
-        for (int k = 1; k <= N; ++k) acc.add(coef(k, N) * rho[(size_t)i * N + k - 1]);
-        nint[i] = acc.value() * plan->dz[0] / 3.0;
+        for (int k = 0; k < N; ++k) acc.add(rho[(size_t)i * N + k]);
+        nint[i] = acc.value() * dz;
     }
-    {
-        KSum acc;
-        for (int k = 1; k <= N; ++k) acc.add(coef(k, N));
-        one = acc.value() * plan->dz[0] / 3.0;
-    }
-    const double kB = 1.380649e-23;
+    const double one = N * dz;
+    const double kB = 1.380649e-23, NAVO = 6.02214076e23;
     for (int t = 0; t < np; ++t) {
         double v = kB * d.T * dF[t];
         if (dmu_dtheta)
             for (int i = 0; i < nc; ++i) v -= dmu_dtheta[(size_t)i * np + t] * nint[i];
         if (dp_dtheta) v += dp_dtheta[t] * one;
-        if (dvext_dtheta)   // k_B T sum_i int rho_i dV_i/dtheta (V in units of k_B T)
+        if (dvext_dtheta)   // R T sum_i int rho_i dV_i/dtheta (rho in mol/m^3, V in units of k_B T)
             for (int i = 0; i < nc; ++i) {
                 KSum acc;
                 const double* dv = dvext_dtheta + ((size_t)t * nc + i) * N;
-                for (int k = 1; k <= N; ++k) acc.add(coef(k, N) * rho[(size_t)i * N + k - 1] * dv[k - 1]);
-                v += kB * d.T * acc.value() * plan->dz[0] / 3.0;
+                for (int k = 0; k < N; ++k) acc.add(rho[(size_t)i * N + k] * dv[k]);
+                v += NAVO * kB * d.T * acc.value() * dz;
             }
         dOmega[t] = v;
     }

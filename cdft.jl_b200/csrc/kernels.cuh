@@ -1167,3 +1167,57 @@ __global__ void integrals_reduce_kernel(const double* __restrict__ part, int nch
     }
     out[(size_t)blockIdx.x * nq + q] = tot.s + (tot.c + comp);
 }
+
+// ---------------------------------------------------------------------------
+// DDFT right-hand side in ln rho (ext/SciMLBasecDFTExt.jl:10-61, ddft_rhs_log!):
+//   d eta/dt = lap(eta) + lap(mu) + sum_d [ (d_d eta)^2 + d_d mu d_d eta ],
+// mu = dF/drho_res + V_ext.  The reference applies the spectral maps 2 pi i k_d and
+// -(2 pi)^2 |k|^2 by FFT (convolve!, integrals.jl:88-96: real part of the inverse
+// transform); both maps are sums of one-axis maps, so each term is a periodic circulant
+// along one axis whose taps are the real inverse DFT of the one-axis map.
+// ddft_prep_kernel: rho = exp(clamp(eta, -50, 30)).
+// ddft_axis_kernel: one block per (line, output tile) of one axis; the line of eta and mu
+// in shared memory; adds lap_d(eta + mu) + g_eta^2 + g_mu g_eta into deta (first axis
+// writes).  tg / tl: gradient and second-derivative taps of the axis.
+// ---------------------------------------------------------------------------
+#define DDFT_THREADS 256
+__global__ void ddft_prep_kernel(const double* __restrict__ eta, double* __restrict__ rho, size_t n)
+{
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        rho[e] = exp(fmin(fmax(eta[e], -50.0), 30.0));
+}
+
+__global__ void __launch_bounds__(DDFT_THREADS)
+ddft_axis_kernel(const double* __restrict__ eta, const double* __restrict__ mu, double* __restrict__ deta,
+                 const double* __restrict__ tg, const double* __restrict__ tl, int len, long long stride,
+                 long long inner, long long nlines, int first)
+{
+    extern __shared__ double ddft_smem[];
+    double* se = ddft_smem;        // eta of the line
+    double* sm = ddft_smem + len;  // mu of the line
+    const long long line = blockIdx.x;
+    if (line >= nlines) return;
+    // line -> base offset: lines are (outer, inner) pairs around the axis
+    const long long o = line / inner, i = line - o * inner;
+    const long long base = o * inner * len + i;
+    for (int q = threadIdx.x; q < len; q += DDFT_THREADS) {
+        se[q] = eta[base + q * stride];
+        sm[q] = mu[base + q * stride];
+    }
+    __syncthreads();
+    const int j = blockIdx.y * DDFT_THREADS + threadIdx.x;
+    if (j >= len) return;
+    double lap = 0.0, ge = 0.0, gm = 0.0;
+    int src = j;   // (j - q) mod len
+    for (int q = 0; q < len; ++q) {
+        const double a = tg[q], b = tl[q];
+        const double xe = se[src], xm = sm[src];
+        lap = fma(b, xe + xm, lap);
+        ge = fma(a, xe, ge);
+        gm = fma(a, xm, gm);
+        src = (src == 0) ? len - 1 : src - 1;
+    }
+    const double v = lap + ge * ge + gm * ge;
+    const long long e = base + j * stride;
+    deta[e] = first ? v : deta[e] + v;
+}

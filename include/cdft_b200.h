@@ -155,6 +155,27 @@ int cdft_plan_destroy(cdft_plan* plan);
 int cdft_functional_derivative(cdft_plan* plan, const double* rho, double* dFdrho);
 int cdft_functional_derivative_dev(cdft_plan* plan, const double* d_rho, double* d_dFdrho);
 
+/* Bulk molar densities (mol/m^3) of n state points at the temperature of desc, with its
+ * m, hsd, sigma, eps and association (2B self-association only): pressure p[s] (Pa),
+ * mole fractions x[s * nc + i] (normalised here).  phase 0: the stable root (lower Gibbs
+ * energy of the densest and the most dilute root, the default of volume(model, p, T, x)
+ * behind get_species, PCSAFT.jl:65-72, and adsorption, adsorption.jl:48-65); 1 the
+ * densest root; 2 the most dilute root.  status[s] = 0, or 1 where no root exists (rho
+ * NaN).  Fields of desc other than nc, m, hsd, sigma, eps, T and the pairs are ignored. */
+int cdft_bulk_density(const cdft_system_desc* desc, int n, const double* p, const double* x, int phase,
+                      double* rho, int* status);
+
+/* Right-hand side of dynamic DFT in eta = ln rho: deta = lap(eta) + lap(mu) +
+ * sum_d (d_d eta)^2 + d_d mu d_d eta with rho = exp(clamp(eta, -50, 30)) and
+ * mu = dF/drho_res + V_ext, derivatives spectral in reduced lengths (x / L) on the
+ * periodic grid.  Replaces the function ddft_rhs_log! that
+ * SciMLBase.ODEProblem(system, ρ, tspan) integrates, ext/SciMLBasecDFTExt.jl:10-61
+ * (Cartesian 1D and 3D; the derivative maps act as exact periodic circulants along
+ * each axis, the same linear operators as the reference's FFT products).  eta and
+ * deta have the layout of rho. */
+int cdft_ddft_rhs(cdft_plan* plan, const double* eta, double* deta);
+int cdft_ddft_rhs_dev(cdft_plan* plan, const double* d_eta, double* d_deta);
+
 /* Residual Helmholtz energy per unit area (1D) or total (3D) in units of k_B T
  * (per m^2 in 1D), evaluated in FP64 whatever the plan's precision.  Replaces F_res(system, ρ), src/models/models.jl:86-91
  * (Simpson rule of src/utils/integrals.jl:17-41 on the device f_res values,
@@ -178,6 +199,10 @@ int cdft_batch_integrals(cdft_plan* const* plans, int nplans, double* const* rho
  * the Enzyme kernels δf_fwd_kernel!/δf_rev_kernel! (models.jl:355-411) that
  * differentiate f_res (PCSAFT.jl:110-117). */
 int cdft_phi_pointwise(cdft_plan* plan, const double* n, int npts, double* fval, double* dphi);
+
+/* Phi at every grid point of the profile rho (FP64, reduced units: F_res = the quadrature
+ * of Phi over the grid divided by L^3, models.jl:86-91), fval of length prod(ngrid). */
+int cdft_phi_field(cdft_plan* plan, const double* rho, double* fval);
 
 /* Parameter gradient of F_res at a fixed profile (1D): dF[3k + 0..2] =
  * dF_res/d(sigma_k [A], eps_k/k_B [K], m_k) in the units of cdft_free_energy_res,

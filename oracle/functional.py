@@ -280,6 +280,28 @@ class DFTSystem:
         lnG = self.chem_pot_res_dens.reshape((self.nc,) + (1,) * self.nd) - d
         return np.clip(lnG, -100.0, 100.0)
 
+    # ---- dynamic DFT (ext/SciMLBasecDFTExt.jl:10-61) ---------------------------------
+    def ddft_rhs(self, eta):
+        """ddft_rhs_log! of SciMLBase.ODEProblem(system, ρ, tspan): with rho =
+        exp(clamp(eta, -50, 30)) and mu = dF/drho_res + V_ext (δFδρ_res! then
+        evaluate_external_field!), per component
+        d eta = lap(eta) + lap(mu) + sum_d (grad_d eta)^2 + grad_d mu grad_d eta,
+        each derivative the convolve! of the map 2 pi i k_d or -(2 pi)^2 |k|^2 (k = the
+        reduced fftfreq grid, structure_ω * L) -- complex FFT, multiply, inverse, real part."""
+        eta = np.asarray(eta, dtype=np.float64)
+        rho = np.exp(np.clip(eta, -50.0, 30.0))
+        mu = self.dFdrho(rho)
+        om = [np.broadcast_to(o, self.structure.grid_shape) for o in self._omega()]
+        lap = -(2 * np.pi) ** 2 * sum(o * o for o in om)
+        grad = [2 * np.pi * 1j * o for o in om]
+        out = np.zeros_like(eta)
+        for i in range(self.nc):
+            out[i] = self._conv(eta[i], lap) + self._conv(mu[i], lap)
+            for g in grad:
+                ge = self._conv(eta[i], g)
+                out[i] += ge * ge + self._conv(mu[i], g) * ge
+        return out
+
     # ---- profiles ----------------------------------------------------------------
     def initialize_profiles(self):
         s = self.structure
