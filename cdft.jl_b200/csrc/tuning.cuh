@@ -12,10 +12,14 @@
 struct TunedShapes {
     // persistent engine: a system of at most this many elements (N * nc) runs the Anderson
     // vector slots on one warp (no block barriers); larger systems use the whole block.
-    // Measured on the 64-point isotherm (N = 100..400, m = 5, three-pass Anderson update):
-    // 11.26 ms per batch with 0, 10.74 with 256, 10.67 with 512, 10.66 with 1024, so 1024
-    // (every isotherm system takes the warp path).
-    int pers_warp_aa_max_elem = 1024;
+    // The two sections reduce in different orders, and on a few isotherm state points the
+    // evaluation count is chaotic in the last bits, so the batch time mixes the section's cost
+    // with which evaluation count a state point happens to land on.  The sweep therefore
+    // compares the time per evaluation of the critical path (batch time / the largest
+    // evaluation count), and per-stage clock64 timers agree: the Anderson section costs
+    // 2.65 us (block) vs 4.41 us (warp) per evaluation at N = 186 and 1.7 vs 3.6 us at N = 400,
+    // so 0 (the whole block for every system).
+    int pers_warp_aa_max_elem = 0;
     // 3D grids: the strided y and z FFT passes as persistent TMA tile kernels (1) or as one
     // block per tile with per-thread loads (0); both compute the same arithmetic
     int fft3d_tma = 1;
