@@ -1085,10 +1085,42 @@ int launch_iteration(Batch* b)
     return 0;
 }
 
+// Two CTAs per system (a cluster of two, persistent_kernel<..., 2>) when the Anderson vectors
+// live in shared memory, the arithmetic is FP64, the pairs fit the device in one wave and the
+// tuned entry allows it; otherwise one CTA per system.  Both forms give the same bits.
 template <typename T, int NC>
 int launch_persistent_nc(Batch* b, int max_evals, size_t smem, int vec_m)
 {
-    auto kern = persistent_kernel<T, NC, 1>;
+    const int dev = b->plans[0]->device;
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if constexpr (sizeof(T) == 8) {
+        if (g_tuned.pers_cluster && vec_m >= 0 && 2 * b->nsys <= nsm) {
+            auto kern2 = persistent_kernel<T, NC, 1, 2>;
+            CU(cudaFuncSetAttribute(kern2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(2 * b->nsys);
+            cfg.blockDim = dim3(PERS_THREADS);
+            cfg.dynamicSmemBytes = smem;
+            cfg.stream = b->stream;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = 2;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            int nclusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, kern2, &cfg) == cudaSuccess && nclusters >= b->nsys) {
+                CU(cudaLaunchKernelEx(&cfg, kern2, (const SysDev*)b->d_sys, b->d_st, b->d_done, max_evals, vec_m,
+                                      g_tuned.pers_warp_aa_max_elem));
+                g_launches += 1;
+                return 0;
+            }
+            cudaGetLastError();   // the occupancy query's status, if it failed: fall back to one CTA per system
+        }
+    }
+    auto kern = persistent_kernel<T, NC, 1, 1>;
     CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<b->nsys, PERS_THREADS, smem, b->stream>>>(b->d_sys, b->d_st, b->d_done, max_evals, vec_m,
                                                      g_tuned.pers_warp_aa_max_elem);
@@ -1122,8 +1154,10 @@ template <typename T, int NC>
 size_t persistent_static_smem()
 {
     cudaFuncAttributes a;
-    if (cudaFuncGetAttributes(&a, persistent_kernel<T, NC, 1>) != cudaSuccess) return 1u << 30;
-    return a.sharedSizeBytes;
+    if (cudaFuncGetAttributes(&a, persistent_kernel<T, NC, 1, 1>) != cudaSuccess) return 1u << 30;
+    size_t stat = a.sharedSizeBytes;
+    if (cudaFuncGetAttributes(&a, persistent_kernel<T, NC, 1, 2>) != cudaSuccess) return 1u << 30;
+    return std::max(stat, (size_t)a.sharedSizeBytes);
 }
 
 size_t persistent_smem_limit(const Batch* b)

@@ -11,6 +11,7 @@
 // the ones of the grid engine (kernels.cuh), so both engines follow the same
 // aasol trajectory.
 #pragma once
+#include <cooperative_groups.h>
 #include "kernels.cuh"
 
 #define PERS_THREADS 384
@@ -91,15 +92,18 @@ __device__ __forceinline__ void block_reduce_to_smem(double* vals, int K, double
 // window is a ring of PERS_R registers whose rotation is resolved at compile time
 // (the q loop is unrolled by PERS_R), so a step is one tap load, one window load
 // and PERS_R independent FMAs.
+// Tasks task0, task0 + tstride, ... of the stage (a cluster splits them between its CTAs);
+// out2, when not null, receives a second copy of every output (the peer CTA's buffer).
 template <typename T, int NC>
 __device__ __forceinline__ void pers_conv(const T* __restrict__ ext, bool shared_input, const T* __restrict__ taps,
-                                          T* __restrict__ out, int out_comp_stride, int N, int nconv, T scale)
+                                          T* __restrict__ out, int out_comp_stride, int N, int nconv, T scale,
+                                          int task0, int tstride, T* out2)
 {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31;
     const int EXTN = pers_extp(N), OFF = pers_off(N);   // FP32 rows: logical positions, row stride extp
     const int ntiles = (N + PERS_TILE - 1) / PERS_TILE;
     const int ntask = NC * nconv * ntiles;
-    for (int task = warp; task < ntask; task += PERS_WARPS) {
+    for (int task = task0; task < ntask; task += tstride) {
         const int tile = task % ntiles;
         const int f = (task / ntiles) % nconv;
         const int i = task / (ntiles * nconv);
@@ -128,11 +132,15 @@ __device__ __forceinline__ void pers_conv(const T* __restrict__ ext, bool shared
                 }
             }
         }
-        T* o = out + (size_t)i * out_comp_stride + (size_t)f * N;
+        const size_t ob = (size_t)i * out_comp_stride + (size_t)f * N;
 #pragma unroll
         for (int r = 0; r < PERS_R; ++r) {
             const int j = j0 + 32 * r;
-            if (j < N) o[j] = acc[r] * scale;
+            if (j < N) {
+                const T v = acc[r] * scale;
+                out[ob + j] = v;
+                if (out2) out2[ob + j] = v;
+            }
         }
     }
 }
@@ -159,16 +167,17 @@ __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, do
 template <int NC>
 __device__ __forceinline__ void pers_conv_dmma(const double* __restrict__ ext, bool shared_input,
                                                const double* __restrict__ taps, double* __restrict__ out,
-                                               int out_comp_stride, int N, int nconv, double scale)
+                                               int out_comp_stride, int N, int nconv, double scale, int task0,
+                                               int tstride, double* out2)
 {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31;
     const int EXTP = pers_extp(N), OFF = pers_off(N), TS = pers_ts(N);
     const int U = (N + 7) / 8;          // 8-output columns
     const int nut = (U + 7) / 8;        // warp tiles of 8 columns
     const int D = (N + 14) / 8;         // tap blocks: 8 (D - 1) + 7 >= N - 1
     const int ntask = NC * nconv * nut;
     const int r = lane >> 2, k = lane & 3;   // A row / C row, A column / B row
-    for (int task = warp; task < ntask; task += PERS_WARPS) {
+    for (int task = task0; task < ntask; task += tstride) {
         const int ut = task % nut;
         const int f = (task / nut) % nconv;
         const int i = task / (nut * nconv);
@@ -196,21 +205,29 @@ __device__ __forceinline__ void pers_conv_dmma(const double* __restrict__ ext, b
             dmma_m8n8k4(c0, c1, tp[q0], in[pers_pos(x0)]);
             dmma_m8n8k4(e0, e1, tp[q0 - 4], in[pers_pos(x0 + 4)]);
         }
-        double* o = out + (size_t)i * out_comp_stride + (size_t)f * N;
+        const size_t ob = (size_t)i * out_comp_stride + (size_t)f * N;
         const int j0 = 8 * (u0 + 2 * k) + r, j1 = j0 + 8;
-        if (j0 < N) o[j0] = ((c0 + e0) + (g0 + h0)) * scale;
-        if (j1 < N) o[j1] = ((c1 + e1) + (g1 + h1)) * scale;
+        const double v0 = ((c0 + e0) + (g0 + h0)) * scale, v1 = ((c1 + e1) + (g1 + h1)) * scale;
+        if (j0 < N) {
+            out[ob + j0] = v0;
+            if (out2) out2[ob + j0] = v0;
+        }
+        if (j1 < N) {
+            out[ob + j1] = v1;
+            if (out2) out2[ob + j1] = v1;
+        }
     }
 }
 
 template <typename T, int NC>
 __device__ __forceinline__ void pers_conv_any(const T* __restrict__ ext, bool shared_input, const T* __restrict__ taps,
-                                              T* __restrict__ out, int out_comp_stride, int N, int nconv, T scale)
+                                              T* __restrict__ out, int out_comp_stride, int N, int nconv, T scale,
+                                              int task0, int tstride, T* out2)
 {
     if constexpr (sizeof(T) == 8)
-        pers_conv_dmma<NC>(ext, shared_input, taps, out, out_comp_stride, N, nconv, scale);
+        pers_conv_dmma<NC>(ext, shared_input, taps, out, out_comp_stride, N, nconv, scale, task0, tstride, out2);
     else
-        pers_conv<T, NC>(ext, shared_input, taps, out, out_comp_stride, N, nconv, scale);
+        pers_conv<T, NC>(ext, shared_input, taps, out, out_comp_stride, N, nconv, scale, task0, tstride, out2);
 }
 
 // The Anderson section of one fixed-point step (the QR downdate and the vector slots
@@ -252,7 +269,16 @@ __device__ __forceinline__ void pers_anderson_warp(const SysDev& S, AAState& A, 
 // warp_aa_max_elem: a system of at most this many elements (N * nc) runs the Anderson
 // section on warp 0 (pers_anderson_warp), a larger one on the whole block.  The choice
 // depends on the system alone, so a system gets the same arithmetic alone or in a batch.
-template <typename T, int NC, int ND>
+//
+// CL = 2: a cluster of two CTAs per system (launched with cluster dimension 2; only with
+// the Anderson vectors in shared memory).  The convolution tasks and the Phi points are
+// split between the two CTAs; each writes its results into its own shared memory and into
+// the peer's (distributed shared memory), and a cluster barrier follows each of the three
+// stages.  The Euler-Lagrange step and the Anderson section run in both CTAs on identical
+// data, so both hold the same solver state and take the same branches; every value is
+// computed by the same code as with CL = 1, so the results are bit for bit the same.
+// Rank 0 alone writes the state, the profile and the done count back.
+template <typename T, int NC, int ND, int CL>
 __global__ void __launch_bounds__(PERS_THREADS, 1)
 persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int* done_counter, int max_evals,
                   int vec_m, int warp_aa_max_elem)
@@ -261,8 +287,12 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
     __shared__ AAState sA;
     __shared__ SysDev sS;
     __shared__ double sums[RED_SLOTS];
+    __shared__ int done_local;
     constexpr int NF = 6 + ND, NCONV = 5 + ND;
-    const SysDev& G = sys[blockIdx.x];
+    const int rank = (CL == 2) ? (int)(blockIdx.x & 1u) : 0;
+    const int sid = (CL == 2) ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+    int* done_ptr = rank == 0 ? done_counter : &done_local;
+    const SysDev& G = sys[sid];
     const int N = G.N, n_elem = G.n_elem;
     const int EXTN = pers_extn(N), EXTP = pers_extp(N), OFF = pers_off(N), TS = pers_ts(N);
     const int tid = threadIdx.x;
@@ -271,9 +301,23 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
     T* nf = ext + (size_t)NC * NCONV * EXTP;
     T* ip = nf + (size_t)NC * NF * N;
     if (tid == 0) {
-        sA = st[blockIdx.x];
+        sA = st[sid];
         sS = G;
+        done_local = 0;
     }
+    // the peer CTA's copies of the stage buffers (CL = 2), and the stage split
+    T* nf_peer = nullptr;
+    T* ip_peer = nullptr;
+    if constexpr (CL == 2) {
+        cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+        nf_peer = cl.map_shared_rank(nf, rank ^ 1);
+        ip_peer = cl.map_shared_rank(ip, rank ^ 1);
+    }
+    const int task0 = rank * PERS_WARPS + (tid >> 5), tstride = CL * PERS_WARPS;
+    auto stage_sync = [&]() {
+        if constexpr (CL == 2) cooperative_groups::this_cluster().sync();
+        else __syncthreads();
+    };
     {
         const T* src = (sizeof(T) == 8) ? reinterpret_cast<const T*>(G.taps) : reinterpret_cast<const T*>(G.taps32);
         for (int k = tid; k < NC * NCONV * TS; k += PERS_THREADS) {
@@ -289,8 +333,13 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
         for (int e = tid; e < n_elem; e += PERS_THREADS) {
             vs[e] = G.rho[e];
             vs[n_elem + e] = G.sol[e];
-            if (G.vext) vs[5 * n_elem + e] = G.vext[e];
+            vs[5 * n_elem + e] = G.vext ? G.vext[e] : 0.0;
         }
+        // gx, res, df and the history start at zero (the solver writes them before it reads
+        // them; defined contents keep the two CTAs of a cluster bit-identical regardless)
+        for (size_t e = tid; e < 3 * (size_t)n_elem; e += PERS_THREADS) vs[2 * (size_t)n_elem + e] = 0.0;
+        const size_t nhist = ((size_t)pers_qs(vec_m) + (size_t)vec_m) * n_elem;
+        for (size_t e = tid; e < nhist; e += PERS_THREADS) vs[6 * (size_t)n_elem + e] = 0.0;
     }
     __syncthreads();
     if (vec_m >= 0 && tid == 0) {
@@ -322,13 +371,14 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
             nf[(i * NF) * N + j] = T(S.NA * S.rho[e]);
         }
         __syncthreads();
-        pers_conv_any<T, NC>(ext, true, taps, nf + N, NF * N, N, NCONV, NA);
-        __syncthreads();
+        pers_conv_any<T, NC>(ext, true, taps, nf + N, NF * N, N, NCONV, NA, task0, tstride,
+                             nf_peer ? nf_peer + N : nullptr);
+        stage_sync();
         // ---- fused Phi / dPhi/dn, in place: two threads per point ----
         // items j < N: hard sphere + association (fields 1 .. 2 + ND); items N + j: chain +
         // dispersion (fields 0, 3 + ND .. 5 + ND).  The two halves read and write disjoint
         // fields, and they fall in different warps except around item N.
-        for (int w = tid; w < 2 * N; w += PERS_THREADS) {
+        for (int w = rank * PERS_THREADS + tid; w < 2 * N; w += CL * PERS_THREADS) {
             const bool first = w < N;
             const int j = first ? w : w - N;
             T n[NC][NF], g[NC][NF];
@@ -345,9 +395,12 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
             for (int i = 0; i < NC; ++i)
 #pragma unroll
                 for (int a = 0; a < NF; ++a)
-                    if ((a >= 1 && a <= 2 + ND) == first) nf[(i * NF + a) * N + j] = g[i][a];
+                    if ((a >= 1 && a <= 2 + ND) == first) {
+                        nf[(i * NF + a) * N + j] = g[i][a];
+                        if (nf_peer) nf_peer[(i * NF + a) * N + j] = g[i][a];
+                    }
         }
-        __syncthreads();
+        stage_sync();
         // ---- adjoint convolutions (integrate_field!) ----
         {
             for (int k = tid; k < NC * NCONV * EXTN; k += PERS_THREADS) {
@@ -358,9 +411,9 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
                 ext[(size_t)slot * EXTP + (sizeof(T) == 8 ? pers_pos(u) : u)] = nf[(i * NF + f + 1) * N + j];
             }
             __syncthreads();
-            pers_conv_any<T, NC>(ext, false, taps, ip, NCONV * N, N, NCONV, T(1));
+            pers_conv_any<T, NC>(ext, false, taps, ip, NCONV * N, N, NCONV, T(1), task0, tstride, ip_peer);
         }
-        __syncthreads();
+        stage_sync();
         // ---- Euler-Lagrange step + aa_point! bookkeeping ----
         {
             const int mode = sA.mode;
@@ -381,12 +434,12 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
                 ss[0] += el_elem(S, e, i, dF, beta, aa, DGs);
             }
             block_reduce_to_smem<PERS_THREADS>(ss, 1, sums, n_elem);
-            if (tid == 0) ctl_apply(sA, -1, 0, sums, done_counter, true);
+            if (tid == 0) ctl_apply(sA, -1, 0, sums, done_ptr, true);
             __syncthreads();
         }
         // ---- Anderson vector slots ----
         if (warp_aa) {
-            if (tid < 32) pers_anderson_warp(S, sA, sums, done_counter, tid);
+            if (tid < 32) pers_anderson_warp(S, sA, sums, done_ptr, tid);
             __syncthreads();
             continue;
         }
@@ -399,7 +452,7 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
             const int K = vec_op_range<PERS_MAX_M>(op, S, sA, tid, n_elem, PERS_THREADS, acc);
             if (K > 0) {
                 block_reduce_to_smem<PERS_THREADS>(acc, K, sums, n_elem);
-                if (tid == 0) ctl_apply(sA, op, slot, sums, done_counter, true);
+                if (tid == 0) ctl_apply(sA, op, slot, sums, done_ptr, true);
             }
             __syncthreads();
             if (sA.pad0) {   // the next step's QR downdate, from this step's R, on warp 0
@@ -409,11 +462,13 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
             }
         }
     }
-    if (vec_m >= 0) {
+    if (vec_m >= 0 && rank == 0) {
         for (int e = tid; e < n_elem; e += PERS_THREADS) {
             G.rho[e] = S.rho[e];
             G.sol[e] = S.sol[e];
         }
     }
-    if (tid == 0) st[blockIdx.x] = sA;
+    if (tid == 0 && rank == 0) st[sid] = sA;
+    // no CTA of a cluster leaves while its peer may still write into its shared memory
+    if constexpr (CL == 2) cooperative_groups::this_cluster().sync();
 }

@@ -20,6 +20,10 @@ struct TunedShapes {
     // 2.65 us (block) vs 4.41 us (warp) per evaluation at N = 186 and 1.7 vs 3.6 us at N = 400,
     // so 0 (the whole block for every system).
     int pers_warp_aa_max_elem = 0;
+    // persistent engine: two CTAs per system (a cluster of two splitting the convolution tasks
+    // and the Phi points, distributed shared memory between them) when the batch fits the
+    // device in one wave of pairs; same arithmetic, so the same results as one CTA per system
+    int pers_cluster = 1;
     // 3D grids: the strided y and z FFT passes as persistent TMA tile kernels (1) or as one
     // block per tile with per-thread loads (0); both compute the same arithmetic
     int fft3d_tma = 1;
@@ -40,6 +44,7 @@ struct TunedEntry {
 
 static const TunedEntry kTunedEntries[] = {
     {"pers_warp_aa_max_elem", &TunedShapes::pers_warp_aa_max_elem, 0, 1 << 30},
+    {"pers_cluster", &TunedShapes::pers_cluster, 0, 1},
     {"fft3d_tma", &TunedShapes::fft3d_tma, 0, 1},
     {"fft3d_fused_phi", &TunedShapes::fft3d_fused_phi, 0, 1},
 };

@@ -300,3 +300,27 @@ def test_persistent_anderson_warp_and_block_paths_agree():
             assert float(np.max(np.abs(rho / ro - 1))) < 1e-9, thr
     finally:
         cd.tuning("pers_warp_aa_max_elem", old)
+
+
+def test_persistent_cluster_pairs_equal_single_ctas_bitwise():
+    """Two CTAs per system (a cluster of two splitting the convolution tasks and the Phi
+    points) compute every value with the same code as one CTA per system: the 64-point
+    isotherm converges to the same bits, with the same evaluation counts."""
+    import bench
+    import cdft_b200 as cd
+    specs = bench.isotherm_specs(0)[::4]
+    systems, rho0 = bench.build_systems(specs, "fp64")
+    method = cd.AASol.for_system(None, **bench.SOLVER)
+    old = cd.tuning("pers_cluster")
+    out = {}
+    try:
+        for c in (0, 1):
+            cd.tuning("pers_cluster", c)
+            rr = [r.copy() for r in rho0]
+            res = cd.batch_converge(systems, rr, method=method, engine="persistent")
+            out[c] = (rr, [r.evaluations for r in res], [r.errcode for r in res])
+    finally:
+        cd.tuning("pers_cluster", old)
+    assert out[0][1] == out[1][1] and out[0][2] == out[1][2]
+    for a, b in zip(out[0][0], out[1][0]):
+        assert np.array_equal(a, b)
