@@ -92,21 +92,23 @@ __device__ __forceinline__ void block_reduce_to_smem(double* vals, int K, double
 // window is a ring of PERS_R registers whose rotation is resolved at compile time
 // (the q loop is unrolled by PERS_R), so a step is one tap load, one window load
 // and PERS_R independent FMAs.
-// Tasks task0, task0 + tstride, ... of the stage (a cluster splits them between its CTAs);
-// out2, when not null, receives a second copy of every output (the peer CTA's buffer).
+// The fields f = frank, frank + fstride, ... of the stage (a cluster of fstride CTAs splits
+// the fields between them); out2, when not null, receives a second copy of every output
+// (the peer CTA's buffer).
 template <typename T, int NC>
 __device__ __forceinline__ void pers_conv(const T* __restrict__ ext, bool shared_input, const T* __restrict__ taps,
                                           T* __restrict__ out, int out_comp_stride, int N, int nconv, T scale,
-                                          int task0, int tstride, T* out2)
+                                          int frank, int fstride, T* out2)
 {
     const int lane = threadIdx.x & 31;
     const int EXTN = pers_extp(N), OFF = pers_off(N);   // FP32 rows: logical positions, row stride extp
     const int ntiles = (N + PERS_TILE - 1) / PERS_TILE;
-    const int ntask = NC * nconv * ntiles;
-    for (int task = task0; task < ntask; task += tstride) {
+    const int nfm = (nconv - frank + fstride - 1) / fstride;
+    const int ntask = NC * nfm * ntiles;
+    for (int task = threadIdx.x >> 5; task < ntask; task += PERS_WARPS) {
         const int tile = task % ntiles;
-        const int f = (task / ntiles) % nconv;
-        const int i = task / (ntiles * nconv);
+        const int f = ((task / ntiles) % nfm) * fstride + frank;
+        const int i = task / (ntiles * nfm);
         const T* in = ext + (size_t)(shared_input ? i : i * nconv + f) * EXTN + OFF;
         const T* tp = taps + (size_t)(i * nconv + f) * pers_ts(N) + PERS_TPAD;
         const int j0 = tile * PERS_TILE + lane;
@@ -167,20 +169,21 @@ __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, do
 template <int NC>
 __device__ __forceinline__ void pers_conv_dmma(const double* __restrict__ ext, bool shared_input,
                                                const double* __restrict__ taps, double* __restrict__ out,
-                                               int out_comp_stride, int N, int nconv, double scale, int task0,
-                                               int tstride, double* out2)
+                                               int out_comp_stride, int N, int nconv, double scale, int frank,
+                                               int fstride, double* out2)
 {
     const int lane = threadIdx.x & 31;
     const int EXTP = pers_extp(N), OFF = pers_off(N), TS = pers_ts(N);
     const int U = (N + 7) / 8;          // 8-output columns
     const int nut = (U + 7) / 8;        // warp tiles of 8 columns
     const int D = (N + 14) / 8;         // tap blocks: 8 (D - 1) + 7 >= N - 1
-    const int ntask = NC * nconv * nut;
+    const int nfm = (nconv - frank + fstride - 1) / fstride;   // fields of this CTA: f = frank + fstride fl
+    const int ntask = NC * nfm * nut;
     const int r = lane >> 2, k = lane & 3;   // A row / C row, A column / B row
-    for (int task = task0; task < ntask; task += tstride) {
+    for (int task = threadIdx.x >> 5; task < ntask; task += PERS_WARPS) {
         const int ut = task % nut;
-        const int f = (task / nut) % nconv;
-        const int i = task / (nut * nconv);
+        const int f = ((task / nut) % nfm) * fstride + frank;
+        const int i = task / (nut * nfm);
         const double* tp = taps + (size_t)(i * nconv + f) * TS + PERS_TPAD;   // tp[q] = 0 outside [0, N)
         const double* in = ext + (size_t)(shared_input ? i : i * nconv + f) * EXTP;
         const int u0 = ut * 8;
@@ -222,12 +225,12 @@ __device__ __forceinline__ void pers_conv_dmma(const double* __restrict__ ext, b
 template <typename T, int NC>
 __device__ __forceinline__ void pers_conv_any(const T* __restrict__ ext, bool shared_input, const T* __restrict__ taps,
                                               T* __restrict__ out, int out_comp_stride, int N, int nconv, T scale,
-                                              int task0, int tstride, T* out2)
+                                              int frank, int fstride, T* out2)
 {
     if constexpr (sizeof(T) == 8)
-        pers_conv_dmma<NC>(ext, shared_input, taps, out, out_comp_stride, N, nconv, scale, task0, tstride, out2);
+        pers_conv_dmma<NC>(ext, shared_input, taps, out, out_comp_stride, N, nconv, scale, frank, fstride, out2);
     else
-        pers_conv<T, NC>(ext, shared_input, taps, out, out_comp_stride, N, nconv, scale, task0, tstride, out2);
+        pers_conv<T, NC>(ext, shared_input, taps, out, out_comp_stride, N, nconv, scale, frank, fstride, out2);
 }
 
 // The Anderson section of one fixed-point step (the QR downdate and the vector slots
@@ -313,7 +316,6 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
         nf_peer = cl.map_shared_rank(nf, rank ^ 1);
         ip_peer = cl.map_shared_rank(ip, rank ^ 1);
     }
-    const int task0 = rank * PERS_WARPS + (tid >> 5), tstride = CL * PERS_WARPS;
     auto stage_sync = [&]() {
         if constexpr (CL == 2) cooperative_groups::this_cluster().sync();
         else __syncthreads();
@@ -371,14 +373,16 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
             nf[(i * NF) * N + j] = T(S.NA * S.rho[e]);
         }
         __syncthreads();
-        pers_conv_any<T, NC>(ext, true, taps, nf + N, NF * N, N, NCONV, NA, task0, tstride,
+        pers_conv_any<T, NC>(ext, true, taps, nf + N, NF * N, N, NCONV, NA, rank, CL,
                              nf_peer ? nf_peer + N : nullptr);
         stage_sync();
         // ---- fused Phi / dPhi/dn, in place: two threads per point ----
         // items j < N: hard sphere + association (fields 1 .. 2 + ND); items N + j: chain +
         // dispersion (fields 0, 3 + ND .. 5 + ND).  The two halves read and write disjoint
         // fields, and they fall in different warps except around item N.
-        for (int w = rank * PERS_THREADS + tid; w < 2 * N; w += CL * PERS_THREADS) {
+        // (CL = 2: rank 0 takes the hard-sphere halves, rank 1 the chain + dispersion halves)
+        const int w_end = (CL == 2) ? (rank + 1) * N : 2 * N;
+        for (int w = ((CL == 2) ? rank * N : 0) + tid; w < w_end; w += PERS_THREADS) {
             const bool first = w < N;
             const int j = first ? w : w - N;
             T n[NC][NF], g[NC][NF];
@@ -403,15 +407,20 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
         stage_sync();
         // ---- adjoint convolutions (integrate_field!) ----
         {
-            for (int k = tid; k < NC * NCONV * EXTN; k += PERS_THREADS) {
-                const int slot = k / EXTN, u = k - slot * EXTN;
-                const int i = slot / NCONV, f = slot - i * NCONV;
+            // the extended inputs of this CTA's fields only (f = rank + CL fl)
+            constexpr int NFM0 = (NCONV + CL - 1) / CL;
+            const int nfm = (NCONV - rank + CL - 1) / CL;
+            for (int k = tid; k < NC * NFM0 * EXTN; k += PERS_THREADS) {
+                const int ms = k / EXTN, u = k - ms * EXTN;
+                const int i = ms / NFM0, fl = ms - i * NFM0;
+                if (fl >= nfm) continue;
+                const int f = fl * CL + rank, slot = i * NCONV + f;
                 int j = (u - OFF) % N;
                 j += (j < 0) ? N : 0;
                 ext[(size_t)slot * EXTP + (sizeof(T) == 8 ? pers_pos(u) : u)] = nf[(i * NF + f + 1) * N + j];
             }
             __syncthreads();
-            pers_conv_any<T, NC>(ext, false, taps, ip, NCONV * N, N, NCONV, T(1), task0, tstride, ip_peer);
+            pers_conv_any<T, NC>(ext, false, taps, ip, NCONV * N, N, NCONV, T(1), rank, CL, ip_peer);
         }
         stage_sync();
         // ---- Euler-Lagrange step + aa_point! bookkeeping ----
