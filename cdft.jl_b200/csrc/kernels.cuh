@@ -562,6 +562,88 @@ __device__ void aa_downdate(AAState& A)
     for (int r = 0; r < m; ++r) R[r + (m - 1) * m] = 0.0;
 }
 
+// aa_downdate for a compile-time depth M, by one thread with R and Qx in registers: the same
+// operations in the same order (so the same bits) without the round trips through the
+// solver state's memory between dependent steps.  Not inlined: its registers are its own.
+template <int M>
+__device__ __noinline__ void aa_downdate_reg(AAState& A)
+{
+    constexpr int n = M - 1;
+    double R[M][M];
+#pragma unroll
+    for (int c = 0; c < M; ++c)
+#pragma unroll
+        for (int r = 0; r < M; ++r) R[r][c] = A.R[r + c * M];
+    double tau[n], v1[n];
+#pragma unroll
+    for (int j = 0; j < n; ++j) {
+        const double alpha = R[j][j + 1];
+        const double x = R[j + 1][j + 1];
+        const double xnorm = sqrt(x * x);
+        if (xnorm == 0.0) {
+            tau[j] = 0.0;
+            v1[j] = 0.0;
+            continue;
+        }
+        const double beta = -copysign(hypot(alpha, xnorm), alpha);
+        tau[j] = (beta - alpha) / beta;
+        v1[j] = x * (1.0 / (alpha - beta));
+        R[j][j + 1] = beta;
+        R[j + 1][j + 1] = 0.0;
+#pragma unroll
+        for (int c = j + 1; c < n; ++c) {
+            const double w = fma(v1[j], R[j + 1][c + 1], R[j][c + 1]);
+            R[j][c + 1] = fma(-tau[j], w, R[j][c + 1]);
+            R[j + 1][c + 1] = fma(-(tau[j] * v1[j]), w, R[j + 1][c + 1]);
+        }
+    }
+    double Qx[M][n];
+#pragma unroll
+    for (int c = 0; c < n; ++c) {
+#pragma unroll
+        for (int r = 0; r < M; ++r) Qx[r][c] = (r == c) ? 1.0 : 0.0;
+#pragma unroll
+        for (int j = n - 1; j >= 0; --j) {
+            const double w = fma(v1[j], Qx[j + 1][c], Qx[j][c]);
+            Qx[j][c] = fma(-tau[j], w, Qx[j][c]);
+            Qx[j + 1][c] = fma(-(tau[j] * v1[j]), w, Qx[j + 1][c]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < n; ++j) {
+        A.tau[j] = tau[j];
+        A.v1[j] = v1[j];
+    }
+#pragma unroll
+    for (int c = 0; c < n; ++c)
+#pragma unroll
+        for (int r = 0; r < M; ++r) {
+            A.Qx[r + c * M] = Qx[r][c];
+            A.Rn[r + c * M] = (r <= c) ? R[r][c + 1] : 0.0;
+        }
+#pragma unroll
+    for (int r = 0; r < M; ++r) A.Rn[r + n * M] = 0.0;
+}
+
+// aa_downdate through the register form for depths up to 12 (deeper histories: the loop form)
+__device__ void aa_downdate_fast(AAState& A)
+{
+    switch (A.m) {
+    case 2: aa_downdate_reg<2>(A); return;
+    case 3: aa_downdate_reg<3>(A); return;
+    case 4: aa_downdate_reg<4>(A); return;
+    case 5: aa_downdate_reg<5>(A); return;
+    case 6: aa_downdate_reg<6>(A); return;
+    case 7: aa_downdate_reg<7>(A); return;
+    case 8: aa_downdate_reg<8>(A); return;
+    case 9: aa_downdate_reg<9>(A); return;
+    case 10: aa_downdate_reg<10>(A); return;
+    case 11: aa_downdate_reg<11>(A); return;
+    case 12: aa_downdate_reg<12>(A); return;
+    default: aa_downdate(A); return;
+    }
+}
+
 // aa_downdate by one warp: lane 0 forms each reflector, the lanes update the trailing
 // columns and build Qx column by column; per element the arithmetic of aa_downdate (a
 // reflector with tau = v1 = 0 leaves the columns unchanged).  A lives in shared memory.
@@ -724,7 +806,7 @@ __device__ __forceinline__ void aa_plan_downdate(AAState& A, bool defer)
     A.downdate = (A.m > 1 && A.k >= A.m) ? 1 : 0;
     if (A.downdate) {
         if (defer) A.pad0 = 1;
-        else aa_downdate(A);
+        else aa_downdate_fast(A);
     }
 }
 

@@ -464,10 +464,13 @@ persistent_kernel(const SysDev* __restrict__ sys, AAState* __restrict__ st, int*
                 if (tid == 0) ctl_apply(sA, op, slot, sums, done_ptr, true);
             }
             __syncthreads();
-            if (sA.pad0) {   // the next step's QR downdate, from this step's R, on warp 0
-                if (tid < 32) aa_downdate_warp(sA, tid);
+            if (sA.pad0) {   // the next step's QR downdate, from this step's R, by one thread
                 __syncthreads();
-                if (tid == 0) sA.pad0 = 0;
+                if (tid == 0) {
+                    aa_downdate_fast(sA);
+                    sA.pad0 = 0;
+                }
+                __syncthreads();
             }
         }
     }
