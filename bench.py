@@ -418,6 +418,9 @@ def _solutes3d_system(N, precision):
 #   (d) Anderson vectors    8 nc (2 m + 6)                     208
 # = 512 B in FP64 (s = 8), 364 B mixed (s = 4); FFT-internal passes are excluded.
 BYTES_3D_ITER = {"fp64": 512, "mixed": 364}
+# DRAM bytes per point of one FP64 Anderson iteration as measured (ncu, dram__bytes_read.sum +
+# dram__bytes_write.sum over one iteration's 20 launches at 128^3: 2.494e9 B / 128^3)
+TRAFFIC_3D_ITER_BYTES_PER_POINT = 1189.3
 # What the FFT pipeline of one functional derivative moves per point (x, y, z passes
 # of rho, the 8 convolved fields and the 8 dPhi/dn fields, Phi and the EL output;
 # the half spectrum holds 16 B per (N/2+1)/N point, counted as 8 B per real point):
@@ -489,7 +492,10 @@ def solutes3d_run(N, precision, reps=2):
         "functional_derivative_ms": round(ms_eval.value, 4),
         "roofline": {
             "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "peak_source": src,
-            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+            "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": (TRAFFIC_3D_ITER_BYTES_PER_POINT * N ** 3 if precision == "fp64" else None),
+            "traffic_unit": ("DRAM bytes per iteration, all of its launches (ncu at 128^3 in the Anderson phase, "
+                             "per point scaled to N^3; profiles/solutes3d_128_fp64_kernels.md)"),
             "algorithmic_bytes_per_point_iteration": BYTES_3D_ITER[precision]},
         "functional_derivative_pipeline": {
             "bytes_per_point": BYTES_3D_PIPE[precision], "achieved_gbs": round(pipe, 1),
