@@ -734,7 +734,7 @@ def batch_properties(systems, rhos=None):
 
 def F_res_grad(system, rho):
     """dF_res/d(sigma_k [A], eps_k/k_B [K], m_k) at a fixed profile, shape (nc, 3);
-    units of F_res (1D).  No counterpart in the reference."""
+    units of F_res (k_B T per m^2 in 1D, k_B T in 3D).  No counterpart in the reference."""
     _check_rho(system, rho)
     out = np.zeros(3 * system.nc)
     _lib.check(_LIB.cdft_free_energy_res_grad(system._plan, _lib.dptr(rho), _lib.dptr(out)))
@@ -758,11 +758,15 @@ def grad_params(system, rho, dmu_dtheta=None, dp_dtheta=None):
         _lib.check(_LIB.cdft_grad_params(system._plan, _lib.dptr(rho), mu_p, dp_p, _lib.dptr(out)))
     else:
         st = system.structure
-        if st.nd != 1 or st.coord != "cart" or not all(isinstance(f, Steele) for f in system.external_field):
-            raise NotImplementedError("parameter gradients with external fields: planar Steele walls")
-        z = st.coords(0)
         T = st.conditions[1]
-        dv = np.ascontiguousarray(sum(f.potential_dtheta(system.model, z, T) for f in system.external_field))
+        if st.coord == "cart" and st.nd == 3 and all(isinstance(f, HardSphereSolutes) for f in system.external_field):
+            # V_ext / k_B T of hard solutes is a constant height: no parameter dependence
+            dv = np.zeros((nt, system.nc) + tuple(reversed(st.ngrid)))
+        elif st.nd == 1 and st.coord == "cart" and all(isinstance(f, Steele) for f in system.external_field):
+            z = st.coords(0)
+            dv = np.ascontiguousarray(sum(f.potential_dtheta(system.model, z, T) for f in system.external_field))
+        else:
+            raise NotImplementedError("parameter gradients with external fields: planar Steele walls, hard solutes")
         _lib.check(_LIB.cdft_grad_params_ext(system._plan, _lib.dptr(rho), mu_p, dp_p, _lib.dptr(dv), _lib.dptr(out)))
     return out.reshape(system.nc, 3)
 
@@ -785,31 +789,29 @@ def grand_potential(system, rho, quadrature="simpson"):
     if quadrature != "uniform":
         raise ValueError("quadrature is 'simpson' or 'uniform'")
     st = system.structure
-    if st.nd != 1 or st.coord != "cart":
-        raise NotImplementedError("the uniform quadrature is defined for 1D Cartesian grids")
-    lb, ub = st.bounds[0]
-    dz = (ub - lb) / st.ngrid[0]
+    if st.coord != "cart":
+        raise NotImplementedError("the uniform quadrature is defined for Cartesian grids")
+    dv = float(np.prod([(ub - lb) / n for (lb, ub), n in zip(st.bounds, st.ngrid)]))   # volume per point
+    n_pts = int(np.prod(st.ngrid))
     p, _ = st.conditions
     mu = system.model.chemical_potential(st.rho_bulk, T)
-    # F_res by the device (Simpson) is not what is needed here: the uniform sum of Phi
-    n_pts = st.ngrid[0]
     f_res = _uniform_F_res(system, rho)
-    f_id = sum(float(np.sum(N_A * rho[i] * (np.log(rho[i]) - 1.5 * np.log(T) - 1))) for i in range(system.nc)) * dz
-    om = (f_res + f_id) * K_B * T - sum(mu[i] * float(np.sum(rho[i])) * dz for i in range(system.nc)) + p * n_pts * dz
+    f_id = sum(float(np.sum(N_A * rho[i] * (np.log(rho[i]) - 1.5 * np.log(T) - 1))) for i in range(system.nc)) * dv
+    om = (f_res + f_id) * K_B * T - sum(mu[i] * float(np.sum(rho[i])) * dv for i in range(system.nc)) + p * n_pts * dv
     if system.vext is not None:
-        om += N_A * K_B * T * sum(float(np.sum(rho[i] * system.vext[i])) for i in range(system.nc)) * dz
+        om += N_A * K_B * T * sum(float(np.sum(rho[i] * system.vext[i])) for i in range(system.nc)) * dv
     return om
 
 
 def _uniform_F_res(system, rho):
-    """F_res (k_B T per m^2) summed with uniform weights dz: Phi at every point from the
-    device (cdft_phi_pointwise on the plan's own weighted densities)."""
+    """F_res (k_B T per m^2 in 1D, k_B T in 3D) summed with uniform weights: Phi at every point
+    from the device (cdft_phi_field)."""
     _check_rho(system, rho)
-    f = np.empty(system.structure.ngrid[0])
-    _lib.check(_LIB.cdft_phi_field(system._plan, _lib.dptr(rho), _lib.dptr(f)))
     st = system.structure
-    lb, ub = st.bounds[0]
-    return float(np.sum(f)) * (ub - lb) / st.ngrid[0] / system.L ** 3
+    f = np.empty(int(np.prod(st.ngrid)))
+    _lib.check(_LIB.cdft_phi_field(system._plan, _lib.dptr(rho), _lib.dptr(f)))
+    dv = float(np.prod([(ub - lb) / n for (lb, ub), n in zip(st.bounds, st.ngrid)]))
+    return float(np.sum(f)) * dv / system.L ** 3
 
 
 def dgamma_dtheta(system, rho):

@@ -1700,7 +1700,10 @@ int ddft_rhs(cdft_plan* p, const double* eta, double* deta, bool is_dev)
 template <int NC>
 int launch_grad_points(cdft_plan* p, Batch* b, const double* dn, double* gp, double* kt)
 {
-    grad_points_kernel<NC><<<(p->N + 127) / 128, 128, 0, p->stream>>>(b->d_sys, dn, gp, kt);
+    if (p->desc.nd == 3)
+        grad_points_kernel<NC, 3><<<(p->N + 127) / 128, 128, 0, p->stream>>>(b->d_sys, dn, gp, kt);
+    else
+        grad_points_kernel<NC, 1><<<(p->N + 127) / 128, 128, 0, p->stream>>>(b->d_sys, dn, gp, kt);
     CHECK_LAUNCH();
     return 0;
 }
@@ -2094,6 +2097,8 @@ int cdft_tuning_set(const char* name, int value)
 // weights dz of the discrete functional whose gradient the pointwise Euler-Lagrange equation
 // of converge! is (what cdft_grad_params differentiates)
 static int fres_grad_impl(cdft_plan* plan, const double* rho, double* dF, bool uniform);
+static int fres_grad_chain(cdft_plan* plan, const std::vector<double>& G, const std::vector<double>& Gd, double* dF);
+static int fres_grad3d(cdft_plan* plan, Batch* b, bool uniform, int NP, double* dF);
 
 int cdft_free_energy_res_grad(cdft_plan* plan, const double* rho, double* dF)
 {
@@ -2105,8 +2110,8 @@ static int fres_grad_impl(cdft_plan* plan, const double* rho, double* dF, bool u
 {
     if (!plan || !rho || !dF) return set_error(CDFT_E_INVALID, "NULL argument");
     const cdft_system_desc& d = plan->desc;
-    if (d.nd != 1 || d.coord != CDFT_COORD_CART)
-        return set_error(CDFT_E_UNSUPPORTED, "the parameter gradient is implemented for 1D Cartesian grids");
+    if (d.coord != CDFT_COORD_CART || (d.nd != 1 && d.nd != 3))
+        return set_error(CDFT_E_UNSUPPORTED, "the parameter gradient is implemented for 1D and 3D Cartesian grids");
     if (d.n_assoc > 1)
         return set_error(CDFT_E_UNSUPPORTED, "the parameter gradient covers one association pair");
     const int nc = d.nc, N = plan->N;
@@ -2130,13 +2135,14 @@ static int fres_grad_impl(cdft_plan* plan, const double* rho, double* dF, bool u
     const int nconv = S.nconv;
     const size_t ne = (size_t)S.n_elem;
     CU(cudaMemcpyAsync(S.rho, rho, ne * sizeof(double), cudaMemcpyHostToDevice, plan->stream));
+    const int NP = 2 * nc + 2 * nc * nc + 2;
+    if (d.nd == 3) return fres_grad3d(plan, b, uniform, NP, dF);
     // weighted densities (FP64 in every precision mode)
     {
         const size_t smem = (size_t)(CONV_QC + CONV_TILE + CONV_QC + 31) * sizeof(double);
         conv1d_kernel<double><<<b->ntasks, CONV_WARPS * 32, smem, plan->stream>>>(b->d_tasks, b->d_sys, nullptr, 0);
         CHECK_LAUNCH();
     }
-    const int NP = 2 * nc + 2 * nc * nc + 2;
     const double wf[6] = {0.5, 0.5, 0.5, 1.0, 1.0, PSI_DISP};
     double *d_dt = nullptr, *d_dn = nullptr, *d_gp = nullptr, *d_kt = nullptr, *d_scale = nullptr;
     const size_t ntap = (size_t)nc * nconv * N;
@@ -2196,7 +2202,17 @@ static int fres_grad_impl(cdft_plan* plan, const double* rho, double* dF, bool u
         for (int k = 1; k <= N; ++k) acc.add(coef(k, N) * kt[(size_t)i * N + k - 1]);
         Gd[i] = acc.value() * w;
     }
-    // chain to theta = (sigma_k [A], eps_k / k_B [K], m_k) with the length unit L held fixed
+    return fres_grad_chain(plan, G, Gd, dF);
+}
+
+// dF_res/dP_q (G) and dF_res/dd_i through the kernels (Gd) chained to theta = (sigma_k [A],
+// eps_k / k_B [K], m_k) with the length unit L held fixed
+static int fres_grad_chain(cdft_plan* plan, const std::vector<double>& G, const std::vector<double>& Gd, double* dF)
+{
+    const cdft_system_desc& d = plan->desc;
+    const SysDev& S = plan->sys;
+    const int nc = d.nc;
+    const double L = d.L, T = d.T;
     const int iM = 0, iD = nc, iC1 = 2 * nc, iC2 = 2 * nc + nc * nc, iAD = 2 * nc + 2 * nc * nc, iAK = iAD + 1;
     const PhiParams& P = S.phi;
     for (int k = 0; k < nc; ++k) {
@@ -2247,6 +2263,101 @@ static int fres_grad_impl(cdft_plan* plan, const double* rho, double* dF, bool u
     return 0;
 }
 
+// 3D parameter gradient of F_res.  The weighted densities' dependence on the diameters goes
+// through the FFT pipeline with derivative kernel tables: d omega_hat / dR of each table's
+// kernel times dR/dd = 2 pi w_t (type 1: 2 cos(wR) / 2 pi; type 2: 4 pi R sin(wR) / w / (2 pi)^3,
+// 4 pi R^2 / (2 pi)^3 at w = 0; the vector fields take the type-2 table times i w_d, as the
+// kernels do).  The pipeline with those tables gives dn_f = N_A L^3 rho (*) d omega_f / d d_i in
+// the plan's field buffer; the pipeline with the plan's own tables then leaves the weighted
+// densities there for the per-point terms.
+static int fres_grad3d(cdft_plan* p, Batch* b, bool uniform, int NP, double* dF)
+{
+    const cdft_system_desc& d = p->desc;
+    SysDev& S = p->sys;
+    const int nc = d.nc, L3 = p->L3;
+    const size_t npts = (size_t)L3 * L3 * L3;
+    const double PI = 3.14159265358979323846, TWO_PI = 2.0 * PI;
+    const int types[5] = {1, 2, 2, 1, 2};
+    const double wf[5] = {0.5, 0.5, 1.0, 1.0, PSI_DISP};
+    std::vector<double> tab((size_t)nc * 5 * (p->k2max + 1));
+    for (int i = 0; i < nc; ++i)
+        for (int t = 0; t < 5; ++t) {
+            const double dR = TWO_PI * wf[t], R = dR * S.phi.d[i];
+            for (int k2 = 0; k2 <= p->k2max; ++k2) {
+                const double w = std::sqrt((double)k2) * p->w0;
+                double v;
+                if (types[t] == 1) v = 2.0 * std::cos(w * R) / TWO_PI;
+                else v = (w == 0.0 ? 4.0 * PI * R * R : 4.0 * PI * R * std::sin(w * R) / w) / (TWO_PI * TWO_PI * TWO_PI);
+                tab[((size_t)i * 5 + t) * (p->k2max + 1) + k2] = v * dR;
+            }
+        }
+    double *d_tab = nullptr, *d_dn = nullptr, *d_gp = nullptr, *d_kt = nullptr;
+    const size_t nfield = (size_t)nc * S.nconv * npts;
+    int rc = 0;
+    auto cleanup = [&]() {
+        cudaFree(d_tab);
+        cudaFree(d_dn);
+        cudaFree(d_gp);
+        cudaFree(d_kt);
+    };
+    if (cudaMalloc(&d_tab, tab.size() * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&d_dn, nfield * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&d_gp, (size_t)NP * npts * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&d_kt, (size_t)nc * npts * sizeof(double)) != cudaSuccess) {
+        cleanup();
+        return set_error(CDFT_E_CUDA, "3D parameter gradient: out of device memory");
+    }
+    cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, p->stream);
+    double* keep = p->d_ktab;
+    p->d_ktab = d_tab;
+    rc = launch_eval_stages<double>(b, nullptr, false);   // S.part = d n_f / d d_i (Phi of it is unused)
+    p->d_ktab = keep;
+    if (!rc) {
+        cudaMemcpyAsync(d_dn, S.part, nfield * sizeof(double), cudaMemcpyDeviceToDevice, p->stream);
+        rc = launch_eval_stages<double>(b, nullptr, false);   // S.part = the weighted densities
+    }
+    if (!rc) {
+        switch (nc) {
+        case 1: rc = launch_grad_points<1>(p, b, d_dn, d_gp, d_kt); break;
+        case 2: rc = launch_grad_points<2>(p, b, d_dn, d_gp, d_kt); break;
+        case 3: rc = launch_grad_points<3>(p, b, d_dn, d_gp, d_kt); break;
+        case 4: rc = launch_grad_points<4>(p, b, d_dn, d_gp, d_kt); break;
+        default: rc = set_error(CDFT_E_UNSUPPORTED, "nc=%d", nc);
+        }
+    }
+    std::vector<double> gp, kt;
+    if (!rc) {
+        gp.resize((size_t)NP * npts);
+        kt.resize((size_t)nc * npts);
+        cudaMemcpyAsync(gp.data(), d_gp, gp.size() * sizeof(double), cudaMemcpyDeviceToHost, p->stream);
+        cudaMemcpyAsync(kt.data(), d_kt, kt.size() * sizeof(double), cudaMemcpyDeviceToHost, p->stream);
+        const cudaError_t e = cudaStreamSynchronize(p->stream);
+        if (e != cudaSuccess) rc = set_error(CDFT_E_CUDA, "3D parameter gradient: %s", cudaGetErrorString(e));
+    }
+    cleanup();
+    if (rc) return rc;
+    // Simpson weights per dimension (integrals.jl:28-41) or the uniform dz^3
+    auto coef = [uniform](int k, int n) {
+        return uniform ? 3.0 : ((k == 1 || k == n) ? 1.0 : ((k % 2 == 0) ? 4.0 : 2.0));
+    };
+    const double Lr = d.L;
+    const double w = (p->dz[0] / 3.0) * (p->dz[1] / 3.0) * (p->dz[2] / 3.0) / (Lr * Lr * Lr);
+    std::vector<double> G(NP), Gd(nc);
+    auto wsum = [&](const double* f) {
+        KSum acc;
+        for (int z = 1; z <= L3; ++z)
+            for (int y = 1; y <= L3; ++y) {
+                const double cyz = coef(z, L3) * coef(y, L3);
+                const double* row = f + ((size_t)(z - 1) * L3 + (y - 1)) * L3;
+                for (int x = 1; x <= L3; ++x) acc.add(cyz * coef(x, L3) * row[x - 1]);
+            }
+        return acc.value() * w;
+    };
+    for (int q = 0; q < NP; ++q) G[q] = wsum(gp.data() + (size_t)q * npts);
+    for (int i = 0; i < nc; ++i) Gd[i] = wsum(kt.data() + (size_t)i * npts);
+    return fres_grad_chain(p, G, Gd, dF);
+}
+
 }  // extern "C"
 
 namespace {
@@ -2269,14 +2380,14 @@ int grad_params_impl(cdft_plan* plan, const double* rho, const double* dmu_dthet
     // uniform weights dz (the adjoint of the periodic convolution), so every integral below
     // uses them.  surface_tension's Simpson weights differ from it where the profile is not
     // resolved on the grid (sharp adsorbed layers); for resolved profiles the two agree.
-    const double dz = plan->dz[0];
+    const double dz = (d.nd == 3) ? plan->dz[0] * plan->dz[1] * plan->dz[2] : plan->dz[0];   // volume per point
     std::vector<double> nint(nc);
     for (int i = 0; i < nc; ++i) {
         KSum acc;
         for (int k = 0; k < N; ++k) acc.add(rho[(size_t)i * N + k]);
         nint[i] = acc.value() * dz;
     }
-    const double one = N * dz;
+    const double one = (double)N * dz;
     const double kB = 1.380649e-23, NAVO = 6.02214076e23;
     for (int t = 0; t < np; ++t) {
         double v = kB * d.T * dF[t];

@@ -1126,17 +1126,17 @@ __global__ void dconv1d_kernel(int N, int nconv, const double* __restrict__ dtap
 
 // per point j: gp[q*N + j] = dPhi/dP_q (explicit parameters) and
 // kt[i*N + j] = sum_f dPhi/dn_{i,f} * dn_{i,f}/dd_i (kernels)
-template <int NC>
+template <int NC, int ND>
 __global__ void grad_points_kernel(const SysDev* __restrict__ sys, const double* __restrict__ dn,
                                    double* __restrict__ gp_out, double* __restrict__ kt_out)
 {
     const SysDev& S = sys[0];
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= S.N) return;
-    double n[NC][7], g[NC][7];
+    double n[NC][6 + ND], g[NC][6 + ND];
     double gp[PhiParamIdx<NC>::NP];
-    load_n<double, NC, 1>(S, j, n);
-    phi_grad<double, NC, 1, true>(S.phi, n, g, gp);
+    load_n<double, NC, ND>(S, j, n);
+    phi_grad<double, NC, ND, true>(S.phi, n, g, gp);
     for (int q = 0; q < PhiParamIdx<NC>::NP; ++q) gp_out[(size_t)q * S.N + j] = gp[q];
 #pragma unroll
     for (int i = 0; i < NC; ++i) {

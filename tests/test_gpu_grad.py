@@ -66,8 +66,8 @@ def test_F_res_grad_matches_oracle_fd(case):
 
 
 def test_grad_params_scope():
-    """Planar Steele walls are differentiated (their dV/dtheta enters the gradient); the
-    3D engine has no parameter gradient and hard solutes no dV/dtheta: both are refused."""
+    """Planar Steele walls are differentiated (their dV/dtheta enters the gradient); radial
+    grids have no parameter gradient and are refused."""
     import cdft_b200 as cd
     from cdft_b200._lib import CDFTError
     sp, _ = S.methane_wall(N=101)
@@ -76,10 +76,10 @@ def test_grad_params_scope():
     g = cd.grad_params(sp, rho)
     assert g.shape == (1, 3) and np.all(np.isfinite(g))
     pm, _ = S.models(["argon"])
-    s3 = cd.DFTSystem(pm, cd.Uniform3DCart((1e5, 100.0), [0.021e30 / cd.N_A], [0.0, 8 * 3.4e-10], 32))
+    r1 = cd.DFTSystem(pm, cd.Uniform1DSphr((1e5, 100.0), [0.021e30 / cd.N_A], [0.0, 8 * 3.4e-10], 64))
     with pytest.raises(CDFTError):
-        cd.F_res_grad(s3, cd.initialize_profiles(s3))
-    s3.close()
+        cd.F_res_grad(r1, cd.initialize_profiles(r1))
+    r1.close()
 
 
 def _lle_system(model, N, box_sigmas=60.0, T=298.15, p=1e5):
@@ -175,3 +175,90 @@ def test_dgrand_potential_dtheta_slit_pore_matches_fd():
     grad = cd.grad_params(sys0, rho0, dmu, dp).ravel()
     err = np.abs(grad - fd) / np.max(np.abs(fd))
     assert float(np.max(err)) < 1e-5, (grad, fd)
+
+
+def _argon_box(N=32, box_sigmas=8.0, solutes=False):
+    import cdft_b200 as cd
+    from oracle import functional as fn
+    pm, om = S.models(["argon"])
+    s = om.sigma[0]
+    box = box_sigmas * s
+    rb = 0.021e30 / cd.N_A
+    field = None
+    if solutes:
+        centres = cd.HardSphereSolutes.seeded(4, 1.2 * s, box, 2 * box / N, seed=1)
+        field = cd.HardSphereSolutes(centres, 1.2 * s)
+    sp = cd.DFTSystem(pm, cd.Uniform3DCart((1e5, 100.0), [rb], [0.0, box], N), field)
+    st = fn.Structure((1e5, 100.0), [rb], [(0.0, box)] * 3, (N, N, N))
+    return sp, st, pm, rb, box
+
+
+def test_F_res_grad_3d_matches_oracle_fd():
+    """The 3D parameter gradient of F_res (explicit terms and the kernels' dependence on the
+    diameter through the FFT pipeline with derivative tables) against the oracle's central
+    differences of its 3D F_res, argon on a 32^3 box with a smooth non-uniform profile."""
+    import cdft_b200 as cd
+    from oracle import functional as fn
+    sp, st, pm, rb, box = _argon_box()
+    N = 32
+    x = np.arange(N) / N
+    Z, Y, X = np.meshgrid(x, x, x, indexing="ij")
+    rho = rb * (1 + 0.2 * np.sin(2 * np.pi * X) * np.cos(2 * np.pi * Y) + 0.1 * np.sin(4 * np.pi * Z))[None]
+    rho = np.ascontiguousarray(rho)
+    g = cd.F_res_grad(sp, rho).ravel()
+    theta0 = pm.theta()
+    fd = np.empty_like(theta0)
+    for t in range(theta0.size):
+        h = 1e-5 * abs(theta0[t])
+        vals = []
+        for sgn in (1.0, -1.0):
+            th = theta0.copy()
+            th[t] += sgn * h
+            vals.append(fn.DFTSystem(_oracle_model(["argon"], th), st).F_res(rho))
+        fd[t] = (vals[0] - vals[1]) / (2 * h)
+    scale = np.maximum(np.abs(fd), 1e-4 * np.max(np.abs(fd)))
+    assert float(np.max(np.abs(g - fd) / scale)) < 1e-6, (g, fd)
+    sp.close()
+
+
+def test_dgrand_potential_dtheta_3d_solutes_matches_fd():
+    """d Omega / d theta of a converged 32^3 argon box with hard solutes (the uniform-weight
+    grand potential the converged profile is stationary in) against central differences
+    through converge at fixed bulk density."""
+    import cdft_b200 as cd
+    sp, st, pm, rb, box = _argon_box(solutes=True)
+    T = 100.0
+    kw = dict(beta=0.1, tol=1e-11, anderson_m=10, maxit=2000)
+
+    def build(model):
+        cen = sp.external_field[0].centres
+        return cd.DFTSystem(model, cd.Uniform3DCart((model.pressure([rb], T), T), [rb], [0.0, box], 32),
+                            cd.HardSphereSolutes(cen, sp.external_field[0].radius))
+
+    sys0 = build(pm)
+    rho0 = cd.initialize_profiles(sys0)
+    assert cd.converge(sys0, rho0, **kw).errcode == 0
+    theta0 = pm.theta()
+    dmu, dp, fd = np.zeros((1, 3)), np.zeros(3), np.zeros(3)
+    for t in range(3):
+        h = 1e-6 * abs(theta0[t])
+        vals, mus, ps = [], [], []
+        for sgn in (1.0, -1.0):
+            th = theta0.copy()
+            th[t] += sgn * h
+            mdl = pm.with_theta(th)
+            mus.append(mdl.chemical_potential([rb], T)[0])
+            ps.append(mdl.pressure([rb], T))
+            s2 = build(mdl)
+            r = rho0.copy()
+            assert cd.converge(s2, r, **kw).errcode in (0, -1)
+            vals.append(cd.grand_potential(s2, r, quadrature="uniform"))
+            s2.close()
+        fd[t] = (vals[0] - vals[1]) / (2 * h)
+        dmu[0, t] = (mus[0] - mus[1]) / (2 * h)
+        dp[t] = (ps[0] - ps[1]) / (2 * h)
+    grad = cd.grad_params(sys0, rho0, dmu, dp).ravel()
+    err = np.abs(grad - fd) / np.max(np.abs(fd))
+    assert float(np.max(err)) < 1e-5, (grad, fd)
+    sys0.close()
+    sp.close()
