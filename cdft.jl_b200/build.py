@@ -19,6 +19,7 @@ NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo",
     "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fopenmp", "-lgomp",   # host-side radial operator construction
 ]
 
 

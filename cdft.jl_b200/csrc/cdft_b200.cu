@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -74,6 +75,25 @@ bool g_const_done[64] = {false};   // per device: PC-SAFT constants uploaded to 
 
 struct Batch;
 
+// Dense radial operators on one device, shared by every plan of the same geometry,
+// length unit and diameters (an isotherm in one pore builds them once); freed with the
+// last plan that holds them.
+struct RadialOps {
+    int device = 0;
+    double* d_mats = nullptr;
+    RadialOps() = default;
+    RadialOps(const RadialOps&) = delete;
+    RadialOps& operator=(const RadialOps&) = delete;
+    ~RadialOps()
+    {
+        int cur = -1;
+        const bool other = cudaGetDevice(&cur) == cudaSuccess && cur != device;
+        if (other) cudaSetDevice(device);
+        cudaFree(d_mats);
+        if (other) cudaSetDevice(cur);
+    }
+};
+
 struct cdft_plan {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -91,7 +111,7 @@ struct cdft_plan {
     void* d_part = nullptr;
     void* d_dfield = nullptr;
     double* d_fval = nullptr;
-    double* d_mats = nullptr;     // radial: dense weighted-density operators (both stages)
+    std::shared_ptr<RadialOps> rops;   // radial: dense weighted-density operators (both stages)
     double* d_rw = nullptr;       // radial: quadrature weights on the device
     std::vector<double> rw;       // radial: quadrature weights of the integral (angular factor included)
     void* d_spec = nullptr;       // 3D: convolved-field spectra [comp][field][z][y][kx]
@@ -129,7 +149,10 @@ struct Batch {
     int graph_iters[2] = {0, 0};
     int vec_mb = CDFT_MAX_M;                          // compile-time depth bound of vec_kernel
     int graph_mb[2] = {0, 0};                         // ... captured in each graph
+    TunedShapes graph_tuned[2];                       // ... and the launch shapes they were captured with
     long long graph_launches[2] = {0, 0};             // kernel launches captured in each graph
+    DenseGroup* d_groups = nullptr;                   // radial: column tiles of systems sharing an operator
+    int ngroups = 0, group_blocks = 0;                // ... and the largest slots x row tiles among them
 };
 
 namespace {
@@ -162,6 +185,7 @@ void free_batch(Batch* b)
     cudaFree(b->d_pchunks);
     cudaFree(b->d_echunks);
     cudaFree(b->d_partials);
+    cudaFree(b->d_groups);
     cudaFree(b->d_done);
     cudaFree(b->d_hist);
     if (b->h_done) cudaFreeHost(b->h_done);
@@ -324,6 +348,14 @@ std::vector<double> bessel_zeros(double nu, int count)
     return z;
 }
 
+struct RadialKey {
+    int device, coord, N, nc, nconv, pad;   // no padding bytes: compared by memcmp
+    uint64_t R, L, d[CDFT_MAX_NC];          // bit patterns
+    bool operator<(const RadialKey& o) const { return std::memcmp(this, &o, sizeof(RadialKey)) < 0; }
+};
+std::mutex g_rops_mu;
+std::map<RadialKey, std::weak_ptr<RadialOps>> g_rops;
+
 int radial_build(cdft_plan* p)
 {
     const cdft_system_desc& d = p->desc;
@@ -345,6 +377,33 @@ int radial_build(cdft_plan* p)
         // int_0^R f r^(2 nu + 1) dr: Fourier-Bessel quadrature of the k -> 0 limit
         p->rw[m] = ang * 2.0 * R * R / (Sz * Sz * jn1[m] * jn1[m]) * std::pow(r[m], 2.0 * nu);
     }
+    CU(cudaMalloc(&p->d_rw, (size_t)N * sizeof(double)));
+    CU(cudaMemcpyAsync(p->d_rw, p->rw.data(), (size_t)N * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    S.qw = p->d_rw;
+    // the operators depend on the grid (coordinates, N, R), L and the diameters only
+    RadialKey key;
+    std::memset(&key, 0, sizeof(key));
+    key.device = p->device;
+    key.coord = d.coord;
+    key.N = N;
+    key.nc = nc;
+    key.nconv = nconv;
+    std::memcpy(&key.R, &R, sizeof(double));
+    std::memcpy(&key.L, &L, sizeof(double));
+    for (int i = 0; i < nc; ++i) std::memcpy(&key.d[i], &S.phi.d[i], sizeof(double));
+    {
+        std::lock_guard<std::mutex> lk(g_rops_mu);
+        auto it = g_rops.find(key);
+        if (it != g_rops.end()) {
+            if (auto ops = it->second.lock()) {
+                p->rops = ops;
+                S.mats = ops->d_mats;
+                CU(cudaStreamSynchronize(p->stream));
+                return 0;
+            }
+        }
+    }
+#pragma omp parallel for schedule(static)
     for (int m = 0; m < N; ++m)
         for (int q = 0; q < N; ++q)
             T[(size_t)m * N + q] = 2.0 * std::cyl_bessel_j(nu, j[m] * j[q] / Sz) / (jn1[m] * jn1[q] * Sz);
@@ -372,6 +431,7 @@ int radial_build(cdft_plan* p)
         for (int m = 0; m < N; ++m)
             for (int q = 0; q < N; ++q) TW[(size_t)m * N + q] = T[(size_t)m * N + q] * w[q];
         M.assign((size_t)N * N, 0.0);
+#pragma omp parallel for schedule(static)
         for (int m = 0; m < N; ++m)
             for (int t = 0; t < N; ++t) {
                 const double v = TW[(size_t)m * N + t];
@@ -410,10 +470,14 @@ int radial_build(cdft_plan* p)
                            / (TWO_PI * TWO_PI * TWO_PI);
                 }
                 conv(w, M);
+                // D has nonzeros in columns m - 1..m + 1 (rows 0 and N - 1: 0..2, N - 3..N - 1), so
+                // the sum over t runs over that band only (the skipped terms are exact zeros)
+#pragma omp parallel for schedule(static)
                 for (int m = 0; m < N; ++m)
                     for (int q = 0; q < N; ++q) {
                         double v = 0.0;
-                        for (int t = 0; t < N; ++t) v += D[(size_t)m * N + t] * M[(size_t)t * N + q];
+                        const int t0 = std::max(0, m - 2), t1 = std::min(N - 1, m + 2);
+                        for (int t = t0; t <= t1; ++t) v += D[(size_t)m * N + t] * M[(size_t)t * N + q];
                         A0[(size_t)m * N + q] = v;
                     }
                 // adjoint: the transpose, added (weighted_densities.jl:368-385); stored negated because
@@ -422,13 +486,17 @@ int radial_build(cdft_plan* p)
                     for (int q = 0; q < N; ++q) A1[(size_t)m * N + q] = -A0[(size_t)q * N + m];
             }
         }
-    CU(cudaMalloc(&p->d_rw, (size_t)N * sizeof(double)));
-    CU(cudaMemcpyAsync(p->d_rw, p->rw.data(), (size_t)N * sizeof(double), cudaMemcpyHostToDevice, p->stream));
-    S.qw = p->d_rw;
-    CU(cudaMalloc(&p->d_mats, mats.size() * sizeof(double)));
-    CU(cudaMemcpyAsync(p->d_mats, mats.data(), mats.size() * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    auto ops = std::make_shared<RadialOps>();
+    ops->device = p->device;
+    CU(cudaMalloc(&ops->d_mats, mats.size() * sizeof(double)));
+    CU(cudaMemcpyAsync(ops->d_mats, mats.data(), mats.size() * sizeof(double), cudaMemcpyHostToDevice, p->stream));
     CU(cudaStreamSynchronize(p->stream));
-    S.mats = p->d_mats;
+    p->rops = ops;
+    S.mats = ops->d_mats;
+    std::lock_guard<std::mutex> lk(g_rops_mu);
+    for (auto it = g_rops.begin(); it != g_rops.end();)   // drop the entries whose plans are gone
+        it = it->second.expired() ? g_rops.erase(it) : std::next(it);
+    g_rops[key] = ops;
     return 0;
 }
 
@@ -739,7 +807,7 @@ int plan_build3d(cdft_plan* p)
 void plan_free(cdft_plan* p)
 {
     cudaFree(p->d_rw);
-    cudaFree(p->d_mats);
+    p->rops.reset();
     cudaFree(p->d_taps);
     cudaFree(p->d_taps32);
     cudaFree(p->d_vext);
@@ -800,6 +868,35 @@ int batch_build(const std::vector<cdft_plan*>& plans, Batch** out)
         for (int e = 0; e < S.n_elem; e += ELEM_CHUNK) ech.push_back({s, e});
         S.chunk_count = (int)ech.size() - S.chunk_begin;
     }
+    // radial: systems whose plans share one operator buffer, in tiles of DGRP_COLS (batch order)
+    std::vector<DenseGroup> groups;
+    if (b->coord != CDFT_COORD_CART) {
+        std::vector<const double*> keys;
+        std::vector<std::vector<int>> members;
+        for (int s = 0; s < b->nsys; ++s) {
+            const double* m = plans[s]->sys.mats;
+            size_t g = std::find(keys.begin(), keys.end(), m) - keys.begin();
+            if (g == keys.size()) {
+                keys.push_back(m);
+                members.emplace_back();
+            }
+            members[g].push_back(s);
+        }
+        for (const auto& mem : members)
+            for (size_t t = 0; t < mem.size(); t += DGRP_COLS) {
+                DenseGroup G;
+                G.ns = (int)std::min<size_t>(DGRP_COLS, mem.size() - t);
+                for (int c = 0; c < DGRP_COLS; ++c) G.sys[c] = mem[t + (c < G.ns ? c : 0)];
+                const SysDev& S = plans[G.sys[0]]->sys;
+                b->group_blocks = std::max(b->group_blocks, S.nc * S.nconv * ((S.N + 7) / 8));
+                groups.push_back(G);
+            }
+    }
+    b->ngroups = (int)groups.size();
+    if (b->ngroups > 65535) {
+        free_batch(b);
+        return set_error(CDFT_E_UNSUPPORTED, "radial batch of %d column tiles (at most 65535)", b->ngroups);
+    }
     b->ntasks = (int)tasks.size();
     b->npchunks = (int)pch.size();
     b->nechunks = (int)ech.size();
@@ -821,6 +918,10 @@ int batch_build(const std::vector<cdft_plan*>& plans, Batch** out)
     BCU(cudaMallocHost(&b->h_done, 2 * sizeof(int)));
     if (!tasks.empty())
         BCU(cudaMemcpy(b->d_tasks, tasks.data(), sizeof(ConvTask) * tasks.size(), cudaMemcpyHostToDevice));
+    if (!groups.empty()) {
+        BCU(cudaMalloc(&b->d_groups, sizeof(DenseGroup) * groups.size()));
+        BCU(cudaMemcpy(b->d_groups, groups.data(), sizeof(DenseGroup) * groups.size(), cudaMemcpyHostToDevice));
+    }
     BCU(cudaMemcpy(b->d_pchunks, pch.data(), sizeof(Chunk) * pch.size(), cudaMemcpyHostToDevice));
     BCU(cudaMemcpy(b->d_echunks, ech.data(), sizeof(Chunk) * ech.size(), cudaMemcpyHostToDevice));
 #undef BCU
@@ -1026,6 +1127,13 @@ int launch_eval3d(Batch* b, const AAState* st, bool with_int)
 template <typename T>
 int launch_dense_stage(Batch* b, const AAState* st, int stage)
 {
+    if (g_tuned.radial_dmma) {
+        dense_group_kernel<T><<<dim3(b->group_blocks, b->ngroups), DGRP_WARPS * 32, 0, b->stream>>>(
+            b->d_sys, b->d_groups, stage, st);
+        g_launches += 1;
+        CHECK_LAUNCH();
+        return 0;
+    }
     for (int s = 0; s < b->nsys; ++s) {
         const SysDev& S = b->plans[s]->sys;
         const long long rows = (long long)S.nc * S.nconv * S.N;
@@ -1182,7 +1290,9 @@ size_t persistent_smem_limit(const Batch* b)
 int batch_capture(Batch* b, int iters)
 {
     const int g32 = b->cur32;
-    if (b->graph[g32] && b->graph_iters[g32] == iters && b->graph_mb[g32] == b->vec_mb) return 0;
+    if (b->graph[g32] && b->graph_iters[g32] == iters && b->graph_mb[g32] == b->vec_mb &&
+        std::memcmp(&b->graph_tuned[g32], &g_tuned, sizeof(TunedShapes)) == 0)
+        return 0;
     if (b->graph[g32]) {
         cudaGraphExecDestroy(b->graph[g32]);
         b->graph[g32] = nullptr;
@@ -1202,6 +1312,7 @@ int batch_capture(Batch* b, int iters)
     if (e != cudaSuccess) return set_error(CDFT_E_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
     b->graph_iters[g32] = iters;
     b->graph_mb[g32] = b->vec_mb;
+    b->graph_tuned[g32] = g_tuned;
     return 0;
 }
 

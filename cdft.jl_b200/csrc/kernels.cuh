@@ -1004,6 +1004,88 @@ dense1d_kernel(const SysDev* __restrict__ sys, int s, int stage, const AAState* 
     if (lane == 0) reinterpret_cast<T*>(S.part)[(size_t)slot * N + j] = T(stage == 0 ? acc * S.NA : acc);
 }
 
+// mma.sync m8n8k4 f64 (the FP64 tensor path of sm_100a): D += A B with A 8x4 (row),
+// B 4x8 (col); lane l holds A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4) + {0,1}].
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// Radial operators of a whole batch as FP64 tensor-core GEMMs.  Plans of one geometry,
+// length unit and set of diameters share one operator buffer (an isotherm of a pore:
+// every pressure), so those systems' matrix-vector products are one product of the
+// operator with a matrix whose columns are the systems' inputs.  Column tiles of up to
+// DGRP_COLS systems of one buffer are built with the batch; a CTA computes, for one
+// slot (component i, field f) and 8 output rows, the 8 x 8 tile Y = A X with
+// mma.sync m8n8k4.  The k = 4 blocks of [0, N) are dealt round-robin to the CTA's
+// DGRP_WARPS warps (four accumulator pairs each) and the warps' tiles are summed in a
+// fixed order in shared memory.  Each output element is a sum over its own operator row
+// and input column only, so a system gets the same bits alone or inside any column tile;
+// each operator row is read once per column tile instead of once per system.
+#define DGRP_COLS 8
+#define DGRP_WARPS 8
+struct DenseGroup {
+    int ns;                   // systems in this column tile (1..DGRP_COLS)
+    int sys[DGRP_COLS];       // their batch indices (unused entries repeat sys[0])
+};
+
+template <typename T>
+__global__ void __launch_bounds__(DGRP_WARPS * 32)
+dense_group_kernel(const SysDev* __restrict__ sys, const DenseGroup* __restrict__ groups, int stage,
+                   const AAState* __restrict__ st)
+{
+    __shared__ double red[DGRP_WARPS][32][2];
+    const DenseGroup& G = groups[blockIdx.y];
+    const SysDev& S0 = sys[G.sys[0]];
+    const int N = S0.N, nconv = S0.nconv, nc = S0.nc;
+    const int rtiles = (N + 7) >> 3;
+    if ((int)blockIdx.x >= nc * nconv * rtiles) return;
+    const int slot = blockIdx.x / rtiles, j0 = (blockIdx.x - slot * rtiles) * 8;
+    const int i = slot / nconv, f = slot - i * nconv;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = lane >> 2, k = lane & 3;
+    // A: operator row j0 + r (rows past N read row N - 1 and are not stored)
+    const double* Arow = S0.mats + (((size_t)stage * nc * nconv + slot) * N + min(j0 + r, N - 1)) * N;
+    // B: column r is the input of the tile's r-th system (zero past ns or once converged)
+    const bool cval = r < G.ns && sys_active(st, G.sys[r]);
+    const SysDev& Sc = sys[G.sys[cval ? r : 0]];
+    const double* x64 = Sc.rho + (size_t)i * N;
+    const T* xT = reinterpret_cast<const T*>(Sc.dfield) + (size_t)(i * Sc.NF + f + 1) * N;
+    const int nk4 = (N + 3) >> 2;
+    double c[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    for (int kb = warp; kb < nk4; kb += 4 * DGRP_WARPS) {   // warp-uniform trip count
+        double a[4], b[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int q = (kb + u * DGRP_WARPS) * 4 + k;
+            const bool in = q < N;
+            a[u] = in ? __ldg(Arow + q) : 0.0;
+            b[u] = (in && cval) ? (stage == 0 ? __ldg(x64 + q) : double(xT[q])) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) dmma_m8n8k4(c[u][0], c[u][1], a[u], b[u]);
+    }
+    red[warp][lane][0] = (c[0][0] + c[1][0]) + (c[2][0] + c[3][0]);
+    red[warp][lane][1] = (c[0][1] + c[1][1]) + (c[2][1] + c[3][1]);
+    __syncthreads();
+    if (warp != 0) return;
+    const int j = j0 + r;
+    if (j >= N) return;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        double acc = 0.0;
+#pragma unroll
+        for (int w = 0; w < DGRP_WARPS; ++w) acc += red[w][lane][h];
+        const int col = 2 * k + h;
+        if (col < G.ns && sys_active(st, G.sys[col])) {
+            const SysDev& So = sys[G.sys[col]];
+            reinterpret_cast<T*>(So.part)[(size_t)slot * N + j] = T(stage == 0 ? acc * So.NA : acc);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Parameter gradient of F_res (1D): derivative taps, rho * dtaps, per-point terms.
 // ---------------------------------------------------------------------------

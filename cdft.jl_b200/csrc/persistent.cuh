@@ -156,12 +156,7 @@ __device__ __forceinline__ void pers_conv(const T* __restrict__ ext, bool shared
 // 8 columns (64 outputs) of one field and runs the k = (d, c) loop as 2 D mma of
 // k = 4 into two accumulators (c < 4, c >= 4).  Every q in [0, N) is visited once
 // per output, so the result is the circulant up to summation order.
-__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b)
-{
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
-}
+// (dmma_m8n8k4 is defined in kernels.cuh.)
 
 // Extended inputs at bank-spread positions (pers_pos), taps zero-padded: the loop has no
 // bounds test.  The d loop runs two tap blocks per step into four independent accumulator

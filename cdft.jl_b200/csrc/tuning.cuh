@@ -32,6 +32,11 @@ struct TunedShapes {
     // (FP64 and mixed): the three kernels are faster (the fused block holds 9 fields of its
     // rows and runs one block per SM), so 0.
     int fft3d_fused_phi = 0;
+    // radial grids: the dense weighted-density operators of a batch as FP64 tensor-core GEMMs
+    // over column tiles of systems that share one operator (1), or one warp-per-row FFMA
+    // matrix-vector launch per system (0).  The two sum in different orders; the GEMM's
+    // per-element sum does not depend on the other systems of the tile.
+    int radial_dmma = 1;
 };
 
 static TunedShapes g_tuned;
@@ -47,6 +52,7 @@ static const TunedEntry kTunedEntries[] = {
     {"pers_cluster", &TunedShapes::pers_cluster, 0, 1},
     {"fft3d_tma", &TunedShapes::fft3d_tma, 0, 1},
     {"fft3d_fused_phi", &TunedShapes::fft3d_fused_phi, 0, 1},
+    {"radial_dmma", &TunedShapes::radial_dmma, 0, 1},
 };
 
 inline const TunedEntry* tuned_entry(const char* name)

@@ -11,6 +11,9 @@ and the fastest value is reported with the time of every candidate:
 * fft3d_tma, fft3d_fused_phi -- 3D grids: TMA tile kernels for the y/z passes, the fused
   x pass with Phi: one functional derivative of the 27-solute argon box at 64^3 and
   128^3, FP64 and mixed.
+* radial_dmma -- radial grids: the batch's dense operators as tensor-core GEMMs over column
+  tiles of state points sharing an operator, or per-system warp-per-row launches: the dense
+  stage of the 64-point spherical-pore isotherm (one launch for the batch).
 
     python cdft.jl_b200/tune.py [--out tuning.json]
 
@@ -93,13 +96,39 @@ def sweep_3d(sizes=(64, 128), precisions=("fp64", "mixed")):
     return out
 
 
+def sweep_radial():
+    """ms per dense stage of the spherical-pore isotherm batch, per radial_dmma value."""
+    import cdft_b200 as cd
+    import bench
+    from cdft_b200 import _lib
+    lib = _lib.load()
+    model = cd.PCSAFT(["methane"], **bench.METHANE)
+    specs = [(float(R), float(p), bench.N_OF_RADIUS[k]) for k, R in enumerate(bench.R_PORES)
+             for p in bench.PRESSURES]
+    systems = [cd.DFTSystem(model, cd.Uniform1DSphr((p, bench.T_ISO), [model.stable_density(p, bench.T_ISO, [1.0])],
+                                                     [0.0, R], N), cd.Steele(["graphite"])) for R, p, N in specs]
+    for sy in systems:
+        cd.dFdrho_res(sy, cd.initialize_profiles(sy))   # the plans' device profiles
+    plans = (ctypes.c_void_p * len(systems))(*[sy._plan.value for sy in systems])
+    out = {}
+    for v in (0, 1):
+        cd.tuning("radial_dmma", v)
+        ms = ctypes.c_double()
+        _lib.check(lib.cdft_batch_time_stage(plans, len(systems), 0, 50, ctypes.byref(ms)))
+        out[v] = ms.value
+    for sy in systems:
+        sy.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
     import cdft_b200 as cd
-    defaults = {k: cd.tuning(k) for k in ("pers_warp_aa_max_elem", "fft3d_tma", "fft3d_fused_phi")}
-    res = {"isotherm64_ms_per_batch": sweep_isotherm(), "solutes3d_ms_per_functional_derivative": sweep_3d()}
+    defaults = {k: cd.tuning(k) for k in ("pers_warp_aa_max_elem", "fft3d_tma", "fft3d_fused_phi", "radial_dmma")}
+    res = {"isotherm64_ms_per_batch": sweep_isotherm(), "solutes3d_ms_per_functional_derivative": sweep_3d(),
+           "radial_isotherm64_ms_per_dense_stage": sweep_radial()}
     for k, v in defaults.items():
         cd.tuning(k, v)
     iso = res["isotherm64_ms_per_batch"]
@@ -112,6 +141,8 @@ def main():
     shape = min(totals, key=totals.get)
     best["fft3d_tma"] = int(shape.split()[0].split("=")[1])
     best["fft3d_fused_phi"] = int(shape.split()[1].split("=")[1])
+    rad = res["radial_isotherm64_ms_per_dense_stage"]
+    best["radial_dmma"] = min(rad, key=rad.get)
     res["best"] = best
     res["defaults_compiled"] = defaults
     res["when"] = time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())

@@ -111,3 +111,71 @@ def test_converge_radial_steele_wall(coord, lb_L):
     ro, out = so.converge(r0, **kw)
     assert res.errcode == 0 and out.errcode == 0, (res, out.errcode)
     assert float(np.max(np.abs(rho / ro - 1))) < 1e-8
+
+
+def _sphere_pores(cases):
+    """Methane in spherical graphite pores: (radius / L, N, pressure) per state point."""
+    import cdft_b200 as cd
+    from oracle import pcsaft_bulk as pb
+    pm, om = S.models(["methane"])
+    L = om.length_scale()
+    out = []
+    for ub_L, N, p in cases:
+        rb = [pb.density(om, p, T_M, [1.0])]
+        st = cd.Uniform1DSphr((p, T_M), rb, [0.0, ub_L * L], N)
+        out.append(cd.DFTSystem(pm, st, cd.Steele(["graphite"])))
+    return out
+
+
+def test_radial_batch_equals_individual_bitwise():
+    """Pores of one radius share one operator buffer and form column tiles of up to 8
+    state points of the FP64 tensor-core GEMM (dense_group_kernel).  Radii with 5, 9 and 2
+    pressures make tiles of 5, 8 + 1 and 2; every state point converged inside the batch
+    gives the same bits and evaluation count as converged alone."""
+    import cdft_b200 as cd
+    assert cd.tuning("radial_dmma") == 1
+    cases = ([(6.0, 101, p) for p in np.logspace(5, 7, 5)] + [(8.0, 131, p) for p in np.logspace(5, 7, 9)]
+             + [(10.0, 151, p) for p in (2e6, 9e6)])
+    systems = _sphere_pores(cases)
+    rhos = [cd.initialize_profiles(sp) for sp in systems]
+    kw = dict(beta=0.1, tol=1e-10, anderson_m=5, maxit=5000, engine="grid")
+    singles = []
+    for sp, r in zip(systems, rhos):
+        rr = r.copy()
+        singles.append((rr, cd.converge(sp, rr, **kw)))
+    batch = [r.copy() for r in rhos]
+    results = cd.batch_converge(systems, batch, **kw)
+    for (rr, rs), rb, res in zip(singles, batch, results):
+        assert res.errcode == rs.errcode == 0
+        assert res.evaluations == rs.evaluations
+        assert np.array_equal(rr, rb)
+    for sp in systems:
+        sp.close()
+
+
+def test_radial_dmma_matches_warp_rows():
+    """The tensor-core GEMM (radial_dmma = 1) and the warp-per-row matrix-vector kernel
+    (radial_dmma = 0) apply the same operators in different summation orders: dF/drho
+    agrees to 1e-13 of its scale at a random profile, and converged profiles to 1e-9."""
+    import cdft_b200 as cd
+    systems = _sphere_pores([(8.0, 131, 1e6), (8.0, 131, 5e6), (10.0, 151, 1e7)])
+    kw = dict(beta=0.1, tol=1e-11, anderson_m=5, maxit=5000, engine="grid")
+    got = {}
+    try:
+        for mode in (1, 0):
+            cd.tuning("radial_dmma", mode)
+            rho = S.random_smooth_profile(systems[0], np.random.default_rng(11), amp=0.2)
+            d = cd.dFdrho_res(systems[0], rho)
+            conv = [cd.initialize_profiles(sp) for sp in systems]
+            res = cd.batch_converge(systems, conv, **kw)
+            assert all(r.errcode == 0 for r in res)
+            got[mode] = (d, conv)
+    finally:
+        cd.tuning("radial_dmma", 1)
+    d1, c1 = got[1]
+    d0, c0 = got[0]
+    assert float(np.max(np.abs(d1 - d0)) / np.max(np.abs(d0))) < 1e-13
+    for a, b in zip(c1, c0):
+        assert float(np.max(np.abs(a / b - 1))) < 1e-9
+    for sp in systems:
+        sp.close()

@@ -323,3 +323,80 @@ def test_tma_shared_memory_fits(fp32, L):
         off_bar = ntiles * tile + (L // 2) * cs
         assert off_bar % 8 == 0
         assert off_bar + 16 + 16 + slack <= 227 * 1024
+
+
+DGRP_COLS, DGRP_WARPS = 8, 8
+
+
+def dense_group_emulate(mats, xs, N, slots, active):
+    """dense_group_kernel (csrc/kernels.cuh) step by step for one column tile: per CTA
+    (slot, 8-row tile) and warp, the k = 4 blocks kb = warp, warp + 8, ... in unrolled
+    groups of four into four accumulator pairs, every index checked against its buffer;
+    then the fixed-order sum over warps.  Returns out[col][slot][j] (NaN where not stored)
+    and the number of times each (row, col, q) product was formed."""
+    ns = len(xs)
+    rtiles = (N + 7) >> 3
+    nk4 = (N + 3) >> 2
+    out = np.full((ns, slots, N), np.nan)
+    seen = np.zeros((slots, N, N), dtype=np.int64)
+    for bx in range(slots * rtiles):
+        slot, j0 = bx // rtiles, (bx % rtiles) * 8
+        red = np.zeros((DGRP_WARPS, 8, 8))
+        for warp in range(DGRP_WARPS):
+            acc = np.zeros((4, 8, 8))
+            kb = warp
+            while kb < nk4:
+                for u in range(4):
+                    for lane in range(32):
+                        r, k = lane >> 2, lane & 3
+                        q = (kb + u * DGRP_WARPS) * 4 + k
+                        row = min(j0 + r, N - 1)
+                        assert 0 <= row < N
+                        if q < N:
+                            assert 0 <= slot * N * N + row * N + q < slots * N * N
+                    # the tile product of this k block: A[8 x 4] B[4 x 8]
+                    for r in range(8):
+                        row = min(j0 + r, N - 1)
+                        for k in range(4):
+                            q = (kb + u * DGRP_WARPS) * 4 + k
+                            if q >= N:
+                                continue
+                            for c in range(8):
+                                if c < ns and active[c]:
+                                    acc[u, r, c] += mats[slot, row, q] * xs[c][slot, q]
+                                    if j0 + r < N:
+                                        seen[slot, j0 + r, q] += (c == 0)
+                kb += 4 * DGRP_WARPS
+            red[warp] = (acc[0] + acc[1]) + (acc[2] + acc[3])
+        tot = np.zeros((8, 8))
+        for w in range(DGRP_WARPS):
+            tot += red[w]
+        for r in range(8):
+            j = j0 + r
+            if j >= N:
+                continue
+            for c in range(8):
+                if c < ns and active[c]:
+                    out[c, slot, j] = tot[r, c]
+    return out, seen
+
+
+@pytest.mark.parametrize("N,ns", [(13, 3), (61, 8), (40, 1)])
+def test_dense_group_index_map(N, ns):
+    """Every operator row meets every input entry exactly once per output, the loads stay
+    inside the operator and input buffers, rows past N and inactive columns are not
+    written, and the result is A x per system."""
+    rng = np.random.default_rng(N)
+    slots = 2
+    mats = rng.standard_normal((slots, N, N))
+    xs = [rng.standard_normal((slots, N)) for _ in range(ns)]
+    active = [c != 1 for c in range(8)]
+    out, seen = dense_group_emulate(mats, xs, N, slots, active)
+    if active[0]:
+        assert np.all(seen == 1)
+    for c in range(ns):
+        if not active[c]:
+            assert np.all(np.isnan(out[c]))
+            continue
+        want = np.einsum("sjq,sq->sj", mats, xs[c])
+        np.testing.assert_allclose(out[c], want, rtol=1e-12, atol=1e-12)
