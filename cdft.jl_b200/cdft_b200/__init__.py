@@ -30,7 +30,7 @@ __all__ = [
     "initialize_profiles", "converge", "batch_converge", "dFdrho_res", "F_res", "F_ideal",
     "free_energy", "surface_tension", "interfacial_tension", "adsorption", "integrate", "ddft_rhs", "ddft_problem", "bulk_density",
     "F_res_grad", "grad_params", "dgamma_dtheta", "batch_integrals", "batch_properties", "grand_potential",
-    "CDFTError", "launch_count", "tuning",
+    "CDFTError", "launch_count", "tuning", "saturation",
 ]
 
 PSI = 1.3862
@@ -566,6 +566,37 @@ def bulk_density(model, p, T, x=None, phase="stable"):
     if np.any(status != 0):
         raise ValueError(f"no density root at pressures {p[status != 0]}")
     return rho
+
+
+def saturation(model, T):
+    """Pure-component vapour-liquid coexistence at temperatures ``T`` (scalar or array, K),
+    solved on the device in one launch (cdft_saturation_pure): arrays (p_sat [Pa],
+    rho_liquid, rho_vapour [mol/m^3]).  The saturation state that surface_tension(model, T, x)
+    takes from bubble_pressure for a pure component (surface_tension.jl:13-20); the host
+    equivalent is PCSAFT.saturation."""
+    if len(model) != 1:
+        raise ValueError("saturation of a pure component")
+    T = np.atleast_1d(np.asarray(T, dtype=np.float64))
+    n = T.size
+    d = _lib.SystemDesc()
+    d.nc = 1
+    d.m[0] = model.m[0]
+    d.hsd[0] = model.d(float(T[0]))[0]
+    d.sigma[0] = model.sigma_ij[0, 0]
+    d.eps[0] = model.eps_ij[0, 0]
+    d.L = model.length_scale()
+    d.T = float(T[0])
+    pairs = model.assoc_pairs()
+    d.n_assoc = len(pairs)
+    for q, (i, a, j, b, eab, kab) in enumerate(pairs):
+        d.assoc[q] = _lib.AssocPair(i, j, a, b, 1, 1, eab, kab)
+    p, rl, rv = np.empty(n), np.empty(n), np.empty(n)
+    status = np.zeros(n, dtype=np.int32)
+    _lib.check(_LIB.cdft_saturation_pure(ctypes.byref(d), n, _lib.dptr(T), _lib.dptr(p), _lib.dptr(rl),
+                                         _lib.dptr(rv), status.ctypes.data_as(ctypes.c_void_p)))
+    if np.any(status != 0):
+        raise ValueError(f"no coexistence at T = {T[status != 0]} (status {status[status != 0]})")
+    return p, rl, rv
 
 
 def ddft_rhs(system, eta):

@@ -33,7 +33,7 @@ LIB_PATH = os.environ.get("CDFT_B200_LIB") or os.path.join(os.path.dirname(os.pa
 # every symbol declared in include/cdft_b200.h
 EXPORTED = [
     "cdft_plan_create", "cdft_plan_destroy",
-    "cdft_functional_derivative", "cdft_functional_derivative_dev", "cdft_ddft_rhs", "cdft_ddft_rhs_dev", "cdft_bulk_density", "cdft_phi_field",
+    "cdft_functional_derivative", "cdft_functional_derivative_dev", "cdft_ddft_rhs", "cdft_ddft_rhs_dev", "cdft_bulk_density", "cdft_saturation_pure", "cdft_phi_field",
     "cdft_free_energy_res", "cdft_phi_pointwise", "cdft_free_energy_res_grad", "cdft_grad_params", "cdft_grad_params_ext",
     "cdft_converge", "cdft_converge_dev",
     "cdft_batch_converge", "cdft_batch_converge_dev",
@@ -131,6 +131,7 @@ def load(path=LIB_PATH):
     lib.cdft_ddft_rhs_dev.argtypes = [P, P, P]
     lib.cdft_phi_field.argtypes = [P, P, P]
     lib.cdft_bulk_density.argtypes = [ctypes.POINTER(SystemDesc), ctypes.c_int, P, P, ctypes.c_int, P, P]
+    lib.cdft_saturation_pure.argtypes = [ctypes.POINTER(SystemDesc), ctypes.c_int, P, P, P, P, P]
     lib.cdft_free_energy_res.argtypes = [P, dp, dp]
     lib.cdft_phi_pointwise.argtypes = [P, dp, ctypes.c_int, dp, dp]
     lib.cdft_free_energy_res_grad.argtypes = [P, dp, dp]

@@ -213,3 +213,86 @@ __global__ void bulk_density_kernel(BulkModel M, int n, const double* __restrict
     rho_out[s] = r / NAVO;
     status[s] = 0;
 }
+
+// d(p / k_B T) / d rho = Z + rho dZ/drho = 1 + 2 rho a' + rho^2 a'' at number density rho,
+// with a' exact (dual numbers) and a'' by a central difference of a' (step 1e-5 rho: the
+// Jacobian only sets Newton's rate, the residuals below are exact).  Also returns
+// Z and the Gibbs term g = a_res + Z + ln rho.
+__device__ __forceinline__ double bulk_dpdrho(const BulkModel& M, const double* x, double rho, double* Z, double* g)
+{
+    const Dual a = bulk_ares(M, x, Dual{rho, 1.0});
+    const double h = 1e-5 * rho;
+    const double ap = bulk_ares(M, x, Dual{rho + h, 1.0}).d, am = bulk_ares(M, x, Dual{rho - h, 1.0}).d;
+    const double a2 = (ap - am) / (2.0 * h);
+    *Z = 1.0 + rho * a.d;
+    *g = a.v + *Z + log(rho);
+    return 1.0 + 2.0 * rho * a.d + rho * rho * a2;
+}
+
+// Pure-component vapour-liquid coexistence, one warp per temperature (models[s] holds the
+// component at T_s).  Start as the host solver does: the densest root of p = p_start (the
+// warp scans the packing-fraction grid of bulk_density_kernel) and the ideal-gas vapour
+// p_start / k_B T.  Then Newton on y = (ln rho_l, ln rho_v) for
+//   F1 = rho_l Z_l - rho_v Z_v   (p_l - p_v over k_B T),   F2 = g_l - g_v   (mu_l - mu_v over k_B T).
+// Gibbs-Duhem (d mu = dp / rho at fixed T) gives the Jacobian from P' = d(p / k_B T)/d rho
+// alone: dF1/dy_l = rho_l P'_l, dF2/dy_l = P'_l (and minus the vapour's), so the step is
+//   dy_l = (rho_v F2 - F1) / (P'_l (rho_v - rho_l)),   dy_v = (rho_l F2 - F1) / (P'_v (rho_v - rho_l)),
+// halved until no component exceeds 0.5, at most 100 steps, converged when both are below
+// 1e-13.  Outputs p_sat = p(rho_v) (Pa) and the densities in mol/m^3; status 0 ok, 1 no
+// liquid root at p_start, 2 not converged, 3 the trivial solution rho_l = rho_v or a
+// non-finite iterate.
+__global__ void saturation_kernel(const BulkModel* __restrict__ models, int n, double p_start,
+                                  double* __restrict__ p_out, double* __restrict__ rl_out,
+                                  double* __restrict__ rv_out, int* __restrict__ status)
+{
+    const double NAVO = 6.02214076e23, kB = 1.380649e-23, PI = 3.14159265358979323846;
+    const int s = blockIdx.x;
+    if (s >= n) return;
+    const int lane = threadIdx.x;
+    const BulkModel& M = models[s];
+    __shared__ double fgrid[BULK_GRID];
+    const double x[1] = {1.0};
+    const double scale = PI / 6.0 * M.m[0] * M.d[0] * M.d[0] * M.d[0];
+    for (int k = lane; k < BULK_GRID; k += 32) fgrid[k] = bulk_pressure(M, x, bulk_grid_eta(k) / scale) - p_start;
+    __syncwarp();
+    if (lane != 0) return;
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    auto fail = [&](int code) {
+        p_out[s] = nan;
+        rl_out[s] = nan;
+        rv_out[s] = nan;
+        status[s] = code;
+    };
+    auto sgn = [](double v) { return v > 0 ? 1 : (v < 0 ? -1 : 0); };
+    int last = -1;
+    for (int k = 0; k + 1 < BULK_GRID; ++k)
+        if (sgn(fgrid[k]) != sgn(fgrid[k + 1])) last = k;
+    if (last < 0) return fail(1);
+    const double rl0 = bulk_refine(M, x, scale, p_start, bulk_grid_eta(last), bulk_grid_eta(last + 1), fgrid[last],
+                                   fgrid[last + 1]) / scale;
+    double yl = log(rl0), yv = log(p_start / (kB * M.T));
+    bool conv = false;
+    for (int it = 0; it < 100; ++it) {
+        const double rl = exp(yl), rv = exp(yv);
+        double Zl, Zv, gl, gv;
+        const double Pl = bulk_dpdrho(M, x, rl, &Zl, &gl), Pv = bulk_dpdrho(M, x, rv, &Zv, &gv);
+        const double F1 = rl * Zl - rv * Zv, F2 = gl - gv;
+        const double dl = (rv * F2 - F1) / (Pl * (rv - rl)), dv = (rl * F2 - F1) / (Pv * (rv - rl));
+        if (!isfinite(dl) || !isfinite(dv)) return fail(3);
+        double lam = 1.0;
+        while (fmax(fabs(lam * dl), fabs(lam * dv)) > 0.5) lam *= 0.5;
+        yl -= lam * dl;
+        yv -= lam * dv;
+        if (fmax(fabs(dl), fabs(dv)) < 1e-13) {
+            conv = true;
+            break;
+        }
+    }
+    const double rl = exp(yl), rv = exp(yv);
+    if (!conv) return fail(2);
+    if (!(fabs(rl / rv - 1.0) > 1e-6)) return fail(3);
+    p_out[s] = bulk_pressure(M, x, rv);   // the vapour side: Z_l ~ 1e-6 at low T makes p(rho_l) ill-conditioned
+    rl_out[s] = rl / NAVO;
+    rv_out[s] = rv / NAVO;
+    status[s] = 0;
+}

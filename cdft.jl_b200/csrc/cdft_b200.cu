@@ -1877,6 +1877,37 @@ int cdft_functional_derivative_dev(cdft_plan* plan, const double* d_rho, double*
     return functional_derivative(plan, d_rho, d_dFdrho, true);
 }
 
+}  // extern "C"
+
+// The bulk model of desc's components at temperature T with hard-sphere diameters hsd (m).
+static int bulk_model_at(const cdft_system_desc& d, double T, const double* hsd, BulkModel& M)
+{
+    M = BulkModel{};
+    M.nc = d.nc;
+    M.T = T;
+    for (int i = 0; i < d.nc; ++i) {
+        if (!(d.m[i] > 0) || !(hsd[i] > 0)) return set_error(CDFT_E_INVALID, "component %d: m and hsd", i);
+        M.m[i] = d.m[i];
+        M.d[i] = hsd[i];
+        for (int j = 0; j < d.nc; ++j) {
+            const double sg = d.sigma[i * d.nc + j];
+            M.s3[i * CDFT_MAX_NC + j] = sg * sg * sg;
+            M.eT[i * CDFT_MAX_NC + j] = d.eps[i * d.nc + j] / T;
+        }
+    }
+    for (int q = 0; q < d.n_assoc; ++q) {   // the closed form covers 2B self-association
+        const cdft_assoc_pair& a = d.assoc[q];
+        if (a.icomp != a.jcomp || a.isite == a.jsite || a.n_ia != 1 || a.n_jb != 1 || a.icomp < 0 || a.icomp >= d.nc ||
+            M.aK[a.icomp] != 0.0)
+            return set_error(CDFT_E_UNSUPPORTED, "device bulk densities cover 2B self-association only");
+        const double sg = d.sigma[a.icomp * d.nc + a.icomp];
+        M.aK[a.icomp] = sg * sg * sg * a.kappa_ab * (exp(a.eps_ab / T) - 1.0);
+    }
+    return 0;
+}
+
+extern "C" {
+
 int cdft_bulk_density(const cdft_system_desc* desc, int n, const double* p, const double* x, int phase,
                       double* rho, int* status)
 {
@@ -1887,26 +1918,8 @@ int cdft_bulk_density(const cdft_system_desc* desc, int n, const double* p, cons
     if (d.nc < 1 || d.nc > CDFT_MAX_NC || !(d.T > 0)) return set_error(CDFT_E_INVALID, "nc and T");
     if (n == 0) return 0;
     BulkModel M{};
-    M.nc = d.nc;
-    M.T = d.T;
-    for (int i = 0; i < d.nc; ++i) {
-        if (!(d.m[i] > 0) || !(d.hsd[i] > 0)) return set_error(CDFT_E_INVALID, "component %d: m and hsd", i);
-        M.m[i] = d.m[i];
-        M.d[i] = d.hsd[i];
-        for (int j = 0; j < d.nc; ++j) {
-            const double sg = d.sigma[i * d.nc + j];
-            M.s3[i * CDFT_MAX_NC + j] = sg * sg * sg;
-            M.eT[i * CDFT_MAX_NC + j] = d.eps[i * d.nc + j] / d.T;
-        }
-    }
-    for (int q = 0; q < d.n_assoc; ++q) {   // the closed form covers 2B self-association
-        const cdft_assoc_pair& a = d.assoc[q];
-        if (a.icomp != a.jcomp || a.isite == a.jsite || a.n_ia != 1 || a.n_jb != 1 || a.icomp < 0 || a.icomp >= d.nc ||
-            M.aK[a.icomp] != 0.0)
-            return set_error(CDFT_E_UNSUPPORTED, "device bulk densities cover 2B self-association only");
-        const double sg = d.sigma[a.icomp * d.nc + a.icomp];
-        M.aK[a.icomp] = sg * sg * sg * a.kappa_ab * (exp(a.eps_ab / d.T) - 1.0);
-    }
+    int rc = bulk_model_at(d, d.T, d.hsd, M);
+    if (rc) return rc;
     double* dbuf = nullptr;
     const size_t nb = (size_t)n * (2 + d.nc) * sizeof(double) + (size_t)n * sizeof(int);
     CU(cudaMalloc(&dbuf, nb));
@@ -1925,6 +1938,47 @@ int cdft_bulk_density(const cdft_system_desc* desc, int n, const double* p, cons
     if (e == cudaSuccess) e = cudaMemcpy(status, ds, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost);
     cudaFree(dbuf);
     if (e != cudaSuccess) return set_error(CDFT_E_CUDA, "bulk densities: %s", cudaGetErrorString(e));
+    return 0;
+}
+
+int cdft_saturation_pure(const cdft_system_desc* desc, int n, const double* T, double* p_sat, double* rho_liquid,
+                         double* rho_vapour, int* status)
+{
+    g_err_code = 0;
+    if (!desc || n < 0 || (n > 0 && (!T || !p_sat || !rho_liquid || !rho_vapour || !status)))
+        return set_error(CDFT_E_INVALID, "invalid argument");
+    const cdft_system_desc& d = *desc;
+    if (d.nc != 1) return set_error(CDFT_E_UNSUPPORTED, "saturation of a pure component: nc=%d", d.nc);
+    if (n == 0) return 0;
+    std::vector<BulkModel> M(n);
+    for (int s = 0; s < n; ++s) {
+        if (!(T[s] > 0)) return set_error(CDFT_E_INVALID, "T[%d]=%g", s, T[s]);
+        // PC-SAFT's temperature-dependent diameter d = sigma (1 - 0.12 exp(-3 eps / T))
+        const double hsd = d.sigma[0] * (1.0 - 0.12 * exp(-3.0 * d.eps[0] / T[s]));
+        const int rc = bulk_model_at(d, T[s], &hsd, M[s]);
+        if (rc) return rc;
+    }
+    BulkModel* dm = nullptr;
+    double* dbuf = nullptr;
+    CU(cudaMalloc(&dm, sizeof(BulkModel) * n));
+    cudaError_t e = cudaMalloc(&dbuf, (size_t)n * (3 * sizeof(double) + sizeof(int)));
+    double* dp = dbuf;
+    double* dl = dp + n;
+    double* dv = dl + n;
+    int* ds = reinterpret_cast<int*>(dv + n);
+    if (e == cudaSuccess) e = cudaMemcpy(dm, M.data(), sizeof(BulkModel) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        saturation_kernel<<<n, 32>>>(dm, n, 1e3, dp, dl, dv, ds);
+        e = cudaGetLastError();
+        g_launches += 1;
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(p_sat, dp, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(rho_liquid, dl, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(rho_vapour, dv, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(status, ds, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(dm);
+    cudaFree(dbuf);
+    if (e != cudaSuccess) return set_error(CDFT_E_CUDA, "saturation: %s", cudaGetErrorString(e));
     return 0;
 }
 

@@ -165,6 +165,20 @@ int cdft_functional_derivative_dev(cdft_plan* plan, const double* d_rho, double*
 int cdft_bulk_density(const cdft_system_desc* desc, int n, const double* p, const double* x, int phase,
                       double* rho, int* status);
 
+/* Vapour-liquid coexistence of a pure component (nc = 1) at n temperatures T[s] (K), one
+ * launch: p_sat[s] (Pa), rho_liquid[s] and rho_vapour[s] (mol/m^3).  Replaces the
+ * saturation state that surface_tension(model, T, x) takes from bubble_pressure(model, T, x)
+ * for a pure component (src/methods/surface_tension.jl:13-20; Clapeyron's
+ * saturation_pressure).  Uses desc's m, sigma (m), eps (K) and 2B self-association; the
+ * diameter at each T is PC-SAFT's sigma (1 - 0.12 exp(-3 eps / T)), so desc's hsd and T
+ * are ignored.  Newton on (ln rho_l, ln rho_v) from the densest root at 1e3 Pa and the
+ * ideal-gas vapour there; p_sat is the vapour root's pressure (the liquid's compressibility
+ * factor is ~1e-6 at low T, so its pressure amplifies the last bits of rho_l).  status[s] = 0 ok, 1 no liquid root at 1e3 Pa, 2 not converged
+ * in 100 steps, 3 the trivial solution (T at or above the critical temperature); outputs
+ * NaN where status != 0. */
+int cdft_saturation_pure(const cdft_system_desc* desc, int n, const double* T, double* p_sat, double* rho_liquid,
+                         double* rho_vapour, int* status);
+
 /* Right-hand side of dynamic DFT in eta = ln rho: deta = lap(eta) + lap(mu) +
  * sum_d (d_d eta)^2 + d_d mu d_d eta with rho = exp(clamp(eta, -50, 30)) and
  * mu = dF/drho_res + V_ext, derivatives spectral in reduced lengths (x / L) on the

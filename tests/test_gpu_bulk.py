@@ -42,3 +42,32 @@ def test_cross_association_is_refused():
     pm, _ = S.models(["water", "ethanol"])
     with pytest.raises(CDFTError):
         cd.bulk_density(pm, [1e5], 298.15, [0.5, 0.5], "liquid")
+
+
+@pytest.mark.parametrize("name,Ts", [("octane", [250.0, 298.15, 350.0, 450.0, 500.0]),
+                                     ("methane", [100.0, 120.0, 150.0, 170.0]),
+                                     ("water", [298.15, 373.15, 450.0])])
+def test_saturation_matches_oracle(name, Ts):
+    """Pure-component coexistence of every temperature in one launch (cdft_saturation_pure)
+    against the oracle's saturation_pure (the same equations p_l = p_v, mu_l = mu_v from the
+    same starting point, Newton with a finite-difference Jacobian on the host): both
+    densities and the pressure of the vapour root to 1e-10, water with its 2B association.
+    (The oracle reports the liquid root's pressure, whose compressibility factor is ~5e-6
+    for octane at 250 K: the last bits of rho_l move it by ~1e-7.)"""
+    import cdft_b200 as cd
+    from oracle import pcsaft_bulk as pb
+    pm, om = S.models([name])
+    p, rl, rv = cd.saturation(pm, Ts)
+    for k, T in enumerate(Ts):
+        _, wl, wv = pb.saturation_pure(om, T)
+        wp = pb.pressure(om, [wv], T)
+        np.testing.assert_allclose([p[k], rl[k], rv[k]], [wp, wl, wv], rtol=1e-10, err_msg=f"{name} {T} K")
+        assert rl[k] > rv[k]
+
+
+def test_saturation_above_the_critical_temperature_is_refused():
+    """Above T_c the Newton iteration collapses onto one phase: status 3, a ValueError."""
+    import cdft_b200 as cd
+    pm, _ = S.models(["methane"])
+    with pytest.raises(ValueError):
+        cd.saturation(pm, [120.0, 260.0])
