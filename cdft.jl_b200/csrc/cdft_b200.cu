@@ -151,6 +151,12 @@ struct Batch {
     int graph_mb[2] = {0, 0};                         // ... captured in each graph
     TunedShapes graph_tuned[2];                       // ... and the launch shapes they were captured with
     long long graph_launches[2] = {0, 0};             // kernel launches captured in each graph
+    CopyTask* d_copy = nullptr;                       // profile copies in [0, nsys) and out [nsys, 2 nsys)
+    CopyTask* h_copy = nullptr;                       // ... their pinned host staging
+    AAInit* d_init = nullptr;                         // per-system solver-state initialisation
+    AAInit* h_init = nullptr;
+    AASummary* d_sum = nullptr;                       // the final states' status fields
+    AASummary* h_sum = nullptr;
     DenseGroup* d_groups = nullptr;                   // radial: column tiles of systems sharing an operator
     int ngroups = 0, group_blocks = 0;                // ... and the largest slots x row tiles among them
 };
@@ -186,6 +192,12 @@ void free_batch(Batch* b)
     cudaFree(b->d_echunks);
     cudaFree(b->d_partials);
     cudaFree(b->d_groups);
+    cudaFree(b->d_copy);
+    cudaFree(b->d_init);
+    cudaFree(b->d_sum);
+    if (b->h_copy) cudaFreeHost(b->h_copy);
+    if (b->h_init) cudaFreeHost(b->h_init);
+    if (b->h_sum) cudaFreeHost(b->h_sum);
     cudaFree(b->d_done);
     cudaFree(b->d_hist);
     if (b->h_done) cudaFreeHost(b->h_done);
@@ -916,6 +928,12 @@ int batch_build(const std::vector<cdft_plan*>& plans, Batch** out)
     BCU(cudaMalloc(&b->d_partials, sizeof(double) * RED_SLOTS * ech.size()));
     BCU(cudaMalloc(&b->d_done, 2 * sizeof(int)));        // [0] finished systems, [1] kernel error word
     BCU(cudaMallocHost(&b->h_done, 2 * sizeof(int)));
+    BCU(cudaMalloc(&b->d_copy, sizeof(CopyTask) * 2 * b->nsys));
+    BCU(cudaMallocHost(&b->h_copy, sizeof(CopyTask) * 2 * b->nsys));
+    BCU(cudaMalloc(&b->d_init, sizeof(AAInit) * b->nsys));
+    BCU(cudaMallocHost(&b->h_init, sizeof(AAInit) * b->nsys));
+    BCU(cudaMalloc(&b->d_sum, sizeof(AASummary) * b->nsys));
+    BCU(cudaMallocHost(&b->h_sum, sizeof(AASummary) * b->nsys));
     if (!tasks.empty())
         BCU(cudaMemcpy(b->d_tasks, tasks.data(), sizeof(ConvTask) * tasks.size(), cudaMemcpyHostToDevice));
     if (!groups.empty()) {
@@ -1366,29 +1384,26 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
               const std::vector<double>* atol_sys = nullptr)
 {
     const long long max_evals = (long long)opts->maxit + 2LL * opts->picard_maxit + 4;
+    // every state starts zeroed with aasol's options (state_init_kernel); per system the
+    // tolerances and its slice of the residual history
     for (int s = 0; s < b->nsys; ++s) {
-        AAState& A = st[s];
-        memset(&A, 0, sizeof(A));
-        A.mode = MODE_EVAL_INIT;
-        A.m = opts->m;
-        A.maxit = opts->maxit;
-        A.picard_maxit = opts->picard_maxit;
-        A.beta = opts->beta;
-        A.picard_beta = opts->picard_beta;
+        AAInit& I = b->h_init[s];
         const bool abs_tol = atol_sys && (*atol_sys)[s] >= 0.0;
-        A.rtol = abs_tol ? 0.0 : rtol;
-        A.atol = abs_tol ? (*atol_sys)[s] : atol;
+        I.rtol = abs_tol ? 0.0 : rtol;
+        I.atol = abs_tol ? (*atol_sys)[s] : atol;
         // an FP64 polish of an FP32 result starts with Anderson: the Picard warm-up of
         // aasol targets picard_rtol times the residual of its first iterate, which is
         // already small here, and damped Picard does not reach it
-        if (abs_tol) A.picard_maxit = 0;
-        A.picard_rtol = opts->picard_rtol;
-        A.picard_atol = opts->picard_atol;
+        I.picard_maxit = abs_tol ? 0 : opts->picard_maxit;
         const int off = std::min(hist_off[s], b->hist_cap);
-        A.history = b->d_hist + (size_t)s * b->hist_cap + off;
-        A.history_cap = b->hist_cap - off;
+        I.history = b->d_hist + (size_t)s * b->hist_cap + off;
+        I.history_cap = b->hist_cap - off;
     }
-    CU(cudaMemcpyAsync(b->d_st, st.data(), sizeof(AAState) * b->nsys, cudaMemcpyHostToDevice, b->stream));
+    const AACommon common{opts->m, opts->maxit, opts->beta, opts->picard_beta, opts->picard_rtol, opts->picard_atol};
+    CU(cudaMemcpyAsync(b->d_init, b->h_init, sizeof(AAInit) * b->nsys, cudaMemcpyHostToDevice, b->stream));
+    state_init_kernel<<<b->nsys, 128, 0, b->stream>>>(b->d_st, b->d_init, common);
+    CHECK_LAUNCH();
+    g_launches += 1;
     CU(cudaMemsetAsync(b->d_done, 0, 2 * sizeof(int), b->stream));
     init_kernel<<<b->nechunks, ELEM_THREADS, 0, b->stream>>>(b->d_echunks, b->d_sys);
     CHECK_LAUNCH();
@@ -1473,8 +1488,24 @@ int run_phase(Batch* b, const cdft_solver_opts* opts, double rtol, double atol, 
             }
         }
     }
-    CU(cudaMemcpyAsync(st.data(), b->d_st, sizeof(AAState) * b->nsys, cudaMemcpyDeviceToHost, b->stream));
+    // the host reads the status fields of the final states (AASummary), not the whole states
+    state_summary_kernel<<<(b->nsys + 127) / 128, 128, 0, b->stream>>>(b->d_st, b->d_sum, b->nsys);
+    CHECK_LAUNCH();
+    g_launches += 1;
+    CU(cudaMemcpyAsync(b->h_sum, b->d_sum, sizeof(AASummary) * b->nsys, cudaMemcpyDeviceToHost, b->stream));
     CU(cudaStreamSynchronize(b->stream));
+    for (int s = 0; s < b->nsys; ++s) {
+        AAState& A = st[s];
+        memset(&A, 0, sizeof(A));
+        const AASummary& r = b->h_sum[s];
+        A.mode = r.mode;
+        A.idid = r.idid;
+        A.errcode = r.errcode;
+        A.k = r.k;
+        A.nevals = r.nevals;
+        A.resnorm = r.resnorm;
+        A.tol = r.tol;
+    }
     return 0;
 }
 
@@ -1516,10 +1547,27 @@ int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, boo
         CU(cudaMalloc(&b->d_hist, sizeof(double) * (size_t)hist_cap * b->nsys));
         b->hist_cap = hist_cap;
     }
+    // device profiles move in and out by one batch_copy_kernel launch each; host ones by one
+    // copy per system
+    long long max_elem = 0;
     for (int s = 0; s < b->nsys; ++s) {
         cdft_plan* p = plans[s];
-        const size_t bytes = (size_t)p->sys.n_elem * sizeof(double);
-        CU(cudaMemcpyAsync(p->sys.rho, rho[s], bytes, is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->stream));
+        max_elem = std::max<long long>(max_elem, p->sys.n_elem);
+        b->h_copy[s] = CopyTask{rho[s], p->sys.rho, (long long)p->sys.n_elem};
+        b->h_copy[b->nsys + s] = CopyTask{p->sys.rho, rho[s], (long long)p->sys.n_elem};
+    }
+    const dim3 copy_grid((unsigned)std::min<long long>((max_elem + 255) / 256, 64), (unsigned)b->nsys);
+    if (is_dev) {
+        CU(cudaMemcpyAsync(b->d_copy, b->h_copy, sizeof(CopyTask) * 2 * b->nsys, cudaMemcpyHostToDevice, b->stream));
+        batch_copy_kernel<<<copy_grid, 256, 0, b->stream>>>(b->d_copy);
+        CHECK_LAUNCH();
+        g_launches += 1;
+    } else {
+        for (int s = 0; s < b->nsys; ++s) {
+            cdft_plan* p = plans[s];
+            const size_t bytes = (size_t)p->sys.n_elem * sizeof(double);
+            CU(cudaMemcpyAsync(p->sys.rho, rho[s], bytes, cudaMemcpyHostToDevice, b->stream));
+        }
     }
     std::vector<AAState> st(b->nsys), st1;
     std::vector<int> hist_off(b->nsys, 0);
@@ -1569,10 +1617,16 @@ int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, boo
         rc = run_phase(b, opts, opts->rtol, opts->atol, hist_off, st, t0, &budget_hit);
         if (rc) return rc;
     }
-    for (int s = 0; s < b->nsys; ++s) {
-        cdft_plan* p = plans[s];
-        const size_t bytes = (size_t)p->sys.n_elem * sizeof(double);
-        CU(cudaMemcpyAsync(rho[s], p->sys.rho, bytes, is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, b->stream));
+    if (is_dev) {
+        batch_copy_kernel<<<copy_grid, 256, 0, b->stream>>>(b->d_copy + b->nsys);
+        CHECK_LAUNCH();
+        g_launches += 1;
+    } else {
+        for (int s = 0; s < b->nsys; ++s) {
+            cdft_plan* p = plans[s];
+            const size_t bytes = (size_t)p->sys.n_elem * sizeof(double);
+            CU(cudaMemcpyAsync(rho[s], p->sys.rho, bytes, cudaMemcpyDeviceToHost, b->stream));
+        }
     }
     CU(cudaStreamSynchronize(b->stream));
     if (results) {

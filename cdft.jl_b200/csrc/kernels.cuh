@@ -932,6 +932,79 @@ __global__ void init_kernel(const Chunk* __restrict__ echunks, const SysDev* __r
     }
 }
 
+// Device-array copies of a batch in one launch (block row y = one system): the caller's
+// profiles into the plans' buffers and back, instead of one cudaMemcpyAsync per system.
+struct CopyTask {
+    const double* src;
+    double* dst;
+    long long n;
+};
+
+__global__ void batch_copy_kernel(const CopyTask* __restrict__ tasks)
+{
+    const CopyTask c = tasks[blockIdx.y];
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < c.n; e += (long long)gridDim.x * blockDim.x)
+        c.dst[e] = c.src[e];
+}
+
+// The solver state of every system at the start of a phase, written on the device: all
+// zero, then aasol's options and the system's slice of the residual history.
+struct AAInit {
+    double* history;
+    int history_cap, picard_maxit;
+    double rtol, atol;
+};
+struct AACommon {
+    int m, maxit;
+    double beta, picard_beta, picard_rtol, picard_atol;
+};
+
+__global__ void state_init_kernel(AAState* __restrict__ st, const AAInit* __restrict__ init, AACommon c)
+{
+    static_assert(sizeof(AAState) % sizeof(double) == 0, "AAState is zeroed in doubles");
+    AAState& A = st[blockIdx.x];
+    double* w = reinterpret_cast<double*>(&A);
+    for (int k = threadIdx.x; k < (int)(sizeof(AAState) / sizeof(double)); k += blockDim.x) w[k] = 0.0;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    const AAInit& I = init[blockIdx.x];
+    A.mode = MODE_EVAL_INIT;
+    A.m = c.m;
+    A.maxit = c.maxit;
+    A.picard_maxit = I.picard_maxit;
+    A.beta = c.beta;
+    A.picard_beta = c.picard_beta;
+    A.rtol = I.rtol;
+    A.atol = I.atol;
+    A.picard_rtol = c.picard_rtol;
+    A.picard_atol = c.picard_atol;
+    A.history = I.history;
+    A.history_cap = I.history_cap;
+}
+
+// The fields of the final solver states that the host reads (status, counts, residuals).
+struct AASummary {
+    int mode, idid, errcode, k, nevals, pad;
+    double resnorm, tol;
+};
+
+__global__ void state_summary_kernel(const AAState* __restrict__ st, AASummary* __restrict__ out, int n)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const AAState& A = st[s];
+    AASummary r;
+    r.mode = A.mode;
+    r.idid = A.idid;
+    r.errcode = A.errcode;
+    r.k = A.k;
+    r.nevals = A.nevals;
+    r.pad = 0;
+    r.resnorm = A.resnorm;
+    r.tol = A.tol;
+    out[s] = r;
+}
+
 // ---------------------------------------------------------------------------
 // Circulant taps of the 1D kernels: t[q] = Re((1/N) sum_k Omega_k exp(2 pi i k q / N)).
 // Omega_k are the reference's closed forms (weighted_densities.jl:28-80,193-246)
