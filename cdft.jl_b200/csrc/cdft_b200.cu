@@ -127,6 +127,9 @@ struct cdft_plan {
     Batch* self = nullptr;        // batch of this plan alone
 };
 
+// host profiles of a batch of at most this many doubles in all are staged through one pinned buffer
+#define CDFT_STAGE_MAX_ELEMS (4LL << 20)
+
 struct Batch {
     std::vector<cdft_plan*> plans;
     int nsys = 0, nc = 0, nd = 0, mixed = 0, coord = 0;
@@ -157,6 +160,9 @@ struct Batch {
     AAInit* h_init = nullptr;
     AASummary* d_sum = nullptr;                       // the final states' status fields
     AASummary* h_sum = nullptr;
+    double* h_stage = nullptr;                        // host profiles staged back to back (pinned) ...
+    double* d_stage = nullptr;                        // ... and on the device; small batches only
+    long long stage_elems = 0;
     DenseGroup* d_groups = nullptr;                   // radial: column tiles of systems sharing an operator
     int ngroups = 0, group_blocks = 0;                // ... and the largest slots x row tiles among them
 };
@@ -198,6 +204,8 @@ void free_batch(Batch* b)
     if (b->h_copy) cudaFreeHost(b->h_copy);
     if (b->h_init) cudaFreeHost(b->h_init);
     if (b->h_sum) cudaFreeHost(b->h_sum);
+    if (b->h_stage) cudaFreeHost(b->h_stage);
+    cudaFree(b->d_stage);
     cudaFree(b->d_done);
     cudaFree(b->d_hist);
     if (b->h_done) cudaFreeHost(b->h_done);
@@ -1557,7 +1565,35 @@ int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, boo
         b->h_copy[b->nsys + s] = CopyTask{p->sys.rho, rho[s], (long long)p->sys.n_elem};
     }
     const dim3 copy_grid((unsigned)std::min<long long>((max_elem + 255) / 256, 64), (unsigned)b->nsys);
-    if (is_dev) {
+    // host profiles of a small batch (at most CDFT_STAGE_MAX_ELEMS doubles in all) go through one
+    // pinned staging buffer: one host-to-device copy and the scatter kernel, instead of a
+    // pageable copy per system; larger ones (3D grids) are copied directly
+    long long total_elem = 0;
+    for (auto* p : plans) total_elem += p->sys.n_elem;
+    const bool staged = !is_dev && total_elem <= CDFT_STAGE_MAX_ELEMS;
+    if (staged && b->stage_elems < total_elem) {
+        if (b->h_stage) cudaFreeHost(b->h_stage);
+        cudaFree(b->d_stage);
+        b->h_stage = nullptr;
+        b->d_stage = nullptr;
+        b->stage_elems = 0;
+        CU(cudaMallocHost(&b->h_stage, sizeof(double) * (size_t)total_elem));
+        CU(cudaMalloc(&b->d_stage, sizeof(double) * (size_t)total_elem));
+        b->stage_elems = total_elem;
+    }
+    if (staged) {
+        long long off = 0;
+        for (int s = 0; s < b->nsys; ++s) {
+            const long long ne = plans[s]->sys.n_elem;
+            std::memcpy(b->h_stage + off, rho[s], sizeof(double) * (size_t)ne);
+            b->h_copy[s].src = b->d_stage + off;
+            b->h_copy[b->nsys + s].dst = b->d_stage + off;
+            off += ne;
+        }
+        CU(cudaMemcpyAsync(b->d_stage, b->h_stage, sizeof(double) * (size_t)total_elem, cudaMemcpyHostToDevice,
+                           b->stream));
+    }
+    if (is_dev || staged) {
         CU(cudaMemcpyAsync(b->d_copy, b->h_copy, sizeof(CopyTask) * 2 * b->nsys, cudaMemcpyHostToDevice, b->stream));
         batch_copy_kernel<<<copy_grid, 256, 0, b->stream>>>(b->d_copy);
         CHECK_LAUNCH();
@@ -1617,10 +1653,13 @@ int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, boo
         rc = run_phase(b, opts, opts->rtol, opts->atol, hist_off, st, t0, &budget_hit);
         if (rc) return rc;
     }
-    if (is_dev) {
+    if (is_dev || staged) {
         batch_copy_kernel<<<copy_grid, 256, 0, b->stream>>>(b->d_copy + b->nsys);
         CHECK_LAUNCH();
         g_launches += 1;
+        if (staged)
+            CU(cudaMemcpyAsync(b->h_stage, b->d_stage, sizeof(double) * (size_t)total_elem, cudaMemcpyDeviceToHost,
+                               b->stream));
     } else {
         for (int s = 0; s < b->nsys; ++s) {
             cdft_plan* p = plans[s];
@@ -1629,6 +1668,14 @@ int batch_converge(const std::vector<cdft_plan*>& plans, double* const* rho, boo
         }
     }
     CU(cudaStreamSynchronize(b->stream));
+    if (staged) {
+        long long off = 0;
+        for (int s = 0; s < b->nsys; ++s) {
+            const long long ne = plans[s]->sys.n_elem;
+            std::memcpy(rho[s], b->h_stage + off, sizeof(double) * (size_t)ne);
+            off += ne;
+        }
+    }
     if (results) {
         for (int s = 0; s < b->nsys; ++s) {
             cdft_result& r = results[s];
