@@ -732,11 +732,37 @@ def _omega_ex(system, q):
     return F * K_B * T - float(np.dot(mu, q["int_rho"])) + p * q["int_one"]
 
 
-def surface_tension(system, rho):
+def surface_tension(system, rho, x=None):
     """surface_tension(system, ρ) (surface_tension.jl:31-53), J/m^2; the
     periodic two-interface seed gives twice the tension (callers divide by 2).
-    The integrals run on the device (cdft_batch_integrals)."""
+    The integrals run on the device (cdft_batch_integrals).
+
+    surface_tension(model, T, x=[1.0]) (surface_tension.jl:13-29), for a pure component and
+    one or many temperatures T: the coexistence of every T from one device launch
+    (cdft_saturation_pure, the state bubble_pressure gives the reference), a TwoPhase1DCart
+    on [-10L, 10L] with 201 points per T, the systems converged together (converge!'s
+    default solver) and surface_tension(system, ρ) / 2.  Returns gamma (J/m^2), a float for
+    a scalar T, else an array."""
+    if isinstance(system, PCSAFT):
+        return _surface_tension_model(system, rho, x)
     return _omega_ex(system, _integrals(system, rho))
+
+
+def _surface_tension_model(model, T, x=None):
+    if x is not None and (len(x) != 1 or float(x[0]) != 1.0):
+        raise ValueError("surface_tension(model, T, x) covers pure components (x = [1.0])")
+    scalar = np.ndim(T) == 0
+    Ts = np.atleast_1d(np.asarray(T, dtype=np.float64))
+    p, rl, rv = saturation(model, Ts)
+    L = model.length_scale()
+    systems = [DFTSystem(model, TwoPhase1DCart((float(pk), float(Tk)), [float(lk)], [float(vk)], [-10 * L, 10 * L], 201))
+               for pk, Tk, lk, vk in zip(p, Ts, rl, rv)]
+    rhos = [initialize_profiles(sy) for sy in systems]
+    batch_converge(systems, rhos)
+    gam = np.array([surface_tension(sy, r) / 2 for sy, r in zip(systems, rhos)])
+    for sy in systems:
+        sy.close()
+    return float(gam[0]) if scalar else gam
 
 
 def interfacial_tension(system, rho):

@@ -71,3 +71,29 @@ def test_saturation_above_the_critical_temperature_is_refused():
     pm, _ = S.models(["methane"])
     with pytest.raises(ValueError):
         cd.saturation(pm, [120.0, 260.0])
+
+
+def test_surface_tension_of_a_model():
+    """surface_tension(model, T) (surface_tension.jl:13-29) for n-octane at three
+    temperatures: the device coexistence, one batched converge of the 201-point
+    TwoPhase1DCart systems on [-10L, 10L] and gamma = surface_tension(system, rho) / 2.  It
+    equals the same construction from the oracle's coexistence converged one system at a
+    time (1e-7), is a float for a scalar T, and falls with T."""
+    import cdft_b200 as cd
+    from oracle import pcsaft_bulk as pb
+    pm, om = S.models(["octane"])
+    Ts = [280.0, 298.15, 320.0]
+    g = cd.surface_tension(pm, Ts)
+    L = pm.length_scale()
+    for k, T in enumerate(Ts):
+        _, wl, wv = pb.saturation_pure(om, T)
+        wp = pb.pressure(om, [wv], T)
+        sy = cd.DFTSystem(pm, cd.TwoPhase1DCart((wp, T), [wl], [wv], [-10 * L, 10 * L], 201))
+        rho = cd.initialize_profiles(sy)
+        cd.converge(sy, rho)
+        want = cd.surface_tension(sy, rho) / 2
+        sy.close()
+        assert g[k] == pytest.approx(want, rel=1e-7), T
+    assert g[0] > g[1] > g[2] > 0.0
+    assert 0.005 < g[1] < 0.05   # J/m^2: n-octane's tension at 298 K is about 0.021
+    assert isinstance(cd.surface_tension(pm, 298.15), float)
