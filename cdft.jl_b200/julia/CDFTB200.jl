@@ -12,6 +12,7 @@ module CDFTB200
 using cDFT
 using cDFT: DFTSystem, DFTOptions, DFTProblem, AASol
 using Clapeyron: PCSAFTModel
+import Clapeyron                 # qualified calls (Clapeyron.assoc_pair_length)
 using ChainRulesCore
 using CUDA
 
@@ -334,6 +335,64 @@ end
 and `dpdθ` (3nc, Pa) describe how the bulk state follows θ (e.g. along the LLE, from
 Clapeyron with ForwardDiff); `nothing` holds it fixed.  Differentiable with ChainRulesCore.
 """
+"""
+    saturation_b200(model, T) -> (p, ρl, ρv)
+
+Vapour-liquid coexistence of a pure PC-SAFT component at every temperature in `T` (K), in
+one device launch (`cdft_saturation_pure`): pressures in Pa, densities in mol/m³.  This is
+the state `surface_tension(model, T, x)` takes from `bubble_pressure` for a pure component
+(src/methods/surface_tension.jl:13-20).  The association pair (2B self-association) comes
+from `pack_assoc_params`; its diameters do not enter the bulk equations.
+"""
+function saturation_b200(model::PCSAFTModel, T::AbstractVector{<:Real})
+    length(model) == 1 || error("saturation_b200 covers pure components")
+    Tv = Vector{Float64}(T)
+    n = length(Tv)
+    σ, ϵ = model.params.sigma.values[1, 1], model.params.epsilon.values[1, 1]
+    nassoc = Clapeyron.assoc_pair_length(model)
+    empty = CDFTAssocPair(0, 0, 0, 0, 0, 0, 0.0, 0.0)
+    pairs = if nassoc >= 1
+        (icomp, jcomp, isite, jsite, epsa, kap, _, _, nsflat, nscum, _) = cDFT.pack_assoc_params(model, [1.0])
+        ntuple(MAX_ASSOC) do p
+            p > nassoc && return empty
+            CDFTAssocPair(icomp[p] - 1, jcomp[p] - 1, isite[p] - 1, jsite[p] - 1,
+                          nsflat[nscum[icomp[p]] + isite[p]], nsflat[nscum[jcomp[p]] + jsite[p]], epsa[p], kap[p])
+        end
+    else
+        ntuple(_ -> empty, MAX_ASSOC)
+    end
+    d0 = σ * (1 - 0.12 * exp(-3ϵ / Tv[1]))     # hsd and T of the descriptor are not used
+    desc = CDFTSystemDesc(1, (Cint(1), Cint(1), Cint(1)), ntuple(_ -> 0.0, 6), 0, 1,
+                          pad([model.params.segment.values[1]], MAX_NC), pad([d0], MAX_NC),
+                          pad([σ], MAX_NC * MAX_NC), pad([ϵ], MAX_NC * MAX_NC), cDFT.length_scale(model),
+                          Tv[1], nassoc, pairs, pad([0.0], MAX_NC), Ptr{Cdouble}(C_NULL), Cint(0))
+    p, ρl, ρv, st = zeros(n), zeros(n), zeros(n), zeros(Cint, n)
+    check(ccall((:cdft_saturation_pure, LIB), Cint,
+                (Ref{CDFTSystemDesc}, Cint, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cint}),
+                desc, n, Tv, p, ρl, ρv, st))
+    all(==(0), st) || error("no coexistence at T = $(Tv[st .!= 0]) (status $(st[st .!= 0]))")
+    return p, ρl, ρv
+end
+
+"""
+    surface_tension_b200(model, T; mixed = false)
+
+`surface_tension(model, T, [1.0])` (src/methods/surface_tension.jl:13-29) at every
+temperature in `T` on the B200: the coexistence from `saturation_b200`, a
+`TwoPhase1DCart` on [-10L, 10L] with 201 points per temperature, the systems converged in one
+batch and `surface_tension(system, ρ) / 2`.
+"""
+function surface_tension_b200(model::PCSAFTModel, T::AbstractVector{<:Real}; mixed = false)
+    p, ρl, ρv = saturation_b200(model, T)
+    L = cDFT.length_scale(model)
+    systems = [DFTSystem(model, cDFT.TwoPhase1DCart((p[k], Float64(T[k])), [ρl[k]], [ρv[k]], [-10L, 10L], (201,)),
+                         DFTOptions(B200Device(mixed))) for k in eachindex(p)]
+    ρs = [cDFT.initialize_profiles(s) for s in systems]
+    converge_batch!(systems, ρs)
+    return [cDFT.surface_tension(s, ρ) / 2 for (s, ρ) in zip(systems, ρs)]
+end
+export saturation_b200, surface_tension_b200
+
 function interface_tension(θ::AbstractVector, system::B200System, ρ::Array{Float64}; dμdθ = nothing, dpdθ = nothing)
     model = system.model
     nc = length(model)
