@@ -165,6 +165,7 @@ struct Batch {
     long long stage_elems = 0;
     DenseGroup* d_groups = nullptr;                   // radial: column tiles of systems sharing an operator
     int ngroups = 0, group_blocks = 0;                // ... and the largest slots x row tiles among them
+    int group_blocks2 = 0;                            // ... the same in tiles of 16 rows
 };
 
 namespace {
@@ -909,6 +910,7 @@ int batch_build(const std::vector<cdft_plan*>& plans, Batch** out)
                 for (int c = 0; c < DGRP_COLS; ++c) G.sys[c] = mem[t + (c < G.ns ? c : 0)];
                 const SysDev& S = plans[G.sys[0]]->sys;
                 b->group_blocks = std::max(b->group_blocks, S.nc * S.nconv * ((S.N + 7) / 8));
+                b->group_blocks2 = std::max(b->group_blocks2, S.nc * S.nconv * ((S.N + 15) / 16));
                 groups.push_back(G);
             }
     }
@@ -1153,8 +1155,15 @@ int launch_eval3d(Batch* b, const AAState* st, bool with_int)
 template <typename T>
 int launch_dense_stage(Batch* b, const AAState* st, int stage)
 {
+    if (g_tuned.radial_dmma == 2) {
+        dense_group_kernel<T, 2><<<dim3(b->group_blocks2, b->ngroups), DGRP_WARPS * 32, 0, b->stream>>>(
+            b->d_sys, b->d_groups, stage, st);
+        g_launches += 1;
+        CHECK_LAUNCH();
+        return 0;
+    }
     if (g_tuned.radial_dmma) {
-        dense_group_kernel<T><<<dim3(b->group_blocks, b->ngroups), DGRP_WARPS * 32, 0, b->stream>>>(
+        dense_group_kernel<T, 1><<<dim3(b->group_blocks, b->ngroups), DGRP_WARPS * 32, 0, b->stream>>>(
             b->d_sys, b->d_groups, stage, st);
         g_launches += 1;
         CHECK_LAUNCH();

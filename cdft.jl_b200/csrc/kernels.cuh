@@ -1104,53 +1104,69 @@ struct DenseGroup {
     int sys[DGRP_COLS];       // their batch indices (unused entries repeat sys[0])
 };
 
-template <typename T>
+// RT: 8-row tiles per CTA (1 or 2).  With RT = 2 the two tiles share each input fragment
+// (12 loads in flight per lane instead of 8, half the CTAs); every output element runs the
+// same sequence of products and additions as with RT = 1, so the bits are the same.
+template <typename T, int RT>
 __global__ void __launch_bounds__(DGRP_WARPS * 32)
 dense_group_kernel(const SysDev* __restrict__ sys, const DenseGroup* __restrict__ groups, int stage,
                    const AAState* __restrict__ st)
 {
-    __shared__ double red[DGRP_WARPS][32][2];
+    __shared__ double red[DGRP_WARPS][RT][32][2];
     const DenseGroup& G = groups[blockIdx.y];
     const SysDev& S0 = sys[G.sys[0]];
     const int N = S0.N, nconv = S0.nconv, nc = S0.nc;
-    const int rtiles = (N + 7) >> 3;
+    const int rtiles = (N + 8 * RT - 1) / (8 * RT);   // CTA row blocks of 8 RT rows
     if ((int)blockIdx.x >= nc * nconv * rtiles) return;
-    const int slot = blockIdx.x / rtiles, j0 = (blockIdx.x - slot * rtiles) * 8;
+    const int slot = blockIdx.x / rtiles, j0 = (blockIdx.x - slot * rtiles) * 8 * RT;
     const int i = slot / nconv, f = slot - i * nconv;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r = lane >> 2, k = lane & 3;
-    // A: operator row j0 + r (rows past N read row N - 1 and are not stored)
-    const double* Arow = S0.mats + (((size_t)stage * nc * nconv + slot) * N + min(j0 + r, N - 1)) * N;
+    // A: operator rows j0 + 8 t + r (rows past N read row N - 1 and are not stored)
+    const double* Abase = S0.mats + ((size_t)stage * nc * nconv + slot) * N * (size_t)N;
+    const double* Arow[RT];
+#pragma unroll
+    for (int t = 0; t < RT; ++t) Arow[t] = Abase + (size_t)min(j0 + 8 * t + r, N - 1) * N;
     // B: column r is the input of the tile's r-th system (zero past ns or once converged)
     const bool cval = r < G.ns && sys_active(st, G.sys[r]);
     const SysDev& Sc = sys[G.sys[cval ? r : 0]];
     const double* x64 = Sc.rho + (size_t)i * N;
     const T* xT = reinterpret_cast<const T*>(Sc.dfield) + (size_t)(i * Sc.NF + f + 1) * N;
     const int nk4 = (N + 3) >> 2;
-    double c[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    double c[RT][4][2];
+#pragma unroll
+    for (int t = 0; t < RT; ++t)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) c[t][u][0] = c[t][u][1] = 0.0;
     for (int kb = warp; kb < nk4; kb += 4 * DGRP_WARPS) {   // warp-uniform trip count
-        double a[4], b[4];
+        double a[RT][4], b[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int q = (kb + u * DGRP_WARPS) * 4 + k;
             const bool in = q < N;
-            a[u] = in ? __ldg(Arow + q) : 0.0;
+#pragma unroll
+            for (int t = 0; t < RT; ++t) a[t][u] = in ? __ldg(Arow[t] + q) : 0.0;
             b[u] = (in && cval) ? (stage == 0 ? __ldg(x64 + q) : double(xT[q])) : 0.0;
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) dmma_m8n8k4(c[u][0], c[u][1], a[u], b[u]);
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int t = 0; t < RT; ++t) dmma_m8n8k4(c[t][u][0], c[t][u][1], a[t][u], b[u]);
     }
-    red[warp][lane][0] = (c[0][0] + c[1][0]) + (c[2][0] + c[3][0]);
-    red[warp][lane][1] = (c[0][1] + c[1][1]) + (c[2][1] + c[3][1]);
+#pragma unroll
+    for (int t = 0; t < RT; ++t) {
+        red[warp][t][lane][0] = (c[t][0][0] + c[t][1][0]) + (c[t][2][0] + c[t][3][0]);
+        red[warp][t][lane][1] = (c[t][0][1] + c[t][1][1]) + (c[t][2][1] + c[t][3][1]);
+    }
     __syncthreads();
-    if (warp != 0) return;
-    const int j = j0 + r;
+    if (warp >= RT) return;   // warp t sums and stores row tile t
+    const int j = j0 + 8 * warp + r;
     if (j >= N) return;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         double acc = 0.0;
 #pragma unroll
-        for (int w = 0; w < DGRP_WARPS; ++w) acc += red[w][lane][h];
+        for (int w = 0; w < DGRP_WARPS; ++w) acc += red[w][warp][lane][h];
         const int col = 2 * k + h;
         if (col < G.ns && sys_active(st, G.sys[col])) {
             const SysDev& So = sys[G.sys[col]];

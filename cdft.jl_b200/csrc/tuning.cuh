@@ -33,10 +33,13 @@ struct TunedShapes {
     // rows and runs one block per SM), so 0.
     int fft3d_fused_phi = 0;
     // radial grids: the dense weighted-density operators of a batch as FP64 tensor-core GEMMs
-    // over column tiles of systems that share one operator (1), or one warp-per-row FFMA
-    // matrix-vector launch per system (0).  The two sum in different orders; the GEMM's
-    // per-element sum does not depend on the other systems of the tile.
-    int radial_dmma = 1;
+    // over column tiles of systems that share one operator, 8 rows per CTA (1) or 16 rows per
+    // CTA sharing the input fragments (2, the same bits as 1), or one warp-per-row FFMA
+    // matrix-vector launch per system (0).  The GEMM and the FFMA kernel sum in different
+    // orders; the GEMM's per-element sum does not depend on the other systems of the tile.
+    // Measured on the spherical-pore isotherm batch: dense stage 274.5 us (0), 12.35 us (1),
+    // 10.30 us (2), so 2.
+    int radial_dmma = 2;
 };
 
 static TunedShapes g_tuned;
@@ -52,7 +55,7 @@ static const TunedEntry kTunedEntries[] = {
     {"pers_cluster", &TunedShapes::pers_cluster, 0, 1},
     {"fft3d_tma", &TunedShapes::fft3d_tma, 0, 1},
     {"fft3d_fused_phi", &TunedShapes::fft3d_fused_phi, 0, 1},
-    {"radial_dmma", &TunedShapes::radial_dmma, 0, 1},
+    {"radial_dmma", &TunedShapes::radial_dmma, 0, 2},
 };
 
 inline const TunedEntry* tuned_entry(const char* name)

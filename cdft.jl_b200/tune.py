@@ -111,7 +111,7 @@ def sweep_radial():
         cd.dFdrho_res(sy, cd.initialize_profiles(sy))   # the plans' device profiles
     plans = (ctypes.c_void_p * len(systems))(*[sy._plan.value for sy in systems])
     out = {}
-    for v in (0, 1):
+    for v in (0, 1, 2):
         cd.tuning("radial_dmma", v)
         ms = ctypes.c_double()
         _lib.check(lib.cdft_batch_time_stage(plans, len(systems), 0, 50, ctypes.byref(ms)))

@@ -328,70 +328,73 @@ def test_tma_shared_memory_fits(fp32, L):
 DGRP_COLS, DGRP_WARPS = 8, 8
 
 
-def dense_group_emulate(mats, xs, N, slots, active):
-    """dense_group_kernel (csrc/kernels.cuh) step by step for one column tile: per CTA
-    (slot, 8-row tile) and warp, the k = 4 blocks kb = warp, warp + 8, ... in unrolled
-    groups of four into four accumulator pairs, every index checked against its buffer;
-    then the fixed-order sum over warps.  Returns out[col][slot][j] (NaN where not stored)
-    and the number of times each (row, col, q) product was formed."""
+def dense_group_emulate(mats, xs, N, slots, active, RT=1):
+    """dense_group_kernel<T, RT> (csrc/kernels.cuh) step by step for one column tile: per CTA
+    (slot, RT 8-row tiles) and warp, the k = 4 blocks kb = warp, warp + 8, ... in unrolled
+    groups of four into four accumulator pairs per row tile, every index checked against its
+    buffer; then the fixed-order sum over warps.  Returns out[col][slot][j] (NaN where not
+    stored) and the number of times each (row, q) product was formed for column 0."""
     ns = len(xs)
-    rtiles = (N + 7) >> 3
+    rtiles = (N + 8 * RT - 1) // (8 * RT)
     nk4 = (N + 3) >> 2
     out = np.full((ns, slots, N), np.nan)
     seen = np.zeros((slots, N, N), dtype=np.int64)
     for bx in range(slots * rtiles):
-        slot, j0 = bx // rtiles, (bx % rtiles) * 8
-        red = np.zeros((DGRP_WARPS, 8, 8))
+        slot, j0 = bx // rtiles, (bx % rtiles) * 8 * RT
+        red = np.zeros((DGRP_WARPS, RT, 8, 8))
         for warp in range(DGRP_WARPS):
-            acc = np.zeros((4, 8, 8))
+            acc = np.zeros((RT, 4, 8, 8))
             kb = warp
             while kb < nk4:
                 for u in range(4):
-                    for lane in range(32):
-                        r, k = lane >> 2, lane & 3
-                        q = (kb + u * DGRP_WARPS) * 4 + k
-                        row = min(j0 + r, N - 1)
-                        assert 0 <= row < N
-                        if q < N:
-                            assert 0 <= slot * N * N + row * N + q < slots * N * N
-                    # the tile product of this k block: A[8 x 4] B[4 x 8]
-                    for r in range(8):
-                        row = min(j0 + r, N - 1)
-                        for k in range(4):
-                            q = (kb + u * DGRP_WARPS) * 4 + k
-                            if q >= N:
-                                continue
-                            for c in range(8):
-                                if c < ns and active[c]:
-                                    acc[u, r, c] += mats[slot, row, q] * xs[c][slot, q]
-                                    if j0 + r < N:
-                                        seen[slot, j0 + r, q] += (c == 0)
+                    for t in range(RT):
+                        for r in range(8):
+                            row = min(j0 + 8 * t + r, N - 1)
+                            assert 0 <= row < N
+                            for k in range(4):
+                                q = (kb + u * DGRP_WARPS) * 4 + k
+                                if q >= N:
+                                    continue
+                                assert 0 <= slot * N * N + row * N + q < slots * N * N
+                                for c in range(8):
+                                    if c < ns and active[c]:
+                                        acc[t, u, r, c] += mats[slot, row, q] * xs[c][slot, q]
+                                        if j0 + 8 * t + r < N and c == 0:
+                                            seen[slot, j0 + 8 * t + r, q] += 1
                 kb += 4 * DGRP_WARPS
-            red[warp] = (acc[0] + acc[1]) + (acc[2] + acc[3])
-        tot = np.zeros((8, 8))
-        for w in range(DGRP_WARPS):
-            tot += red[w]
-        for r in range(8):
-            j = j0 + r
-            if j >= N:
-                continue
-            for c in range(8):
-                if c < ns and active[c]:
-                    out[c, slot, j] = tot[r, c]
+            for t in range(RT):
+                red[warp, t] = (acc[t, 0] + acc[t, 1]) + (acc[t, 2] + acc[t, 3])
+        for t in range(RT):
+            tot = np.zeros((8, 8))
+            for w in range(DGRP_WARPS):
+                tot += red[w, t]
+            for r in range(8):
+                j = j0 + 8 * t + r
+                if j >= N:
+                    continue
+                for c in range(8):
+                    if c < ns and active[c]:
+                        assert np.isnan(out[c, slot, j])   # every output is stored once
+                        out[c, slot, j] = tot[r, c]
     return out, seen
 
 
+@pytest.mark.parametrize("RT", [1, 2])
 @pytest.mark.parametrize("N,ns", [(13, 3), (61, 8), (40, 1)])
-def test_dense_group_index_map(N, ns):
+def test_dense_group_index_map(N, ns, RT):
     """Every operator row meets every input entry exactly once per output, the loads stay
     inside the operator and input buffers, rows past N and inactive columns are not
-    written, and the result is A x per system."""
+    written, and the result is A x per system; 16-row CTAs (RT = 2) give the same bits as
+    8-row ones."""
     rng = np.random.default_rng(N)
     slots = 2
     mats = rng.standard_normal((slots, N, N))
     xs = [rng.standard_normal((slots, N)) for _ in range(ns)]
     active = [c != 1 for c in range(8)]
-    out, seen = dense_group_emulate(mats, xs, N, slots, active)
+    out, seen = dense_group_emulate(mats, xs, N, slots, active, RT)
+    if RT == 2:
+        ref, _ = dense_group_emulate(mats, xs, N, slots, active, 1)
+        assert np.array_equal(np.nan_to_num(out, nan=7.0), np.nan_to_num(ref, nan=7.0))
     if active[0]:
         assert np.all(seen == 1)
     for c in range(ns):
