@@ -214,24 +214,9 @@ __global__ void bulk_density_kernel(BulkModel M, int n, const double* __restrict
     status[s] = 0;
 }
 
-// d(p / k_B T) / d rho = Z + rho dZ/drho = 1 + 2 rho a' + rho^2 a'' at number density rho,
-// with a' exact (dual numbers) and a'' by a central difference of a' (step 1e-5 rho: the
-// Jacobian only sets Newton's rate, the residuals below are exact).  Also returns
-// Z and the Gibbs term g = a_res + Z + ln rho.
-__device__ __forceinline__ double bulk_dpdrho(const BulkModel& M, const double* x, double rho, double* Z, double* g)
-{
-    const Dual a = bulk_ares(M, x, Dual{rho, 1.0});
-    const double h = 1e-5 * rho;
-    const double ap = bulk_ares(M, x, Dual{rho + h, 1.0}).d, am = bulk_ares(M, x, Dual{rho - h, 1.0}).d;
-    const double a2 = (ap - am) / (2.0 * h);
-    *Z = 1.0 + rho * a.d;
-    *g = a.v + *Z + log(rho);
-    return 1.0 + 2.0 * rho * a.d + rho * rho * a2;
-}
-
 // Pure-component vapour-liquid coexistence, one warp per temperature (models[s] holds the
 // component at T_s).  Start as the host solver does: the densest root of p = p_start (the
-// warp scans the packing-fraction grid of bulk_density_kernel) and the ideal-gas vapour
+// warp scans the packing-fraction grid of bulk_density_kernel, lane 0 refines it) and the ideal-gas vapour
 // p_start / k_B T.  Then Newton on y = (ln rho_l, ln rho_v) for
 //   F1 = rho_l Z_l - rho_v Z_v   (p_l - p_v over k_B T),   F2 = g_l - g_v   (mu_l - mu_v over k_B T).
 // Gibbs-Duhem (d mu = dp / rho at fixed T) gives the Jacobian from P' = d(p / k_B T)/d rho
@@ -255,27 +240,51 @@ __global__ void saturation_kernel(const BulkModel* __restrict__ models, int n, d
     const double scale = PI / 6.0 * M.m[0] * M.d[0] * M.d[0] * M.d[0];
     for (int k = lane; k < BULK_GRID; k += 32) fgrid[k] = bulk_pressure(M, x, bulk_grid_eta(k) / scale) - p_start;
     __syncwarp();
-    if (lane != 0) return;
     const double nan = __longlong_as_double(0x7ff8000000000000LL);
     auto fail = [&](int code) {
+        if (lane != 0) return;
         p_out[s] = nan;
         rl_out[s] = nan;
         rv_out[s] = nan;
         status[s] = code;
     };
-    auto sgn = [](double v) { return v > 0 ? 1 : (v < 0 ? -1 : 0); };
+    // lane 0 finds the densest sign change and refines the liquid root there
     int last = -1;
-    for (int k = 0; k + 1 < BULK_GRID; ++k)
-        if (sgn(fgrid[k]) != sgn(fgrid[k + 1])) last = k;
+    double rl0 = 0.0;
+    if (lane == 0) {
+        auto sgn = [](double v) { return v > 0 ? 1 : (v < 0 ? -1 : 0); };
+        for (int k = 0; k + 1 < BULK_GRID; ++k)
+            if (sgn(fgrid[k]) != sgn(fgrid[k + 1])) last = k;
+        if (last >= 0)
+            rl0 = bulk_refine(M, x, scale, p_start, bulk_grid_eta(last), bulk_grid_eta(last + 1), fgrid[last],
+                              fgrid[last + 1]) / scale;
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    rl0 = __shfl_sync(0xffffffffu, rl0, 0);
     if (last < 0) return fail(1);
-    const double rl0 = bulk_refine(M, x, scale, p_start, bulk_grid_eta(last), bulk_grid_eta(last + 1), fgrid[last],
-                                   fgrid[last + 1]) / scale;
+    // Newton on the whole warp: lanes 0-2 evaluate a_res (dual numbers: a and a') at rho_l,
+    // rho_l + h, rho_l - h and lanes 3-5 at rho_v, rho_v + h, rho_v - h, h = 1e-5 rho (the other
+    // lanes repeat one of them); every lane then forms the same step from the shuffled values:
+    // Z = 1 + rho a', g = a + Z + ln rho, and P' = d(p / k_B T)/d rho = 1 + 2 rho a' + rho^2 a''
+    // with a'' the central difference of a' (it only sets Newton's rate; the residuals are
+    // exact), so the warp takes the same steps as one lane would
+    const int ph = lane < 3 ? 0 : 1, kind = lane % 3;
     double yl = log(rl0), yv = log(p_start / (kB * M.T));
     bool conv = false;
     for (int it = 0; it < 100; ++it) {
         const double rl = exp(yl), rv = exp(yv);
-        double Zl, Zv, gl, gv;
-        const double Pl = bulk_dpdrho(M, x, rl, &Zl, &gl), Pv = bulk_dpdrho(M, x, rv, &Zv, &gv);
+        const double r = ph == 0 ? rl : rv;
+        const double h = 1e-5 * r;
+        const Dual a = bulk_ares(M, x, Dual{kind == 0 ? r : (kind == 1 ? r + h : r - h), 1.0});
+        const double avl = __shfl_sync(0xffffffffu, a.v, 0), adl = __shfl_sync(0xffffffffu, a.d, 0);
+        const double apl = __shfl_sync(0xffffffffu, a.d, 1), aml = __shfl_sync(0xffffffffu, a.d, 2);
+        const double avv = __shfl_sync(0xffffffffu, a.v, 3), adv = __shfl_sync(0xffffffffu, a.d, 3);
+        const double apv = __shfl_sync(0xffffffffu, a.d, 4), amv = __shfl_sync(0xffffffffu, a.d, 5);
+        const double hl = 1e-5 * rl, hv = 1e-5 * rv;
+        const double a2l = (apl - aml) / (2.0 * hl), a2v = (apv - amv) / (2.0 * hv);
+        const double Zl = 1.0 + rl * adl, Zv = 1.0 + rv * adv;
+        const double gl = avl + Zl + log(rl), gv = avv + Zv + log(rv);
+        const double Pl = 1.0 + 2.0 * rl * adl + rl * rl * a2l, Pv = 1.0 + 2.0 * rv * adv + rv * rv * a2v;
         const double F1 = rl * Zl - rv * Zv, F2 = gl - gv;
         const double dl = (rv * F2 - F1) / (Pl * (rv - rl)), dv = (rl * F2 - F1) / (Pv * (rv - rl));
         if (!isfinite(dl) || !isfinite(dv)) return fail(3);
@@ -291,6 +300,7 @@ __global__ void saturation_kernel(const BulkModel* __restrict__ models, int n, d
     const double rl = exp(yl), rv = exp(yv);
     if (!conv) return fail(2);
     if (!(fabs(rl / rv - 1.0) > 1e-6)) return fail(3);
+    if (lane != 0) return;
     p_out[s] = bulk_pressure(M, x, rv);   // the vapour side: Z_l ~ 1e-6 at low T makes p(rho_l) ill-conditioned
     rl_out[s] = rl / NAVO;
     rv_out[s] = rv / NAVO;
